@@ -1,0 +1,296 @@
+"""Benchmark of the mesh -> node-grid path.
+
+Workload (one step): the room scene -- an inward 10 x 7.5 x 5 box shell plus
+200 rotated icospheres / tori, 1,049,868 float32 triangles, 17 materials --
+voxelized with Voxelizer<LongNode>::voxelizeToNodesToRAM(1024) semantics:
+solid + surface voxelization, split-ordered pruning and node emission into a
+1088 x 771 x 515 LongNode grid (432,006,720 nodes, 864 MB).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value: Gvoxels/s of node grid, device resident (mesh already on the GPU,
+  output in HBM), timed with CUDA events on the launching stream; the L2 is
+  flushed (256 MB write) before every timed step.
+e2e: the same metric through the reference-facing C ABI with host buffers:
+  each step constructs the voxelizer from pinned host arrays, uploads the
+  mesh, voxelizes and copies the node grid back into pinned host memory.
+--impl reference: the reference algorithm's CPU restatement (oracle/) on
+  all host cores, on a bounded sample of the same workload.
+Multi-GPU: replicas only (the path does not shard); under torchrun every
+rank voxelizes its own copy and value sums the voxels of all ranks over the
+slowest rank's time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "node-grid voxelization throughput (Gvoxels/s), bit-exact vs reference"
+UNIT = "Gvoxels/s"
+WORKLOAD = "room scene, 1,049,868 triangles, 17 materials, LongNode, maxDimension 1024 -> 1088x771x515 nodes"
+MAX_DIM = 1024
+CPU_SAMPLE_DIM = 384
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the emit kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    try:
+        with open(path) as fh:
+            for line in fh:
+                k, _, v = line.partition("=")
+                if k.strip() == "emit_cartesian_long_room1024_bytes":
+                    return float(v)
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                           "-i", str(self.index), "-lms", "100"], stdout=subprocess.PIPE,
+                                          stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self._proc = None
+        return self
+
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self._proc:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
+        mx = max(float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[4 + i] == "Active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args, world, rank):
+    """CPU restatement of the reference (oracle/) on all host cores."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from voxelizer_b200 import scenes
+
+    mesh = scenes.room_scene()
+    cores = os.cpu_count() or 1
+    times = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        out, info, _ = O.voxelize(mesh, 1, 1, 1, CPU_SAMPLE_DIM, threads=cores)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+        del out
+    n = info.dims[0] * info.dims[1] * info.dims[2]
+    t = sum(times)
+    value = n * len(times) / t / 1e9
+    sample = (f"room scene (1,049,868 triangles, 17 materials), LongNode, maxDimension {CPU_SAMPLE_DIM} -> "
+              f"{info.dims[0]}x{info.dims[1]}x{info.dims[2]} nodes per step (full path)")
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t / len(times), 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32+u32",
+            "data": "synthetic (seeded room scene)",
+            "config": {"workload": WORKLOAD, "sample": sample},
+            "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(mesh):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    out, info, _ = O.voxelize(mesh, 1, 1, 1, CPU_SAMPLE_DIM, threads=cores)
+    dt = time.perf_counter() - t0
+    n = info.dims[0] * info.dims[1] * info.dims[2]
+    return {"value": round(n / dt / 1e9, 6), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"same scene at maxDimension {CPU_SAMPLE_DIM} ({info.dims[0]}x{info.dims[1]}x{info.dims[2]} "
+                      f"nodes), one full path, {dt:.1f} s"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import torch
+
+    from voxelizer_b200 import scenes
+    from voxelizer_b200.api import LONG, Voxelizer
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    mesh = scenes.room_scene()
+    vx = Voxelizer(mesh.vertices, mesh.indices, mesh.materials, mesh.n_materials, node_type=LONG, device=local)
+    info = vx.plan(1, MAX_DIM)
+    n_nodes = int(info.count)
+    out = torch.empty(int(info.bytes), dtype=torch.uint8, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    vx.set_profiling(True)
+    for _ in range(args.warmup):
+        vx.voxelize_device(1, MAX_DIM, out, stream=sh)
+    stream.synchronize()
+    launches = vx.last_launch_count()
+
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    stage_acc = {}
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            evs[i][0].record(stream)
+            vx.voxelize_device(1, MAX_DIM, out, stream=sh)
+            evs[i][1].record(stream)
+            st = vx.stage_times()
+            for k, v in st.items():
+                stage_acc.setdefault(k, []).append(v)
+        stream.synchronize()
+    torch.cuda.synchronize()
+    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    ms = total_ms / args.steps
+    value = n_nodes * world / (ms * 1e-3) / 1e9
+
+    # e2e through the reference-facing entry with host buffers.
+    vx.set_profiling(False)
+    pin_v = torch.from_numpy(mesh.vertices.reshape(-1)).pin_memory().numpy()
+    pin_i = torch.from_numpy(mesh.indices.reshape(-1).view(np.int32)).pin_memory().numpy().view(np.uint32)
+    pin_m = torch.from_numpy(mesh.materials).pin_memory().numpy()
+    host_out = torch.empty(int(info.bytes), dtype=torch.uint8).pin_memory().numpy().view(np.uint16)
+    e2e_ms = []
+    for i in range(args.e2e_steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with Voxelizer(pin_v, pin_i, pin_m, mesh.n_materials, node_type=LONG, device=local) as v2:
+            v2.voxelizeToNodesToRAM(MAX_DIM, out=host_out)
+        torch.cuda.synchronize()
+        if i > 0:
+            e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    e2e = sum(e2e_ms) / len(e2e_ms)
+    if dist:
+        t = torch.tensor([e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e = float(t.item())
+    e2e_value = n_nodes * world / (e2e * 1e-3) / 1e9
+
+    peak, peak_kind = peaks()
+    emit_ms = sorted(stage_acc.get("emit", [0.0]))[len(stage_acc.get("emit", [0.0])) // 2]
+    emit_bytes = n_nodes * 2 + 2 * n_nodes / 8  # node grid write + final and surface bit grids read
+    achieved = emit_bytes / (emit_ms * 1e-3) / 1e9 if emit_ms > 0 else None
+    path_bytes = 12 * mesh.n_vertices + 13 * mesh.n_triangles + n_nodes * 2
+    traffic = ncu_traffic()
+    line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+f32+u32", "data": "synthetic (seeded room scene)",
+            "config": {"workload": WORKLOAD, "l2": "256 MB flush before every timed step",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "kernel": "emitCartesianKernel<LongNode>",
+                         "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
+                         "peak_kind": peak_kind, "frac": round(achieved / peak, 4) if achieved else None,
+                         "traffic": traffic, "algorithmic_bytes": int(emit_bytes), "ms": round(emit_ms, 4)},
+            "path_roofline": {"algorithmic_bytes": int(path_bytes),
+                              "achieved": round(path_bytes / (ms * 1e-3) / 1e9, 1),
+                              "frac": round(path_bytes / (ms * 1e-3) / 1e9 / peak, 4)},
+            "stages_ms": {k: round(sorted(v)[len(v) // 2], 4) for k, v in stage_acc.items()},
+            "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "ms_per_step": round(e2e, 3),
+                    "h2d_bytes_per_step": int(12 * mesh.n_vertices + 13 * mesh.n_triangles),
+                    "d2h_bytes_per_step": int(info.bytes)},
+            "gpu_launches": int(launches * args.steps),
+            "clocks": clk.summary()}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(mesh)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,138 @@
+/* vxb: C ABI of the B200 voxelizer (mesh -> solid bit array / FDTD node grid).
+ *
+ * This is the drop-in boundary for hakarlss/Voxelizer's single-GPU path.
+ * Every entry point below replaces one public member of the reference's
+ * `vox::Voxelizer<Node>` (include/voxelizer.h) or, for the device-resident
+ * and batched calls, the launcher seam beneath it
+ * (include/host_device_interface.h).  Types are plain C: pointers, sizes and
+ * POD structs.  Every function returns a vxb_status; on failure
+ * vxb_last_error() holds a message (thread-local).
+ *
+ * Node layouts in output buffers are byte-identical to
+ * include/node_types.h of the reference:
+ *   VXB_SHORT_NODE      1 byte : bid bits 0-4, material bits 5-7
+ *   VXB_LONG_NODE       2 bytes: bid, material
+ *   VXB_PARTIAL_NODE    8 bytes: bid, material, 2 padding bytes, float ratio
+ *   VXB_SHORT_FCC_NODE  2 bytes: 12-bit neighbour mask, 4-bit material
+ *   VXB_LONG_FCC_NODE   4 bytes: uint16 mask, material, 1 padding byte
+ * Plain voxelization output is the reference's bit array: uint32 words, row
+ * major (z, y, x/32), voxel x = 32*w + b stored in bit (31 - b) of word w.
+ */
+#ifndef VXB_H
+#define VXB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int vxb_status;
+#define VXB_OK              0
+#define VXB_EINVAL         -1   /* invalid argument */
+#define VXB_ENOMEM         -2   /* device or host allocation failed */
+#define VXB_ECUDA          -3   /* CUDA runtime error */
+#define VXB_EUNSUPPORTED   -4   /* combination the reference rejects (e.g. FCC + plain voxelization) */
+#define VXB_ETIMEDOUT      -5   /* a bounded device-side wait ran out */
+#define VXB_EOVERFLOW      -6   /* grid or work list exceeds 32-bit indexing (as in the reference) */
+#define VXB_ENOMATERIALS   -7   /* material output requested without materials */
+
+typedef enum {
+    VXB_SHORT_NODE = 0,
+    VXB_LONG_NODE = 1,
+    VXB_PARTIAL_NODE = 2,
+    VXB_SHORT_FCC_NODE = 3,
+    VXB_LONG_FCC_NODE = 4
+} vxb_node_type;
+
+typedef struct { uint32_t x, y, z; } vxb_uint3;
+
+/* One voxelization request: the arguments of Voxelizer::voxelize* (either a
+ * maxDimension or a cubeLength, plus the internal split sizes). */
+typedef struct {
+    int by_cube_length;        /* 1: cube_length is used, 0: max_dimension */
+    uint32_t max_dimension;    /* voxels along the longest bounding-box side */
+    double cube_length;        /* distance between voxel centres */
+    vxb_uint3 vox_split_res;   /* reference default (1024, 512, 512) */
+    vxb_uint3 mat_split_res;   /* reference default (512, 512, 512) */
+} vxb_request;
+
+/* Shape of a result; mirrors NodePointer<Node>::dim plus the plan values. */
+typedef struct {
+    vxb_uint3 dim;             /* output dims: nodes, or voxels for bit arrays */
+    uint64_t bytes;            /* output size in bytes */
+    uint64_t count;            /* nodes, or uint32 words for bit arrays */
+    double voxel_length;
+    double min_vertex[3];
+    double max_vertex[3];
+    vxb_uint3 resolution;      /* voxel resolution incl. x padding/rounding, before y/z padding */
+    uint32_t x_splits;
+} vxb_grid_info;
+
+typedef struct vxb_voxelizer vxb_voxelizer;
+
+/* Last error message of the calling thread ("" if none). */
+const char* vxb_last_error(void);
+/* Library version string. */
+const char* vxb_version(void);
+
+/* Voxelizer(vertices, indices, nrOfVertices, nrOfTriangles),
+ * include/voxelizer.h:712-716.  The arrays are copied; the caller may free
+ * them after the call.  `device` selects the CUDA device (reference: 0). */
+vxb_status vxb_create(vxb_voxelizer** out, int node_type, const float* vertices, const uint32_t* indices,
+                      uint32_t n_vertices, uint32_t n_triangles, int device);
+/* ~Voxelizer(): frees the instance and every device buffer it holds. */
+vxb_status vxb_destroy(vxb_voxelizer* v);
+
+/* setMaterials(materials, nrOfUniqueMaterials), include/voxelizer.h:862,
+ * src/host_side.cpp:218-243: one material id per triangle; rejects more
+ * unique materials than the node type holds; enables material output. */
+vxb_status vxb_set_materials(vxb_voxelizer* v, const uint8_t* materials, uint32_t n_unique_materials);
+/* setMaterialOutput(bool), include/voxelizer.h:864. */
+vxb_status vxb_set_material_output(vxb_voxelizer* v, int enable);
+/* verboseOutput(bool), include/voxelizer.h:866. */
+vxb_status vxb_verbose_output(vxb_voxelizer* v, int enable);
+
+/* Dimensions, voxel length and bounds a request produces, without running
+ * it (getArrayDimensions, include/voxelizer.h:868-875, plus the getters
+ * getVoxelLength / getMinVertex / getMaxVertex / getResolution).
+ * `nodes` = 1 for node grids, 0 for the plain bit array. */
+vxb_status vxb_plan(vxb_voxelizer* v, int nodes, const vxb_request* req, vxb_grid_info* info);
+
+/* getArrayDimensions(longestSizeInVoxels | cubeLength, maxInternalXSize,
+ * sliceAlongX), src/host_side.cpp:3329-3475.  sliceAlongX is not supported
+ * (the slice API is outside this library) and returns VXB_EUNSUPPORTED. */
+vxb_status vxb_get_array_dimensions(vxb_voxelizer* v, int by_cube_length, uint32_t max_dimension,
+                                    double cube_length, uint32_t max_internal_x, int slice_along_x,
+                                    vxb_uint3* dims);
+
+/* voxelizeToRAM / voxelizeToNodesToRAM, include/voxelizer.h:727-782,
+ * src/host_side.cpp:1829-1886 and 2275-2337: runs the whole path and copies
+ * the result into `host_out` (>= info.bytes bytes).  Synchronous. */
+vxb_status vxb_voxelize_to_host(vxb_voxelizer* v, int nodes, const vxb_request* req, void* host_out,
+                                uint64_t host_bytes, vxb_grid_info* info);
+
+/* voxelize / voxelizeToNodes with devConfig (1,1), include/voxelizer.h:718-770:
+ * writes the result into the caller's device buffer `dev_out`, stream-ordered
+ * on `stream` (a cudaStream_t, NULL for the default stream).  The mesh is
+ * uploaded on the first call and stays resident.  Returns once the work is
+ * enqueued unless a split needs a host decision (none on the default path). */
+vxb_status vxb_voxelize_to_device(vxb_voxelizer* v, int nodes, const vxb_request* req, void* dev_out,
+                                  uint64_t dev_bytes, void* stream, vxb_grid_info* info);
+
+/* Number of kernels the last voxelize call launched on the device. */
+vxb_status vxb_last_launch_count(vxb_voxelizer* v, uint32_t* launches);
+
+/* Stage timing with CUDA events on the call's stream (off by default; no
+ * reference counterpart, the reference only prints clock() stamps in verbose
+ * mode).  Stages: 0 solid voxelization, 1 surface voxelization, 2 pruning,
+ * 3 node emission.  vxb_stage_times waits for the last call and writes the
+ * milliseconds of up to n stages (-1 for a stage that did not run). */
+vxb_status vxb_set_profiling(vxb_voxelizer* v, int enable);
+vxb_status vxb_stage_times(vxb_voxelizer* v, float* ms, uint32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VXB_H */

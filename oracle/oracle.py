@@ -1,0 +1,140 @@
+"""ctypes binding of the CPU restatement (liboracle.so, built from
+vox_oracle.cpp by ``make -C oracle oracle``).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg as the checker.  The product library never uses
+it.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+# Expression sites of the contraction model, in the order of ORC_S_* in
+# vox_oracle.h.
+SITES = ["P_BIN", "E_BIN", "D_BIN", "TN", "P_GEN", "CR_GEN", "D_GEN", "E_GEN", "B_GEN",
+         "CRF_CLS", "CRF_2D", "CRF_3D", "PC_2D", "PC_3D", "PC_3DL",
+         "DE_2D_YZ", "DE_2D_ZX", "DE_2D_XY", "DE_3D_YZ", "DE_3D_ZX", "DE_3D_XY",
+         "OT_2D_YZ", "OT_2D_ZX", "OT_2D_XY", "OT_3D_YZ", "OT_3D_ZX", "OT_3D_XY",
+         "OT_3DX_ZX", "OT_3DX_XY", "OT_3DY_XY", "OT_3DY_YZ", "OT_3DZ_YZ", "OT_3DZ_ZX",
+         "DT_3DX", "DT_3DY", "DT_3DZ"]
+SITE = {n: i for i, n in enumerate(SITES)}
+
+# Contraction modes of the reference build, pinned against the reference's
+# own CUDA output on a B200 (tests/golden).  The CUDA kernels compile the same
+# table (voxelizer_b200/csrc/vxb_sites.inc), which is parsed here so that the
+# checker and the product always evaluate identical expression forms.
+SITES_INC = os.path.join(os.path.dirname(HERE), "voxelizer_b200", "csrc", "vxb_sites.inc")
+
+
+def _read_sites(path=SITES_INC):
+    out = {}
+    with open(path) as fh:
+        for line in fh:
+            line = line.strip()
+            if line.startswith("constexpr int "):
+                name, val = line[len("constexpr int "):].rstrip(";").split("=")
+                out[name.strip()] = int(val)
+    return out
+
+
+PINNED_FMA = _read_sites()
+
+
+def fma_sites(model=None):
+    """48-entry site array from a {site name: mode} dict (None: pinned)."""
+    arr = [0] * 48
+    for k, v in (PINNED_FMA if model is None else model).items():
+        arr[SITE[k]] = int(v)
+    return arr
+
+NODE_BYTES = {0: 1, 1: 2, 2: 8, 3: 2, 4: 4}
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("node_type", ctypes.c_int), ("node_output", ctypes.c_int), ("materials", ctypes.c_int),
+                ("by_cube_length", ctypes.c_int), ("max_dim", ctypes.c_uint32), ("cube_length", ctypes.c_double),
+                ("vox_split", ctypes.c_uint32 * 3), ("mat_split", ctypes.c_uint32 * 3),
+                ("fma_sites", ctypes.c_uint8 * 48), ("threads", ctypes.c_int)]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [("dims", ctypes.c_uint32 * 3), ("out_bytes", ctypes.c_uint64), ("voxel_length", ctypes.c_double),
+                ("min_vertex", ctypes.c_double * 3), ("resolution", ctypes.c_uint32 * 3),
+                ("x_splits", ctypes.c_uint32), ("n_conflicts", ctypes.c_uint64), ("n_surface", ctypes.c_uint64),
+                ("prune_passes", ctypes.c_uint32)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run `make -C oracle oracle`")
+        _lib = ctypes.CDLL(LIB_PATH)
+        _lib.orc_plan.restype = ctypes.c_int
+        _lib.orc_plan.argtypes = [ctypes.POINTER(_Params), ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(Info)]
+        _lib.orc_voxelize.restype = ctypes.c_int
+        _lib.orc_voxelize.argtypes = [ctypes.POINTER(_Params), ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                      ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                      ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(Info)]
+    return _lib
+
+
+def _params(node_type, nodes, materials, size, vox, mat, fma_model, threads):
+    p = _Params()
+    p.node_type = int(node_type)
+    p.node_output = int(bool(nodes))
+    p.materials = int(bool(materials))
+    p.by_cube_length = int(isinstance(size, float))
+    p.max_dim = 0 if isinstance(size, float) else int(size)
+    p.cube_length = float(size) if isinstance(size, float) else 0.0
+    p.vox_split[:] = list(vox)
+    p.mat_split[:] = list(mat)
+    p.fma_sites[:] = fma_sites(fma_model)
+    p.threads = int(threads)
+    return p
+
+
+def out_dtype(node_type, nodes):
+    if not nodes:
+        return np.uint32
+    return {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}[NODE_BYTES[node_type]]
+
+
+def plan(mesh, node_type, nodes, size, vox=(1024, 512, 512)):
+    p = _params(node_type, nodes, 0, size, vox, (512, 512, 512), None, 0)
+    info = Info()
+    rc = lib().orc_plan(ctypes.byref(p), mesh.vertices.ctypes.data, mesh.n_vertices, ctypes.byref(info))
+    if rc:
+        raise RuntimeError(f"orc_plan failed: {rc}")
+    return info
+
+
+def voxelize(mesh, node_type, nodes, materials, size, vox=(1024, 512, 512), mat=(512, 512, 512),
+             fma_model=None, threads=0, want_conflicts=False):
+    """Returns (output array (flat), Info, conflict mask or None)."""
+    p = _params(node_type, nodes, materials, size, vox, mat, fma_model, threads)
+    info = Info()
+    L = lib()
+    rc = L.orc_plan(ctypes.byref(p), mesh.vertices.ctypes.data, mesh.n_vertices, ctypes.byref(info))
+    if rc:
+        raise RuntimeError(f"orc_plan failed: {rc}")
+    dt = out_dtype(node_type, nodes)
+    out = np.empty(int(info.out_bytes) // np.dtype(dt).itemsize, dtype=dt)
+    conf = np.zeros(out.size if nodes else 0, np.uint8) if want_conflicts else None
+    mats = mesh.materials if mesh.materials is not None else np.zeros(mesh.n_triangles, np.uint8)
+    rc = L.orc_voxelize(ctypes.byref(p), mesh.vertices.ctypes.data, mesh.n_vertices, mesh.indices.ctypes.data,
+                        mesh.n_triangles, mats.ctypes.data, mesh.n_materials, out.ctypes.data, out.nbytes,
+                        conf.ctypes.data if conf is not None else None, ctypes.byref(info))
+    if rc:
+        raise RuntimeError(f"orc_voxelize failed: {rc}")
+    return out, info, conf

@@ -1,0 +1,89 @@
+"""CPU-only checks of the host side: the C ABI library loads and exports
+every symbol include/vxb.h declares, planning (dimensions, padding, x
+rounding) matches the oracle and the reference's golden dims, and argument
+errors surface as the reference's errors.  Nothing here touches a GPU."""
+
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+import cases as C
+import oracle as O
+from voxelizer_b200 import _lib
+from voxelizer_b200.api import Voxelizer
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+INDEX = json.load(open(os.path.join(ROOT, "tests", "golden", "index.json")))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "vxb.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:const char\*|vxb_status)\s+(vxb_\w+)\s*\(", src, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    decl = declared_symbols()
+    assert decl, "no declarations parsed from include/vxb.h"
+    assert sorted(_lib.EXPORTS) == decl
+    for name in decl:
+        assert hasattr(L, name), name
+    assert b"sm_100a" in L.vxb_version()
+
+
+@pytest.mark.parametrize("name", sorted(INDEX))
+def test_plan_matches_golden_dims(name):
+    c = C.BY_NAME[name]
+    m = C.mesh(c["mesh"])
+    with Voxelizer(m.vertices, m.indices, node_type=c["node_type"]) as v:
+        info = v.plan(c["nodes"], c["size"], c["vox"], c["mat"])
+    assert info.dims == tuple(INDEX[name]["dims"])
+    oi = O.plan(m, c["node_type"], c["nodes"], c["size"], c["vox"])
+    assert info.dims == tuple(oi.dims)
+    assert info.voxel_length == oi.voxel_length
+    assert info.x_splits == oi.x_splits
+
+
+def test_mesh_generators_reproduce_golden_inputs():
+    for name, e in INDEX.items():
+        m = C.mesh(C.BY_NAME[name]["mesh"])
+        assert C.mesh_digest(m) == e["mesh_sha256"], name
+
+
+def test_errors_mirror_reference():
+    v0, f0 = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], np.float32), np.array([[0, 1, 2], [0, 1, 3]])
+    # Too many materials for ShortNode (max 7 -> 8 unique), src/host_side.cpp:225-227.
+    with Voxelizer(v0, f0, node_type=_lib.SHORT) as v:
+        with pytest.raises(_lib.VxbError) as e:
+            v.setMaterials(np.zeros(2, np.uint8), 9)
+        assert e.value.status == -1 and "exceeds" in str(e.value)
+        v.setMaterials(np.zeros(2, np.uint8), 8)
+    # FCC nodes refuse plain voxelization and maxDimension sizing.
+    with Voxelizer(v0, f0, node_type=_lib.SHORT_FCC) as v:
+        with pytest.raises(_lib.VxbError) as e:
+            v.voxelizeToRAM(1.0 / 16.0)
+        assert e.value.status == -4
+        with pytest.raises(_lib.VxbError) as e:
+            v.voxelizeToNodesToRAM(32)
+        assert e.value.status == -4
+    # Out-of-range index.
+    with pytest.raises(_lib.VxbError):
+        Voxelizer(v0, np.array([[0, 1, 9]]))
+    # x passes above 1024 voxels are undefined in the reference.
+    with Voxelizer(v0, f0) as v:
+        with pytest.raises(_lib.VxbError):
+            v.plan(1, 2000, (2048, 512, 512))
+
+
+def test_array_dimensions_match_plan():
+    m = C.mesh("ico4")
+    for nt in range(5):
+        with Voxelizer(m.vertices, m.indices, node_type=nt) as v:
+            d = v.getArrayDimensions(1.0 / 100.0, 1024, False)
+            info = v.plan(1, 1.0 / 100.0)
+            assert d == info.dims
+            with pytest.raises(_lib.VxbError):
+                v.getArrayDimensions(1.0 / 100.0, 1024, True)

@@ -1,0 +1,139 @@
+"""Python mirror of the reference's ``vox::Voxelizer<Node>`` interface
+(include/voxelizer.h), over the C ABI of libvxb.so.
+
+Member names, argument meaning and defaults follow the reference:
+``voxelizeToRAM`` returns the plain solid bit array, ``voxelizeToNodesToRAM``
+the node grid; an ``int`` size is a maxDimension, a ``float`` size a
+cubeLength.  Results are numpy arrays with the reference's byte layout
+(``uint32`` words for bit arrays; ``uint8`` / ``uint16`` / ``uint64`` /
+``uint16`` / ``uint32`` per node for ShortNode / LongNode / PartialNode /
+ShortFCCNode / LongFCCNode).  Device variants write into a caller-owned
+device buffer (any object with ``data_ptr()``, e.g. a torch CUDA tensor).
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import LONG, LONG_FCC, NODE_BYTES, PARTIAL, SHORT, SHORT_FCC, check, lib, make_request  # noqa: F401
+
+NODE_DTYPE = {SHORT: np.uint8, LONG: np.uint16, PARTIAL: np.uint64, SHORT_FCC: np.uint16, LONG_FCC: np.uint32}
+DEFAULT_VOX = (1024, 512, 512)
+DEFAULT_MAT = (512, 512, 512)
+
+
+class Voxelizer:
+    """One mesh, one node type (the template argument of the reference)."""
+
+    def __init__(self, vertices, indices, materials=None, n_unique_materials=None, node_type=SHORT, device=0):
+        v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1)
+        i = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1)
+        if v.size % 3 or i.size % 3:
+            raise ValueError("vertices and indices must hold 3 values per vertex / triangle")
+        self.node_type = int(node_type)
+        self.n_vertices = v.size // 3
+        self.n_triangles = i.size // 3
+        h = ctypes.c_void_p()
+        check(lib().vxb_create(ctypes.byref(h), self.node_type, v.ctypes.data, i.ctypes.data, self.n_vertices,
+                               self.n_triangles, int(device)))
+        self._h = h
+        if materials is not None:
+            self.setMaterials(materials, n_unique_materials)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().vxb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- configuration (include/voxelizer.h:862-866) --
+    def setMaterials(self, materials, n_unique_materials):
+        m = np.ascontiguousarray(materials, dtype=np.uint8).reshape(-1)
+        if m.size != self.n_triangles:
+            raise ValueError("one material per triangle is required")
+        if n_unique_materials is None:
+            n_unique_materials = int(m.max()) + 1 if m.size else 0
+        check(lib().vxb_set_materials(self._h, m.ctypes.data, int(n_unique_materials)))
+
+    def setMaterialOutput(self, enable):
+        check(lib().vxb_set_material_output(self._h, int(bool(enable))))
+
+    def verboseOutput(self, enable):
+        check(lib().vxb_verbose_output(self._h, int(bool(enable))))
+
+    # -- planning --
+    def plan(self, nodes, size, voxSplitRes=DEFAULT_VOX, matSplitRes=DEFAULT_MAT):
+        info = _lib.GridInfo()
+        r = make_request(size, voxSplitRes, matSplitRes)
+        check(lib().vxb_plan(self._h, int(bool(nodes)), ctypes.byref(r), ctypes.byref(info)))
+        return info
+
+    def getArrayDimensions(self, size, maxInternalXSize=1024, sliceAlongX=False):
+        d = _lib.Uint3()
+        cube = isinstance(size, float)
+        check(lib().vxb_get_array_dimensions(self._h, int(cube), 0 if cube else int(size), float(size) if cube else 0.0,
+                                             int(maxInternalXSize), int(bool(sliceAlongX)), ctypes.byref(d)))
+        return (int(d.x), int(d.y), int(d.z))
+
+    # -- voxelization to host memory --
+    def _to_host(self, nodes, size, voxSplitRes, matSplitRes, out=None):
+        info = self.plan(nodes, size, voxSplitRes, matSplitRes)
+        dt = NODE_DTYPE[self.node_type] if nodes else np.uint32
+        if out is None:
+            out = np.empty(int(info.count), dtype=dt)
+        elif out.nbytes < info.bytes:
+            raise ValueError("output buffer too small")
+        r = make_request(size, voxSplitRes, matSplitRes)
+        check(lib().vxb_voxelize_to_host(self._h, int(bool(nodes)), ctypes.byref(r), out.ctypes.data, out.nbytes,
+                                         ctypes.byref(info)))
+        return out, info
+
+    def voxelizeToRAM(self, size=256, voxSplitRes=DEFAULT_VOX, out=None):
+        """Plain solid voxelization: uint32 words, shape info.dims (voxels)."""
+        return self._to_host(0, size, voxSplitRes, DEFAULT_MAT, out)
+
+    def voxelizeToNodesToRAM(self, size=256, voxSplitRes=DEFAULT_VOX, matSplitRes=DEFAULT_MAT, out=None):
+        """Node grid with boundary ids (and materials when enabled)."""
+        return self._to_host(1, size, voxSplitRes, matSplitRes, out)
+
+    # -- voxelization into a caller-owned device buffer --
+    def voxelize_device(self, nodes, size, out, voxSplitRes=DEFAULT_VOX, matSplitRes=DEFAULT_MAT, stream=None):
+        """``out`` exposes data_ptr() and nbytes (torch tensor); ``stream``
+        is a raw cudaStream_t handle (int) or None for the default stream.
+        Returns the GridInfo; the work is enqueued on ``stream``."""
+        info = _lib.GridInfo()
+        r = make_request(size, voxSplitRes, matSplitRes)
+        nbytes = out.numel() * out.element_size() if hasattr(out, "element_size") else int(out.nbytes)
+        check(lib().vxb_voxelize_to_device(self._h, int(bool(nodes)), ctypes.byref(r), ctypes.c_void_p(out.data_ptr()),
+                                           nbytes, ctypes.c_void_p(stream or 0), ctypes.byref(info)))
+        return info
+
+    def set_profiling(self, enable):
+        check(lib().vxb_set_profiling(self._h, int(bool(enable))))
+
+    STAGES = ("solid", "surface", "prune", "emit")
+
+    def stage_times(self):
+        """Milliseconds per stage of the last call (-1: stage did not run)."""
+        buf = (ctypes.c_float * 4)()
+        check(lib().vxb_stage_times(self._h, buf, 4))
+        return dict(zip(self.STAGES, [float(x) for x in buf]))
+
+    def last_launch_count(self):
+        n = ctypes.c_uint32()
+        check(lib().vxb_last_launch_count(self._h, ctypes.byref(n)))
+        return int(n.value)

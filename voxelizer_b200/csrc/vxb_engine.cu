@@ -1,0 +1,499 @@
+// Host orchestration and the C ABI (include/vxb.h).
+//
+// One vxb_voxelizer holds a copy of the mesh (as the reference's constructor
+// does, src/host_side.cpp:72-99), its device copy, and a scratch arena that
+// grows on demand and is reused across calls.  A voxelization is a fixed
+// sequence of stream-ordered launches; the only host round trips are the
+// pruning convergence checks (one small read per pruning batch).
+
+#include "vxb.h"
+#include "vxb_kernels.cuh"
+#include "vxb_plan.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_lastError;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_lastError = buf;
+    return code;
+}
+
+#define VXB_CUDA(call)                                                                          \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess) return fail(VXB_ECUDA, "%s @ %s:%d", cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+const uint32_t kNodeBytes[5] = {1, 2, 8, 2, 4};
+const uint32_t kMaxMat[5] = {7, 255, 255, 15, 255};
+
+bool isFcc(int t) { return t == VXB_SHORT_FCC_NODE || t == VXB_LONG_FCC_NODE; }
+
+// A device buffer that only grows.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    ~DevBuf() { if (p) cudaFree(p); }
+    int ensure(size_t bytes) {
+        if (bytes <= cap) return 0;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = bytes + bytes / 8 + 256;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(VXB_ENOMEM, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+        }
+        cap = want;
+        return 0;
+    }
+    template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+}  // namespace
+
+struct vxb_voxelizer {
+    int nodeType = 0;
+    int device = 0;
+    bool materialsOn = false;
+    bool verbose = false;
+    uint32_t nUniqueMaterials = 0;
+    uint32_t nV = 0, nT = 0;
+    std::vector<float> vertices;
+    std::vector<uint32_t> indices;
+    std::vector<uint8_t> materials;
+    double mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
+    bool meshOnDevice = false, matsOnDevice = false;
+    DevBuf dV, dI, dM;
+    // scratch
+    DevBuf counts, offsets, tileSums, small, codes, splitsBuf, matSplitsBuf, laterFlags, outStage;
+    DevBuf fill[4], surf[4], fin;
+    uint32_t launches = 0;
+    // Optional per-stage CUDA-event timing (vxb_set_profiling): stage k is
+    // bracketed by events 2k and 2k+1 on the call's stream.
+    static constexpr int kStages = 4;  // 0 solid, 1 surface, 2 prune, 3 emit
+    bool profiling = false;
+    cudaEvent_t ev[2 * kStages] = {};
+    bool evUsed[kStages] = {};
+    void mark(int stage, bool end, cudaStream_t s) {
+        if (!profiling) return;
+        if (!ev[0])
+            for (auto& e : ev) cudaEventCreate(&e);
+        cudaEventRecord(ev[2 * stage + (end ? 1 : 0)], s);
+        evUsed[stage] = true;
+    }
+    ~vxb_voxelizer() {
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+
+    int plan(int nodes, const vxb_request* r, vxb::Plan& p, vxb_grid_info* info);
+    // Combinations the reference refuses (src/host_side.cpp:568-573,
+    // 1744-1749, 1836-1841, 2280-2285) and missing materials.
+    int validate(int nodes, const vxb_request* r) const {
+        if (!nodes && isFcc(nodeType))
+            return fail(VXB_EUNSUPPORTED, "Please use a standard Node-type when producing a plain voxelization.");
+        if (nodes && isFcc(nodeType) && !r->by_cube_length)
+            return fail(VXB_EUNSUPPORTED,
+                        "FCC Nodes can currently only be defined through the side length of their cubic cells");
+        if (nodes && materialsOn && materials.empty())
+            return fail(VXB_ENOMATERIALS, "material output requested but no materials were set");
+        return 0;
+    }
+    int upload(cudaStream_t s);
+    int run(int nodes, const vxb_request* r, void* dout, uint64_t bytes, cudaStream_t s, vxb_grid_info* info);
+    int solidPass(const vxb::Plan& p, const vxb::PassGeom& g, uint32_t* grid, cudaStream_t s);
+    int surfacePass(const vxb::Plan& p, const vxb::PassGeom& g, int gridType, uint32_t* bits, void* nodes,
+                    cudaStream_t s);
+};
+
+namespace {
+
+vxb::PassGeom makeGeom(const vxb::Plan& p, double sx, double sy, double sz) {
+    vxb::PassGeom g;
+    g.mn[0] = p.mn[0] + sx;
+    g.mn[1] = p.mn[1] + sy;
+    g.mn[2] = p.mn[2] + sz;
+    g.d = p.d;
+    for (int a = 0; a < 3; ++a) g.mnf[a] = (float)g.mn[a];
+    g.df = (float)p.d;
+    g.X = p.res[0];
+    g.resY = p.res[1];
+    g.resZ = p.res[2];
+    g.AY = p.alloc[1];
+    g.AZ = p.alloc[2];
+    g.ipx = p.res[0] / 32;
+    return g;
+}
+
+}  // namespace
+
+int vxb_voxelizer::plan(int nodes, const vxb_request* r, vxb::Plan& p, vxb_grid_info* info) {
+    if (!r) return fail(VXB_EINVAL, "request is NULL");
+    if (nV == 0 || nT == 0) return fail(VXB_EINVAL, "empty mesh");
+    const uint32_t vs[3] = {r->vox_split_res.x, r->vox_split_res.y, r->vox_split_res.z};
+    const uint32_t ms[3] = {r->mat_split_res.x, r->mat_split_res.y, r->mat_split_res.z};
+    int rc = vxb::makePlan(mn, mx, r->by_cube_length, r->max_dimension, r->cube_length, vs, ms, p);
+    if (rc) return fail(VXB_EINVAL, "invalid request (maxDimension >= 2 or cubeLength > 0, split sizes > 0 and an x pass of at most 1024 voxels are required)");
+    const bool fcc = isFcc(nodeType);
+    vxb_grid_info gi;
+    memset(&gi, 0, sizeof(gi));
+    if (nodes) {
+        gi.dim.x = fcc ? 2 * p.alloc[0] : p.alloc[0];
+        gi.dim.y = p.alloc[1];
+        gi.dim.z = fcc ? 2 * p.alloc[2] : p.alloc[2];
+        gi.count = (uint64_t)gi.dim.x * gi.dim.y * gi.dim.z;
+        gi.bytes = gi.count * kNodeBytes[nodeType];
+        // The reference indexes nodes with 32-bit unsigned integers.
+        if (gi.count > 0xFFFFFFFFull) return fail(VXB_EOVERFLOW, "node grid of %llu nodes exceeds 32-bit indexing", (unsigned long long)gi.count);
+    } else {
+        gi.dim.x = p.alloc[0];
+        gi.dim.y = p.alloc[1];
+        gi.dim.z = p.alloc[2];
+        gi.count = (uint64_t)p.alloc[0] * p.alloc[1] * p.alloc[2] / 32;
+        gi.bytes = gi.count * 4;
+        if ((uint64_t)p.alloc[0] * p.alloc[1] * p.alloc[2] > 0xFFFFFFFFull)
+            return fail(VXB_EOVERFLOW, "voxel grid exceeds 32-bit indexing");
+    }
+    gi.voxel_length = p.d;
+    for (int a = 0; a < 3; ++a) { gi.min_vertex[a] = mn[a]; gi.max_vertex[a] = mx[a]; }
+    gi.resolution.x = p.res[0];
+    gi.resolution.y = p.res[1];
+    gi.resolution.z = p.res[2];
+    gi.x_splits = p.xSplits;
+    if (info) *info = gi;
+    return 0;
+}
+
+int vxb_voxelizer::upload(cudaStream_t s) {
+    if (!meshOnDevice) {
+        int rc;
+        if ((rc = dV.ensure(sizeof(float) * 3 * (size_t)nV))) return rc;
+        if ((rc = dI.ensure(sizeof(uint32_t) * 3 * (size_t)nT))) return rc;
+        VXB_CUDA(cudaMemcpyAsync(dV.p, vertices.data(), sizeof(float) * 3 * (size_t)nV, cudaMemcpyHostToDevice, s));
+        VXB_CUDA(cudaMemcpyAsync(dI.p, indices.data(), sizeof(uint32_t) * 3 * (size_t)nT, cudaMemcpyHostToDevice, s));
+        meshOnDevice = true;
+    }
+    if (materialsOn && !matsOnDevice && !materials.empty()) {
+        int rc;
+        if ((rc = dM.ensure(nT))) return rc;
+        VXB_CUDA(cudaMemcpyAsync(dM.p, materials.data(), nT, cudaMemcpyHostToDevice, s));
+        matsOnDevice = true;
+    }
+    return 0;
+}
+
+// Solid voxelization of one (sub-)lattice into `grid` (zeroed here): count
+// candidates, scan, toggle, row fill.
+int vxb_voxelizer::solidPass(const vxb::Plan& p, const vxb::PassGeom& g, uint32_t* grid, cudaStream_t s) {
+    const size_t words = (size_t)g.ipx * g.AY * g.AZ;
+    VXB_CUDA(cudaMemsetAsync(grid, 0, words * 4, s));
+    std::vector<vxb::SplitYZ> sp;
+    for (const auto& z : p.zSplitsExt)
+        for (const auto& y : p.ySplitsExt) sp.push_back(vxb::SplitYZ{y.lo, y.hi, z.lo, z.hi});
+    int rc;
+    if ((rc = splitsBuf.ensure(sp.size() * sizeof(vxb::SplitYZ) + 64))) return rc;
+    VXB_CUDA(cudaMemcpyAsync(splitsBuf.p, sp.data(), sp.size() * sizeof(vxb::SplitYZ), cudaMemcpyHostToDevice, s));
+    uint32_t* cnt = counts.as<uint32_t>();
+    uint32_t* off = offsets.as<uint32_t>();
+    uint32_t* sm = small.as<uint32_t>();
+    vxb::launch_solid_count(dV.as<float>(), dI.as<uint32_t>(), nT, g, splitsBuf.as<vxb::SplitYZ>(), (uint32_t)sp.size(),
+                            cnt, s, &launches);
+    vxb::launch_scan(cnt, off, nT, tileSums.as<uint32_t>(), sm + 0, sm + 1, s, &launches);
+    vxb::launch_solid_toggle(dV.as<float>(), dI.as<uint32_t>(), nT, g, splitsBuf.as<vxb::SplitYZ>(),
+                             (uint32_t)sp.size(), off, sm + 0, grid, s, &launches);
+    vxb::launch_row_fill(grid, g.AY * g.AZ, g.ipx, s, &launches);
+    VXB_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// Surface voxelization of one (sub-)lattice: mark surface bits and seed key
+// slots (mode 0), then merge keys (mode 1).
+int vxb_voxelizer::surfacePass(const vxb::Plan& p, const vxb::PassGeom& g, int gridType, uint32_t* bits, void* nodes,
+                               cudaStream_t s) {
+    const size_t words = (size_t)g.ipx * g.AY * g.AZ;
+    VXB_CUDA(cudaMemsetAsync(bits, 0, words * 4, s));
+    std::vector<vxb::Split3> sp;
+    for (const auto& z : p.zMat)
+        for (const auto& y : p.yMat)
+            for (const auto& x : p.xMat) sp.push_back(vxb::Split3{x.lo, x.hi, y.lo, y.hi, z.lo, z.hi});
+    int rc;
+    if ((rc = matSplitsBuf.ensure(sp.size() * sizeof(vxb::Split3) + 64))) return rc;
+    VXB_CUDA(cudaMemcpyAsync(matSplitsBuf.p, sp.data(), sp.size() * sizeof(vxb::Split3), cudaMemcpyHostToDevice, s));
+    uint32_t* cnt = counts.as<uint32_t>();
+    uint32_t* off = offsets.as<uint32_t>();
+    uint32_t* sm = small.as<uint32_t>();
+    const vxb::Split3* dsp = matSplitsBuf.as<vxb::Split3>();
+    vxb::launch_surface_count(dV.as<float>(), dI.as<uint32_t>(), nT, g, dsp, (uint32_t)sp.size(), codes.as<uint32_t>(),
+                              cnt, s, &launches);
+    vxb::launch_scan(cnt, off, nT, tileSums.as<uint32_t>(), sm + 2, sm + 3, s, &launches);
+    for (int mode = 0; mode < 2; ++mode)
+        vxb::launch_surface_work(nodeType, mode, dV.as<float>(), dI.as<uint32_t>(), dM.as<uint8_t>(), nT, g, gridType,
+                                 dsp, (uint32_t)sp.size(), codes.as<uint32_t>(), off, sm + 2, bits, nodes, s,
+                                 &launches);
+    VXB_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int vxb_voxelizer::run(int nodes, const vxb_request* r, void* dout, uint64_t bytes, cudaStream_t s,
+                       vxb_grid_info* info) {
+    vxb::Plan p;
+    vxb_grid_info gi;
+    int rc = plan(nodes, r, p, &gi);
+    if (rc) return rc;
+    if (info) *info = gi;
+    if (!dout) return fail(VXB_EINVAL, "output buffer is NULL");
+    if (bytes < gi.bytes) return fail(VXB_EINVAL, "output buffer holds %llu bytes, %llu needed",
+                                      (unsigned long long)bytes, (unsigned long long)gi.bytes);
+    if ((rc = validate(nodes, r))) return rc;
+    VXB_CUDA(cudaSetDevice(device));
+    launches = 0;
+    for (bool& u : evUsed) u = false;
+    const bool mats = nodes && materialsOn;
+    if ((rc = upload(s))) return rc;
+    const size_t words = (size_t)(p.res[0] / 32) * p.alloc[1] * p.alloc[2];
+    const size_t gridBytes = ((words + 63) / 64) * 64 * 4;
+    if ((rc = counts.ensure(4 * ((size_t)nT + 1)))) return rc;
+    if ((rc = offsets.ensure(4 * ((size_t)nT + 2)))) return rc;
+    if ((rc = tileSums.ensure(4 * ((size_t)nT / 4096 + 2)))) return rc;
+    if ((rc = small.ensure(64))) return rc;
+    if (mats && (rc = codes.ensure(4 * (size_t)nT))) return rc;
+
+    if (!nodes) {
+        // Plain voxelization: the caller's buffer is the toggle / solid grid.
+        vxb::PassGeom g = makeGeom(p, 0.0, 0.0, 0.0);
+        if ((rc = solidPass(p, g, reinterpret_cast<uint32_t*>(dout), s))) return rc;
+        return 0;
+    }
+    if (!isFcc(nodeType)) {
+        vxb::PassGeom g = makeGeom(p, 0.0, 0.0, 0.0);
+        if ((rc = fill[0].ensure(gridBytes))) return rc;
+        if ((rc = fin.ensure(gridBytes))) return rc;
+        if (mats && (rc = surf[0].ensure(gridBytes))) return rc;
+        mark(0, false, s);
+        if ((rc = solidPass(p, g, fill[0].as<uint32_t>(), s))) return rc;
+        mark(0, true, s);
+        if (mats) {
+            mark(1, false, s);
+            if ((rc = surfacePass(p, g, 1, surf[0].as<uint32_t>(), dout, s))) return rc;
+            mark(1, true, s);
+            mark(2, false, s);
+            vxb::launch_combine(fill[0].as<uint32_t>(), surf[0].as<uint32_t>(), fin.as<uint32_t>(), gridBytes / 4, s,
+                                &launches);
+        } else {
+            mark(2, false, s);
+            VXB_CUDA(cudaMemcpyAsync(fin.p, fill[0].p, gridBytes, cudaMemcpyDeviceToDevice, s));
+        }
+        // Split-ordered pruning (src/host_side.cpp:1183-1206).
+        std::vector<uint8_t> later(p.alloc[1] + p.alloc[2], 0);
+        for (size_t i = 1; i < p.ySplitsAlloc.size(); ++i) later[p.ySplitsAlloc[i].lo - 1] = 1;
+        for (size_t i = 1; i < p.zSplitsAlloc.size(); ++i) later[p.alloc[1] + p.zSplitsAlloc[i].lo - 1] = 1;
+        if ((rc = laterFlags.ensure(later.size() + 64))) return rc;
+        uint32_t* flags = small.as<uint32_t>() + 8;
+        constexpr int kBatch = 4;
+        for (const auto& z : p.zSplitsAlloc)
+            for (const auto& y : p.ySplitsAlloc) {
+                vxb::SplitYZ sp{y.lo, y.hi, z.lo, z.hi};
+                for (int round = 0;; ++round) {
+                    VXB_CUDA(cudaMemsetAsync(flags, 0, kBatch * 4, s));
+                    for (int b = 0; b < kBatch; ++b) vxb::launch_prune(fin.as<uint32_t>(), g, sp, flags + b, s, &launches);
+                    uint32_t h[kBatch];
+                    VXB_CUDA(cudaMemcpyAsync(h, flags, sizeof(h), cudaMemcpyDeviceToHost, s));
+                    VXB_CUDA(cudaStreamSynchronize(s));
+                    if (h[kBatch - 1] == 0) break;
+                    if (round > 1000000) return fail(VXB_ETIMEDOUT, "pruning did not converge");
+                }
+            }
+        VXB_CUDA(cudaMemcpyAsync(laterFlags.p, later.data(), later.size(), cudaMemcpyHostToDevice, s));
+        mark(2, true, s);
+        const uint8_t* yl = laterFlags.as<uint8_t>();
+        mark(3, false, s);
+        vxb::launch_emit_cartesian(nodeType, fin.as<uint32_t>(), fill[0].as<uint32_t>(),
+                                   mats ? surf[0].as<uint32_t>() : nullptr, g, yl, yl + p.alloc[1], dout, mats ? 1 : 0,
+                                   s, &launches);
+        mark(3, true, s);
+        VXB_CUDA(cudaGetLastError());
+        return 0;
+    }
+    // FCC: four shifted sub-lattices (src/host_side.cpp:1432-1484, 1525-1593).
+    const double h = p.d / 2.0;
+    const double shifts[4][3] = {{0.0, 0.0, 0.0}, {h, h, 0.0}, {0.0, h, h}, {h, 0.0, h}};
+    const uint32_t* fp[4];
+    const uint32_t* sp4[4];
+    for (int gt = 0; gt < 4; ++gt) {
+        if ((rc = fill[gt].ensure(gridBytes))) return rc;
+        if (mats && (rc = surf[gt].ensure(gridBytes))) return rc;
+    }
+    for (int gt = 0; gt < 4; ++gt) {
+        vxb::PassGeom g = makeGeom(p, shifts[gt][0], shifts[gt][1], shifts[gt][2]);
+        if ((rc = solidPass(p, g, fill[gt].as<uint32_t>(), s))) return rc;
+        fp[gt] = fill[gt].as<uint32_t>();
+        sp4[gt] = nullptr;
+        if (mats) {
+            if ((rc = surfacePass(p, g, gt + 1, surf[gt].as<uint32_t>(), dout, s))) return rc;
+            sp4[gt] = surf[gt].as<uint32_t>();
+        }
+    }
+    vxb::PassGeom g = makeGeom(p, 0.0, 0.0, 0.0);
+    mark(3, false, s);
+    vxb::launch_emit_fcc(nodeType, fp, sp4, g, dout, mats ? 1 : 0, s, &launches);
+    mark(3, true, s);
+    VXB_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+
+extern "C" {
+
+const char* vxb_last_error(void) { return g_lastError.c_str(); }
+const char* vxb_version(void) { return "vxb 0.1 (sm_100a)"; }
+
+vxb_status vxb_create(vxb_voxelizer** out, int node_type, const float* vertices, const uint32_t* indices,
+                      uint32_t n_vertices, uint32_t n_triangles, int device) {
+    if (!out) return fail(VXB_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (node_type < 0 || node_type > 4) return fail(VXB_EINVAL, "unknown node type %d", node_type);
+    if ((!vertices && n_vertices) || (!indices && n_triangles)) return fail(VXB_EINVAL, "NULL mesh arrays");
+    for (uint64_t i = 0; i < 3ull * n_triangles; ++i)
+        if (indices[i] >= n_vertices) return fail(VXB_EINVAL, "index %u of triangle %llu is out of range", indices[i], (unsigned long long)(i / 3));
+    vxb_voxelizer* v = new (std::nothrow) vxb_voxelizer();
+    if (!v) return fail(VXB_ENOMEM, "out of host memory");
+    v->nodeType = node_type;
+    v->device = device;
+    v->nV = n_vertices;
+    v->nT = n_triangles;
+    v->vertices.assign(vertices, vertices + 3 * (size_t)n_vertices);
+    v->indices.assign(indices, indices + 3 * (size_t)n_triangles);
+    if (n_vertices) vxb::boundingBox(vertices, n_vertices, v->mn, v->mx);
+    *out = v;
+    return VXB_OK;
+}
+
+vxb_status vxb_destroy(vxb_voxelizer* v) {
+    delete v;
+    return VXB_OK;
+}
+
+vxb_status vxb_set_materials(vxb_voxelizer* v, const uint8_t* materials, uint32_t n_unique_materials) {
+    if (!v) return fail(VXB_EINVAL, "voxelizer is NULL");
+    if (!materials) return fail(VXB_EINVAL, "No valid materials provided (Received null pointer) @ setMaterials.");
+    if (n_unique_materials > kMaxMat[v->nodeType] + 1)
+        return fail(VXB_EINVAL, "The number of unique materials exceeds the capabilities of the node type @ setMaterials.");
+    v->nUniqueMaterials = n_unique_materials;
+    v->materials.assign(materials, materials + v->nT);
+    v->matsOnDevice = false;
+    v->materialsOn = true;
+    return VXB_OK;
+}
+
+vxb_status vxb_set_material_output(vxb_voxelizer* v, int enable) {
+    if (!v) return fail(VXB_EINVAL, "voxelizer is NULL");
+    v->materialsOn = enable != 0;
+    return VXB_OK;
+}
+
+vxb_status vxb_verbose_output(vxb_voxelizer* v, int enable) {
+    if (!v) return fail(VXB_EINVAL, "voxelizer is NULL");
+    v->verbose = enable != 0;
+    return VXB_OK;
+}
+
+vxb_status vxb_plan(vxb_voxelizer* v, int nodes, const vxb_request* req, vxb_grid_info* info) {
+    if (!v) return fail(VXB_EINVAL, "voxelizer is NULL");
+    vxb::Plan p;
+    return v->plan(nodes, req, p, info);
+}
+
+vxb_status vxb_get_array_dimensions(vxb_voxelizer* v, int by_cube_length, uint32_t max_dimension, double cube_length,
+                                    uint32_t max_internal_x, int slice_along_x, vxb_uint3* dims) {
+    if (!v || !dims) return fail(VXB_EINVAL, "NULL argument");
+    if (slice_along_x) return fail(VXB_EUNSUPPORTED, "slicing along x is not part of this library");
+    vxb_request r;
+    r.by_cube_length = by_cube_length;
+    r.max_dimension = max_dimension;
+    r.cube_length = cube_length;
+    r.vox_split_res = vxb_uint3{max_internal_x, 512, 512};
+    r.mat_split_res = vxb_uint3{512, 512, 512};
+    vxb_grid_info gi;
+    vxb::Plan p;
+    int rc = v->plan(1, &r, p, &gi);
+    if (rc == VXB_EOVERFLOW) rc = 0;
+    if (rc) return rc;
+    dims->x = isFcc(v->nodeType) ? 2 * p.alloc[0] : p.alloc[0];
+    dims->y = p.alloc[1];
+    dims->z = isFcc(v->nodeType) ? 2 * p.alloc[2] : p.alloc[2];
+    return VXB_OK;
+}
+
+vxb_status vxb_voxelize_to_device(vxb_voxelizer* v, int nodes, const vxb_request* req, void* dev_out,
+                                  uint64_t dev_bytes, void* stream, vxb_grid_info* info) {
+    if (!v) return fail(VXB_EINVAL, "voxelizer is NULL");
+    return v->run(nodes, req, dev_out, dev_bytes, reinterpret_cast<cudaStream_t>(stream), info);
+}
+
+vxb_status vxb_voxelize_to_host(vxb_voxelizer* v, int nodes, const vxb_request* req, void* host_out,
+                                uint64_t host_bytes, vxb_grid_info* info) {
+    if (!v) return fail(VXB_EINVAL, "voxelizer is NULL");
+    vxb_grid_info gi;
+    vxb::Plan p;
+    int rc = v->plan(nodes, req, p, &gi);
+    if (rc) return rc;
+    if (info) *info = gi;
+    if ((rc = v->validate(nodes, req))) return rc;
+    if (!host_out) return fail(VXB_EINVAL, "output buffer is NULL");
+    if (host_bytes < gi.bytes) return fail(VXB_EINVAL, "output buffer too small");
+    VXB_CUDA(cudaSetDevice(v->device));
+    if ((rc = v->outStage.ensure(gi.bytes))) return rc;
+    rc = v->run(nodes, req, v->outStage.p, gi.bytes, 0, info);
+    if (rc == 0) {
+        cudaError_t e = cudaMemcpy(host_out, v->outStage.p, gi.bytes, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = fail(VXB_ECUDA, "%s", cudaGetErrorString(e));
+    }
+    return rc;
+}
+
+vxb_status vxb_set_profiling(vxb_voxelizer* v, int enable) {
+    if (!v) return fail(VXB_EINVAL, "voxelizer is NULL");
+    v->profiling = enable != 0;
+    return VXB_OK;
+}
+
+vxb_status vxb_stage_times(vxb_voxelizer* v, float* ms, uint32_t n) {
+    if (!v || !ms) return fail(VXB_EINVAL, "NULL argument");
+    for (uint32_t k = 0; k < n && k < (uint32_t)vxb_voxelizer::kStages; ++k) {
+        ms[k] = -1.0f;
+        if (!v->profiling || !v->evUsed[k]) continue;
+        cudaError_t e = cudaEventSynchronize(v->ev[2 * k + 1]);
+        if (e != cudaSuccess) return fail(VXB_ECUDA, "%s", cudaGetErrorString(e));
+        float t = 0.0f;
+        if (cudaEventElapsedTime(&t, v->ev[2 * k], v->ev[2 * k + 1]) == cudaSuccess) ms[k] = t;
+    }
+    return VXB_OK;
+}
+
+vxb_status vxb_last_launch_count(vxb_voxelizer* v, uint32_t* launches) {
+    if (!v || !launches) return fail(VXB_EINVAL, "NULL argument");
+    *launches = v->launches;
+    return VXB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,59 @@
+// Kernel declarations and the plain structs the host engine passes to them.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vxb {
+
+// Geometry of one solid / surface pass.  For FCC lattices each of the four
+// sub-lattices is one pass with its own shifted minimum corner.
+struct PassGeom {
+    double mn[3];        // minimum corner (FP64, as the reference's extMinVertex)
+    double d;            // voxel length
+    float mnf[3];        // float(mn) for the FP32 surface path
+    float df;            // float(d)
+    uint32_t X;          // voxels along x (padded and rounded to 32 * xSplits)
+    uint32_t resY, resZ; // voxels along y / z before the 1-voxel padding
+    uint32_t AY, AZ;     // allocated rows: resY + 2, resZ + 2
+    uint32_t ipx;        // 32-bit words per row: X / 32
+};
+
+struct SplitYZ { uint32_t y0, y1, z0, z1; };
+struct Split3 { uint32_t x0, x1, y0, y1, z0, z1; };
+
+// Work-list scan: exclusive offsets (n + 1 entries) and the grand total.
+void launch_scan(const uint32_t* in, uint32_t* offsets, uint32_t n, uint32_t* blockSums, uint32_t* total,
+                 uint32_t* overflow, cudaStream_t s, uint32_t* launches);
+
+// ---- Solid (parity) voxelization: src/voxelizer.cu:840-1617 ----
+void launch_solid_count(const float* V, const uint32_t* I, uint32_t nT, PassGeom g, const SplitYZ* splits,
+                        uint32_t nSplits, uint32_t* counts, cudaStream_t s, uint32_t* launches);
+void launch_solid_toggle(const float* V, const uint32_t* I, uint32_t nT, PassGeom g, const SplitYZ* splits,
+                         uint32_t nSplits, const uint32_t* offsets, const uint32_t* total, uint32_t* toggles,
+                         cudaStream_t s, uint32_t* launches);
+void launch_row_fill(uint32_t* words, uint32_t rows, uint32_t ipx, cudaStream_t s, uint32_t* launches);
+
+// ---- Surface voxelization: src/voxelizer.cu:2358-2989, 3040-4201 ----
+void launch_surface_count(const float* V, const uint32_t* I, uint32_t nT, PassGeom g, const Split3* splits,
+                          uint32_t nSplits, uint32_t* codes, uint32_t* counts, cudaStream_t s, uint32_t* launches);
+// mode 0: mark surface bits and seed each node's key slot; mode 1: max-merge keys.
+void launch_surface_work(int nodeKind, int mode, const float* V, const uint32_t* I, const uint8_t* M,
+                         uint32_t nT, PassGeom g, int gridType, const Split3* splits, uint32_t nSplits,
+                         const uint32_t* codes, const uint32_t* offsets, const uint32_t* total, uint32_t* surfBits,
+                         void* nodes, cudaStream_t s, uint32_t* launches);
+
+// ---- Node classification: src/voxelizer.cu:1626-2048 ----
+void launch_combine(const uint32_t* a, const uint32_t* b, uint32_t* out, uint64_t n, cudaStream_t s,
+                    uint32_t* launches);
+void launch_prune(uint32_t* solid, PassGeom g, SplitYZ split, uint32_t* changed, cudaStream_t s,
+                  uint32_t* launches);
+// yLater[y] / zLater[z] are 1 where row y + 1 / plane z + 1 starts a later
+// pruning subspace than row y / plane z.
+void launch_emit_cartesian(int nodeKind, const uint32_t* finalSolid, const uint32_t* fill, const uint32_t* surf,
+                           PassGeom g, const uint8_t* yLater, const uint8_t* zLater, void* nodes, int materials,
+                           cudaStream_t s, uint32_t* launches);
+void launch_emit_fcc(int nodeKind, const uint32_t* const* fill, const uint32_t* const* surf, PassGeom g, void* nodes,
+                     int materials, cudaStream_t s, uint32_t* launches);
+
+}  // namespace vxb
