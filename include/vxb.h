@@ -127,7 +127,7 @@ vxb_status vxb_last_launch_count(vxb_voxelizer* v, uint32_t* launches);
 /* Stage timing with CUDA events on the call's stream (off by default; no
  * reference counterpart, the reference only prints clock() stamps in verbose
  * mode).  Stages: 0 solid voxelization, 1 surface voxelization, 2 pruning,
- * 3 node emission.  vxb_stage_times waits for the last call and writes the
+ * 3 node emission, 4 material merge.  vxb_stage_times waits for the last call and writes the
  * milliseconds of up to n stages (-1 for a stage that did not run). */
 vxb_status vxb_set_profiling(vxb_voxelizer* v, int enable);
 vxb_status vxb_stage_times(vxb_voxelizer* v, float* ms, uint32_t n);

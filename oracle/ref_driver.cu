@@ -228,6 +228,10 @@ struct Runner {
 
     int runImpl(const float* verts, uint nV_, const uint* idx, uint nT_, const uchar* mats, uint nMat,
                 void* out, uint64_t outBytes, uint32_t* dimsOut, double* ms) {
+        // checkCudaErrors (include/common.h:206-215) peeks at the runtime's
+        // last error without clearing it; clear any error left by an
+        // earlier call so it is not reported again here.
+        cudaGetLastError();
         nV = nV_; nT = nT_;
         double3 mn, mx;
         boundingBox(verts, nV, mn, mx);

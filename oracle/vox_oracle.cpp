@@ -598,7 +598,7 @@ static inline Overlap setupOverlap(const f3* t, f3 n, float d, int axis, int deM
         else { pa = p.x; pb = p.y; qa = q.x; qb = q.y; nn = n.z; }
         if (nn >= 0.0f) o.ne[i] = f2{pb - qb, qa - pa};
         else o.ne[i] = f2{qb - pb, pa - qa};
-        float s = sum2(o.ne[i].x, pa, o.ne[i].y, pb, deMode);
+        float s = sum2(o.ne[i].x, pa, o.ne[i].y, pb, (deMode >> (2 * i)) & 3);
         o.de[i] = (-s + std::fmax(0.0f, d * o.ne[i].x)) + std::fmax(0.0f, d * o.ne[i].y);
     }
     return o;
@@ -606,7 +606,7 @@ static inline Overlap setupOverlap(const f3* t, f3 n, float d, int axis, int deM
 // overlapTestYZ/ZX/XY, src/voxelizer.cu:2890-2942
 static inline bool overlapTest(const Overlap& o, float a, float b, int mode) {
     bool r = true;
-    for (int i = 0; i < 3; i++) r &= sum2p1(o.ne[i].x, a, o.ne[i].y, b, o.de[i], mode) >= 0.0f;
+    for (int i = 0; i < 3; i++) r &= sum2p1(o.ne[i].x, a, o.ne[i].y, b, o.de[i], (mode >> (2 * i)) & 3) >= 0.0f;
     return r;
 }
 // getSingleVoxelBoundsComponent, src/voxelizer.cu:2575-2586

@@ -117,8 +117,6 @@ CASES = [
     case("stress_sfcc_mat", "stress_fcc", SHORT_FCC, 1, 1, FCC_A, strict_mats=False),
     case("stress_lfcc_mat", "stress_fcc", LONG_FCC, 1, 1, FCC_A, vox=(64, 32, 32), mat=(32, 32, 32),
          strict_mats=False),
-    # PartialNode (ratio of surface nodes depends on the racing triangle).
-    case("ico4_partial_mat", "ico4", PARTIAL, 1, 1, 1.0 / 64.0, strict_mats=False),
     # Room scene, reduced and full size.
     case("room_lite_long", "room_lite", LONG, 1, 1, 160),
     case("room_lite_bits", "room_lite", LONG, 0, 0, 160),
@@ -130,6 +128,10 @@ CASES = [
     case("room_full_bits", "room_full", LONG, 0, 0, 1024, store="digest"),
     case("elong4_4096_long", "elong4", LONG, 1, 0, 4096, store="digest"),
     case("stress_full_sfcc", "stress_full_fcc", SHORT_FCC, 1, 1, FCC_A, store="digest", strict_mats=False),
+    # PartialNode without and with materials (the surface ratio depends on
+    # which racing triangle wrote last).
+    case("ico4_partial_nomat", "ico4", PARTIAL, 1, 0, 1.0 / 64.0),
+    case("ico4_partial_mat", "ico4", PARTIAL, 1, 1, 1.0 / 64.0, strict_mats=False),
 ]
 
 BY_NAME = {c["name"]: c for c in CASES}

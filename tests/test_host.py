@@ -34,7 +34,10 @@ def test_library_exports_every_declared_symbol():
     assert b"sm_100a" in L.vxb_version()
 
 
-@pytest.mark.parametrize("name", sorted(INDEX))
+RAN = sorted(n for n, e in INDEX.items() if "ref_error" not in e)
+
+
+@pytest.mark.parametrize("name", RAN)
 def test_plan_matches_golden_dims(name):
     c = C.BY_NAME[name]
     m = C.mesh(c["mesh"])
@@ -48,7 +51,8 @@ def test_plan_matches_golden_dims(name):
 
 
 def test_mesh_generators_reproduce_golden_inputs():
-    for name, e in INDEX.items():
+    for name in RAN:
+        e = INDEX[name]
         m = C.mesh(C.BY_NAME[name]["mesh"])
         assert C.mesh_digest(m) == e["mesh_sha256"], name
 

@@ -125,12 +125,12 @@ class Voxelizer:
     def set_profiling(self, enable):
         check(lib().vxb_set_profiling(self._h, int(bool(enable))))
 
-    STAGES = ("solid", "surface", "prune", "emit")
+    STAGES = ("solid", "surface", "prune", "emit", "merge")
 
     def stage_times(self):
         """Milliseconds per stage of the last call (-1: stage did not run)."""
-        buf = (ctypes.c_float * 4)()
-        check(lib().vxb_stage_times(self._h, buf, 4))
+        buf = (ctypes.c_float * len(self.STAGES))()
+        check(lib().vxb_stage_times(self._h, buf, len(self.STAGES)))
         return dict(zip(self.STAGES, [float(x) for x in buf]))
 
     def last_launch_count(self):

@@ -1,0 +1,38 @@
+// Helpers shared by the kernel files.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vxb {
+namespace detail {
+
+struct D3 { double x, y, z; };
+struct F3 { float x, y, z; };
+
+__device__ __forceinline__ uint32_t laneMaskLt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Largest t with offsets[t] <= item (offsets: n + 1 non-decreasing entries).
+__device__ __forceinline__ uint32_t findOwner(const uint32_t* __restrict__ offsets, uint32_t n, uint32_t item) {
+    uint32_t lo = 0, hi = n;  // invariant: offsets[lo] <= item < offsets[hi]
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(offsets + mid) <= item) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Blocks for `work` items at `threads` per block, capped (grid-stride loops).
+inline uint32_t gridFor(uint64_t work, uint32_t threads, uint32_t cap = 148u * 32u) {
+    uint64_t b = (work + threads - 1) / threads;
+    if (b == 0) b = 1;
+    return (uint32_t)(b < cap ? b : cap);
+}
+
+}  // namespace detail
+}  // namespace vxb

@@ -24,6 +24,8 @@ namespace vxb {
 //   a*b - c*d            CR*          0: no fma  1: fma(a,b,-(c*d)) 2: fma(-c,d,a*b)
 //   a*b + c*d + e*f      B_*, TN, DT_* 0: no fma 1: fma(e,f,fma(a,b,c*d)) 2: fma(e,f,fma(c,d,a*b))
 //                                      3: fma(a,b,c*d)+e*f  4: fma(e,f,a*b+c*d)  5: fma(c,d,a*b)+e*f
+// The DE_* and OT_* sites hold one mode per triangle edge: bits 2i..2i+1
+// for edge i.
 namespace site {
 #include "vxb_sites.inc"
 }

@@ -1,10 +1,12 @@
 // Host orchestration and the C ABI (include/vxb.h).
 //
 // One vxb_voxelizer holds a copy of the mesh (as the reference's constructor
-// does, src/host_side.cpp:72-99), its device copy, and a scratch arena that
-// grows on demand and is reused across calls.  A voxelization is a fixed
-// sequence of stream-ordered launches; the only host round trips are the
-// pruning convergence checks (one small read per pruning batch).
+// does, src/host_side.cpp:72-99), its device copy, and scratch buffers that
+// grow on demand and are reused across calls.  A voxelization is a fixed
+// sequence of stream-ordered launches; the only host round trip is one
+// small read after the pruning passes are queued (convergence flags, hit
+// list length and surface voxel count), repeated only when a pruning
+// subspace needs more passes.
 
 #include "vxb.h"
 #include "vxb_kernels.cuh"
@@ -12,6 +14,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -67,6 +70,10 @@ struct DevBuf {
     template <class T> T* as() const { return reinterpret_cast<T*>(p); }
 };
 
+// Slots of the small device status buffer.
+enum : int { kSolidTotal = 0, kSolidOverflow = 1, kSurfTotal = 2, kSurfOverflow = 3, kHitCount = 4,
+             kSurfaceVoxels = 5, kFlags = 8 };
+
 }  // namespace
 
 struct vxb_voxelizer {
@@ -84,11 +91,11 @@ struct vxb_voxelizer {
     DevBuf dV, dI, dM;
     // scratch
     DevBuf counts, offsets, tileSums, small, codes, splitsBuf, matSplitsBuf, laterFlags, outStage;
-    DevBuf fill[4], surf[4], fin;
+    DevBuf fill[4], surfAll, fin, ranks, rankTiles, hitList, keys;
     uint32_t launches = 0;
     // Optional per-stage CUDA-event timing (vxb_set_profiling): stage k is
     // bracketed by events 2k and 2k+1 on the call's stream.
-    static constexpr int kStages = 4;  // 0 solid, 1 surface, 2 prune, 3 emit
+    static constexpr int kStages = 5;  // 0 solid, 1 surface, 2 prune, 3 emit, 4 material merge
     bool profiling = false;
     cudaEvent_t ev[2 * kStages] = {};
     bool evUsed[kStages] = {};
@@ -120,8 +127,11 @@ struct vxb_voxelizer {
     int upload(cudaStream_t s);
     int run(int nodes, const vxb_request* r, void* dout, uint64_t bytes, cudaStream_t s, vxb_grid_info* info);
     int solidPass(const vxb::Plan& p, const vxb::PassGeom& g, uint32_t* grid, cudaStream_t s);
-    int surfacePass(const vxb::Plan& p, const vxb::PassGeom& g, int gridType, uint32_t* bits, void* nodes,
+    int surfacePass(const vxb::Plan& p, const vxb::PassGeom& g, int lattice, size_t gridWords, int mode,
                     cudaStream_t s);
+    int resolveKeys(const vxb::Plan& p, int lattices, size_t gridWords, uint32_t hitCount, uint32_t surfaceVoxels,
+                    cudaStream_t s);
+    uint32_t listCap = 0;
 };
 
 namespace {
@@ -141,6 +151,13 @@ vxb::PassGeom makeGeom(const vxb::Plan& p, double sx, double sy, double sz) {
     g.AZ = p.alloc[2];
     g.ipx = p.res[0] / 32;
     return g;
+}
+
+// Shifts of the four FCC sub-lattices (src/host_side.cpp:1438-1462).
+void latticeShift(const vxb::Plan& p, int lattice, double* sh) {
+    const double h = p.d / 2.0;
+    const double s[4][3] = {{0.0, 0.0, 0.0}, {h, h, 0.0}, {0.0, h, h}, {h, 0.0, h}};
+    for (int a = 0; a < 3; ++a) sh[a] = s[lattice][a];
 }
 
 }  // namespace
@@ -216,20 +233,22 @@ int vxb_voxelizer::solidPass(const vxb::Plan& p, const vxb::PassGeom& g, uint32_
     uint32_t* sm = small.as<uint32_t>();
     vxb::launch_solid_count(dV.as<float>(), dI.as<uint32_t>(), nT, g, splitsBuf.as<vxb::SplitYZ>(), (uint32_t)sp.size(),
                             cnt, s, &launches);
-    vxb::launch_scan(cnt, off, nT, tileSums.as<uint32_t>(), sm + 0, sm + 1, s, &launches);
+    vxb::launch_scan(cnt, off, nT, tileSums.as<uint32_t>(), sm + kSolidTotal, sm + kSolidOverflow, s, &launches);
     vxb::launch_solid_toggle(dV.as<float>(), dI.as<uint32_t>(), nT, g, splitsBuf.as<vxb::SplitYZ>(),
-                             (uint32_t)sp.size(), off, sm + 0, grid, s, &launches);
+                             (uint32_t)sp.size(), off, sm + kSolidTotal, grid, s, &launches);
     vxb::launch_row_fill(grid, g.AY * g.AZ, g.ipx, s, &launches);
     VXB_CUDA(cudaGetLastError());
     return 0;
 }
 
-// Surface voxelization of one (sub-)lattice: mark surface bits and seed key
-// slots (mode 0), then merge keys (mode 1).
-int vxb_voxelizer::surfacePass(const vxb::Plan& p, const vxb::PassGeom& g, int gridType, uint32_t* bits, void* nodes,
+// Surface voxelization of one (sub-)lattice.  mode 0: set its surface bits
+// (zeroed here) and append hits to the hit list; mode 1: merge every hit's
+// key at its rank (the fallback when the list overflowed, and the path for
+// 64-bit PartialNode keys).
+int vxb_voxelizer::surfacePass(const vxb::Plan& p, const vxb::PassGeom& g, int lattice, size_t gridWords, int mode,
                                cudaStream_t s) {
-    const size_t words = (size_t)g.ipx * g.AY * g.AZ;
-    VXB_CUDA(cudaMemsetAsync(bits, 0, words * 4, s));
+    uint32_t* bits = surfAll.as<uint32_t>() + lattice * gridWords;
+    if (mode == 0) VXB_CUDA(cudaMemsetAsync(bits, 0, gridWords * 4, s));
     std::vector<vxb::Split3> sp;
     for (const auto& z : p.zMat)
         for (const auto& y : p.yMat)
@@ -243,12 +262,36 @@ int vxb_voxelizer::surfacePass(const vxb::Plan& p, const vxb::PassGeom& g, int g
     const vxb::Split3* dsp = matSplitsBuf.as<vxb::Split3>();
     vxb::launch_surface_count(dV.as<float>(), dI.as<uint32_t>(), nT, g, dsp, (uint32_t)sp.size(), codes.as<uint32_t>(),
                               cnt, s, &launches);
-    vxb::launch_scan(cnt, off, nT, tileSums.as<uint32_t>(), sm + 2, sm + 3, s, &launches);
-    for (int mode = 0; mode < 2; ++mode)
-        vxb::launch_surface_work(nodeType, mode, dV.as<float>(), dI.as<uint32_t>(), dM.as<uint8_t>(), nT, g, gridType,
-                                 dsp, (uint32_t)sp.size(), codes.as<uint32_t>(), off, sm + 2, bits, nodes, s,
-                                 &launches);
+    vxb::launch_scan(cnt, off, nT, tileSums.as<uint32_t>(), sm + kSurfTotal, sm + kSurfOverflow, s, &launches);
+    vxb::launch_surface_work(mode, nodeType == VXB_PARTIAL_NODE ? 1 : 0, dV.as<float>(), dI.as<uint32_t>(),
+                             dM.as<uint8_t>(), nT, g, dsp, (uint32_t)sp.size(), codes.as<uint32_t>(), off,
+                             sm + kSurfTotal, bits, (uint64_t)lattice * gridWords * 32, ranks.as<uint32_t>(), keys.p,
+                             hitList.as<unsigned long long>(), sm + kHitCount, listCap, s, &launches);
     VXB_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// Material keys by surface rank: zero them, then merge the hit list, or
+// re-run the surface passes in mode 1 when the list overflowed (or for
+// 64-bit keys).  hitCount / surfaceVoxels were read back by the caller.
+int vxb_voxelizer::resolveKeys(const vxb::Plan& p, int lattices, size_t gridWords, uint32_t hitCount,
+                               uint32_t surfaceVoxels, cudaStream_t s) {
+    const bool wide = nodeType == VXB_PARTIAL_NODE;
+    int rc;
+    if ((rc = keys.ensure((size_t)(surfaceVoxels + 1) * (wide ? 8 : 4)))) return rc;
+    uint32_t* sm = small.as<uint32_t>();
+    vxb::launch_surface_keys_zero(keys.p, sm + kSurfaceVoxels, wide ? 1 : 0, s, &launches);
+    if (!wide && hitCount <= listCap) {
+        vxb::launch_surface_merge(hitList.as<unsigned long long>(), sm + kHitCount, listCap, surfAll.as<uint32_t>(),
+                                  ranks.as<uint32_t>(), keys.as<uint32_t>(), s, &launches);
+        return 0;
+    }
+    for (int lt = 0; lt < lattices; ++lt) {
+        double sh[3];
+        latticeShift(p, lt, sh);
+        vxb::PassGeom g = makeGeom(p, sh[0], sh[1], sh[2]);
+        if ((rc = surfacePass(p, g, lt, gridWords, 1, s))) return rc;
+    }
     return 0;
 }
 
@@ -269,12 +312,29 @@ int vxb_voxelizer::run(int nodes, const vxb_request* r, void* dout, uint64_t byt
     const bool mats = nodes && materialsOn;
     if ((rc = upload(s))) return rc;
     const size_t words = (size_t)(p.res[0] / 32) * p.alloc[1] * p.alloc[2];
-    const size_t gridBytes = ((words + 63) / 64) * 64 * 4;
+    const size_t gridWords = ((words + 63) / 64) * 64;
+    const size_t gridBytes = gridWords * 4;
     if ((rc = counts.ensure(4 * ((size_t)nT + 1)))) return rc;
     if ((rc = offsets.ensure(4 * ((size_t)nT + 2)))) return rc;
     if ((rc = tileSums.ensure(4 * ((size_t)nT / 4096 + 2)))) return rc;
-    if ((rc = small.ensure(64))) return rc;
-    if (mats && (rc = codes.ensure(4 * (size_t)nT))) return rc;
+    // Status slots plus three pruning flags per pruning subspace; sized here
+    // so that it never moves while kernels of this call use it.
+    if ((rc = small.ensure(4 * (kFlags + 3 * p.ySplitsAlloc.size() * p.zSplitsAlloc.size()) + 256))) return rc;
+    const int lattices = isFcc(nodeType) ? 4 : 1;
+    if (mats) {
+        if ((rc = codes.ensure(4 * (size_t)nT))) return rc;
+        if ((rc = surfAll.ensure(gridBytes * lattices))) return rc;
+        if ((rc = ranks.ensure(gridBytes * lattices))) return rc;
+        if ((rc = rankTiles.ensure(4 * (gridWords * lattices / 2048 + 2)))) return rc;
+        // Hit list: 8-byte entries (bit position << 24 | key); PartialNode
+        // keys are 64-bit and always take the second traversal.
+        const uint64_t want = nodeType == VXB_PARTIAL_NODE
+                                  ? 0
+                                  : std::min<uint64_t>(96ull << 20, std::max<uint64_t>(8ull << 20, gi.count / 12));
+        listCap = (uint32_t)want;
+        if (want && (rc = hitList.ensure(want * 8))) return rc;
+        VXB_CUDA(cudaMemsetAsync(small.as<uint32_t>() + kHitCount, 0, 4, s));
+    }
 
     if (!nodes) {
         // Plain voxelization: the caller's buffer is the toggle / solid grid.
@@ -282,78 +342,108 @@ int vxb_voxelizer::run(int nodes, const vxb_request* r, void* dout, uint64_t byt
         if ((rc = solidPass(p, g, reinterpret_cast<uint32_t*>(dout), s))) return rc;
         return 0;
     }
+    uint32_t* sm = small.as<uint32_t>();
     if (!isFcc(nodeType)) {
         vxb::PassGeom g = makeGeom(p, 0.0, 0.0, 0.0);
         if ((rc = fill[0].ensure(gridBytes))) return rc;
         if ((rc = fin.ensure(gridBytes))) return rc;
-        if (mats && (rc = surf[0].ensure(gridBytes))) return rc;
         mark(0, false, s);
         if ((rc = solidPass(p, g, fill[0].as<uint32_t>(), s))) return rc;
         mark(0, true, s);
+        const uint32_t* surfp = mats ? surfAll.as<uint32_t>() : nullptr;
         if (mats) {
             mark(1, false, s);
-            if ((rc = surfacePass(p, g, 1, surf[0].as<uint32_t>(), dout, s))) return rc;
+            if ((rc = surfacePass(p, g, 0, gridWords, 0, s))) return rc;
+            vxb::launch_surface_rank(surfAll.as<uint32_t>(), gridWords, ranks.as<uint32_t>(), rankTiles.as<uint32_t>(),
+                                     sm + kSurfaceVoxels, s, &launches);
             mark(1, true, s);
             mark(2, false, s);
-            vxb::launch_combine(fill[0].as<uint32_t>(), surf[0].as<uint32_t>(), fin.as<uint32_t>(), gridBytes / 4, s,
-                                &launches);
+            vxb::launch_combine(fill[0].as<uint32_t>(), surfp, fin.as<uint32_t>(), gridWords, s, &launches);
         } else {
             mark(2, false, s);
             VXB_CUDA(cudaMemcpyAsync(fin.p, fill[0].p, gridBytes, cudaMemcpyDeviceToDevice, s));
         }
-        // Split-ordered pruning (src/host_side.cpp:1183-1206).
+        // Split-ordered pruning (src/host_side.cpp:1183-1206).  Passes for
+        // every subspace are queued in order with one convergence check at
+        // the end: when each subspace's last queued pass changed nothing,
+        // every subspace converged before the next one started, exactly as
+        // in the reference.  Otherwise the first unconverged subspace gets
+        // more passes and every later one is re-run (their state is then a
+        // superset of the right answer, from which further passes converge
+        // to it).
         std::vector<uint8_t> later(p.alloc[1] + p.alloc[2], 0);
         for (size_t i = 1; i < p.ySplitsAlloc.size(); ++i) later[p.ySplitsAlloc[i].lo - 1] = 1;
         for (size_t i = 1; i < p.zSplitsAlloc.size(); ++i) later[p.alloc[1] + p.zSplitsAlloc[i].lo - 1] = 1;
         if ((rc = laterFlags.ensure(later.size() + 64))) return rc;
-        uint32_t* flags = small.as<uint32_t>() + 8;
-        constexpr int kBatch = 4;
-        for (const auto& z : p.zSplitsAlloc)
-            for (const auto& y : p.ySplitsAlloc) {
-                vxb::SplitYZ sp{y.lo, y.hi, z.lo, z.hi};
-                for (int round = 0;; ++round) {
-                    VXB_CUDA(cudaMemsetAsync(flags, 0, kBatch * 4, s));
-                    for (int b = 0; b < kBatch; ++b) vxb::launch_prune(fin.as<uint32_t>(), g, sp, flags + b, s, &launches);
-                    uint32_t h[kBatch];
-                    VXB_CUDA(cudaMemcpyAsync(h, flags, sizeof(h), cudaMemcpyDeviceToHost, s));
-                    VXB_CUDA(cudaStreamSynchronize(s));
-                    if (h[kBatch - 1] == 0) break;
-                    if (round > 1000000) return fail(VXB_ETIMEDOUT, "pruning did not converge");
-                }
-            }
         VXB_CUDA(cudaMemcpyAsync(laterFlags.p, later.data(), later.size(), cudaMemcpyHostToDevice, s));
-        mark(2, true, s);
         const uint8_t* yl = laterFlags.as<uint8_t>();
+        std::vector<vxb::SplitYZ> psplits;
+        for (const auto& z : p.zSplitsAlloc)
+            for (const auto& y : p.ySplitsAlloc) psplits.push_back(vxb::SplitYZ{y.lo, y.hi, z.lo, z.hi});
+        const size_t nS = psplits.size();
+        constexpr int kPasses = 3;
+        uint32_t* flags = sm + kFlags;
+        std::vector<uint32_t> h(kFlags + nS * kPasses);
+        size_t from = 0;
+        for (int round = 0;; ++round) {
+            VXB_CUDA(cudaMemsetAsync(flags, 0, 4 * nS * kPasses, s));
+            for (size_t i = from; i < nS; ++i)
+                for (int b = 0; b < kPasses; ++b)
+                    vxb::launch_prune(fin.as<uint32_t>(), fill[0].as<uint32_t>(), surfp, yl, yl + p.alloc[1], g,
+                                      psplits[i], flags + i * kPasses + b, s, &launches);
+            VXB_CUDA(cudaMemcpyAsync(h.data(), sm, 4 * (kFlags + nS * kPasses), cudaMemcpyDeviceToHost, s));
+            VXB_CUDA(cudaStreamSynchronize(s));
+            size_t bad = nS;
+            for (size_t i = from; i < nS; ++i)
+                if (h[kFlags + i * kPasses + kPasses - 1]) { bad = i; break; }
+            if (bad == nS) break;
+            from = bad;
+            if (round > 1000000) return fail(VXB_ETIMEDOUT, "pruning did not converge");
+        }
+        mark(2, true, s);
+        if (mats) {
+            mark(4, false, s);
+            if ((rc = resolveKeys(p, 1, gridWords, h[kHitCount], h[kSurfaceVoxels], s))) return rc;
+            mark(4, true, s);
+        }
         mark(3, false, s);
-        vxb::launch_emit_cartesian(nodeType, fin.as<uint32_t>(), fill[0].as<uint32_t>(),
-                                   mats ? surf[0].as<uint32_t>() : nullptr, g, yl, yl + p.alloc[1], dout, mats ? 1 : 0,
-                                   s, &launches);
+        vxb::launch_emit_cartesian(nodeType, fin.as<uint32_t>(), fill[0].as<uint32_t>(), surfp, ranks.as<uint32_t>(),
+                                   keys.p, g, yl, yl + p.alloc[1], dout, mats ? 1 : 0, s, &launches);
         mark(3, true, s);
         VXB_CUDA(cudaGetLastError());
         return 0;
     }
     // FCC: four shifted sub-lattices (src/host_side.cpp:1432-1484, 1525-1593).
-    const double h = p.d / 2.0;
-    const double shifts[4][3] = {{0.0, 0.0, 0.0}, {h, h, 0.0}, {0.0, h, h}, {h, 0.0, h}};
     const uint32_t* fp[4];
     const uint32_t* sp4[4];
-    for (int gt = 0; gt < 4; ++gt) {
-        if ((rc = fill[gt].ensure(gridBytes))) return rc;
-        if (mats && (rc = surf[gt].ensure(gridBytes))) return rc;
+    uint64_t base4[4];
+    for (int lt = 0; lt < 4; ++lt)
+        if ((rc = fill[lt].ensure(gridBytes))) return rc;
+    mark(0, false, s);
+    for (int lt = 0; lt < 4; ++lt) {
+        double sh[3];
+        latticeShift(p, lt, sh);
+        vxb::PassGeom g = makeGeom(p, sh[0], sh[1], sh[2]);
+        if ((rc = solidPass(p, g, fill[lt].as<uint32_t>(), s))) return rc;
+        fp[lt] = fill[lt].as<uint32_t>();
+        sp4[lt] = mats ? surfAll.as<uint32_t>() + lt * gridWords : nullptr;
+        base4[lt] = lt * gridWords;
+        if (mats && (rc = surfacePass(p, g, lt, gridWords, 0, s))) return rc;
     }
-    for (int gt = 0; gt < 4; ++gt) {
-        vxb::PassGeom g = makeGeom(p, shifts[gt][0], shifts[gt][1], shifts[gt][2]);
-        if ((rc = solidPass(p, g, fill[gt].as<uint32_t>(), s))) return rc;
-        fp[gt] = fill[gt].as<uint32_t>();
-        sp4[gt] = nullptr;
-        if (mats) {
-            if ((rc = surfacePass(p, g, gt + 1, surf[gt].as<uint32_t>(), dout, s))) return rc;
-            sp4[gt] = surf[gt].as<uint32_t>();
-        }
+    mark(0, true, s);
+    if (mats) {
+        mark(4, false, s);
+        vxb::launch_surface_rank(surfAll.as<uint32_t>(), gridWords * 4, ranks.as<uint32_t>(), rankTiles.as<uint32_t>(),
+                                 sm + kSurfaceVoxels, s, &launches);
+        uint32_t h[8];
+        VXB_CUDA(cudaMemcpyAsync(h, sm, sizeof(h), cudaMemcpyDeviceToHost, s));
+        VXB_CUDA(cudaStreamSynchronize(s));
+        if ((rc = resolveKeys(p, 4, gridWords, h[kHitCount], h[kSurfaceVoxels], s))) return rc;
+        mark(4, true, s);
     }
     vxb::PassGeom g = makeGeom(p, 0.0, 0.0, 0.0);
     mark(3, false, s);
-    vxb::launch_emit_fcc(nodeType, fp, sp4, g, dout, mats ? 1 : 0, s, &launches);
+    vxb::launch_emit_fcc(nodeType, fp, sp4, base4, ranks.as<uint32_t>(), keys.p, g, dout, mats ? 1 : 0, s, &launches);
     mark(3, true, s);
     VXB_CUDA(cudaGetLastError());
     return 0;

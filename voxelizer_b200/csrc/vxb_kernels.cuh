@@ -37,23 +37,42 @@ void launch_row_fill(uint32_t* words, uint32_t rows, uint32_t ipx, cudaStream_t 
 // ---- Surface voxelization: src/voxelizer.cu:2358-2989, 3040-4201 ----
 void launch_surface_count(const float* V, const uint32_t* I, uint32_t nT, PassGeom g, const Split3* splits,
                           uint32_t nSplits, uint32_t* codes, uint32_t* counts, cudaStream_t s, uint32_t* launches);
-// mode 0: mark surface bits and seed each node's key slot; mode 1: max-merge keys.
-void launch_surface_work(int nodeKind, int mode, const float* V, const uint32_t* I, const uint8_t* M,
-                         uint32_t nT, PassGeom g, int gridType, const Split3* splits, uint32_t nSplits,
-                         const uint32_t* codes, const uint32_t* offsets, const uint32_t* total, uint32_t* surfBits,
-                         void* nodes, cudaStream_t s, uint32_t* launches);
+// Surface work, one thread per (triangle, material subspace, column).
+// mode 0: set surface bits in `surfBits` and append (bit position << 24 |
+// key) to `list` (entries past listCap are counted, not stored); mode 1:
+// merge every hit's key at its rank (needs complete bits and `ranks`).
+// posBase is the bit position of surfBits[0] in the rank space (FCC
+// sub-lattices are stacked).  wide: 64-bit keys (PartialNode).
+void launch_surface_work(int mode, int wide, const float* V, const uint32_t* I, const uint8_t* M, uint32_t nT,
+                         PassGeom g, const Split3* splits, uint32_t nSplits, const uint32_t* codes,
+                         const uint32_t* offsets, const uint32_t* total, uint32_t* surfBits, uint64_t posBase,
+                         const uint32_t* ranks, void* keys, unsigned long long* list, uint32_t* listCount,
+                         uint32_t listCap, cudaStream_t s, uint32_t* launches);
+// Exclusive popcount prefix over `words` surface words; *total = surface voxels.
+void launch_surface_rank(const uint32_t* bits, uint64_t words, uint32_t* ranks, uint32_t* tileSums, uint32_t* total,
+                         cudaStream_t s, uint32_t* launches);
+void launch_surface_keys_zero(void* keys, const uint32_t* count, int wide, cudaStream_t s, uint32_t* launches);
+void launch_surface_merge(const unsigned long long* list, const uint32_t* listCount, uint32_t listCap,
+                          const uint32_t* bits, const uint32_t* ranks, uint32_t* keys, cudaStream_t s,
+                          uint32_t* launches);
 
 // ---- Node classification: src/voxelizer.cu:1626-2048 ----
 void launch_combine(const uint32_t* a, const uint32_t* b, uint32_t* out, uint64_t n, cudaStream_t s,
                     uint32_t* launches);
-void launch_prune(uint32_t* solid, PassGeom g, SplitYZ split, uint32_t* changed, cudaStream_t s,
+// One in-place pruning pass over `split`; neighbours in later subspaces
+// (yLater / zLater) are read from fill | surf.  Sets *changed if any word
+// changed.
+void launch_prune(uint32_t* solid, const uint32_t* fill, const uint32_t* surf, const uint8_t* yLater,
+                  const uint8_t* zLater, PassGeom g, SplitYZ split, uint32_t* changed, cudaStream_t s,
                   uint32_t* launches);
 // yLater[y] / zLater[z] are 1 where row y + 1 / plane z + 1 starts a later
-// pruning subspace than row y / plane z.
+// pruning subspace than row y / plane z.  ranks / keys: surface voxel ranks
+// and merged material keys (materials only).
 void launch_emit_cartesian(int nodeKind, const uint32_t* finalSolid, const uint32_t* fill, const uint32_t* surf,
-                           PassGeom g, const uint8_t* yLater, const uint8_t* zLater, void* nodes, int materials,
-                           cudaStream_t s, uint32_t* launches);
-void launch_emit_fcc(int nodeKind, const uint32_t* const* fill, const uint32_t* const* surf, PassGeom g, void* nodes,
+                           const uint32_t* ranks, const void* keys, PassGeom g, const uint8_t* yLater,
+                           const uint8_t* zLater, void* nodes, int materials, cudaStream_t s, uint32_t* launches);
+void launch_emit_fcc(int nodeKind, const uint32_t* const* fill, const uint32_t* const* surf,
+                     const uint64_t* surfWordBase, const uint32_t* ranks, const void* keys, PassGeom g, void* nodes,
                      int materials, cudaStream_t s, uint32_t* launches);
 
 }  // namespace vxb
