@@ -1,9 +1,22 @@
-// Solid (parity) voxelization kernels.
+// Solid (parity) voxelization kernels: calculateTileOverlap /
+// constructWorkQueue / generateVoxelization (src/voxelizer.cu:840-1617),
+// FP64 as in the reference.
+//
+// The reference sorts (tile, triangle) pairs and voxelizes one tile per
+// block.  Here the work list is the flat set of (triangle, yz subspace, 4x4
+// tile) candidates over an exclusive scan of per-triangle candidate counts;
+// a candidate is a member of the tile's list iff one voxel centre of the
+// tile inside the triangle's clipped bounding box passes the binning test,
+// and a member toggles, for each centre of the tile inside the subspace that
+// passes the strict generation test, the bit of its x-intercept voxel in the
+// centre's row.  Toggles commute (XOR), so no sort is needed; a row prefix
+// XOR then turns toggles into solid runs.  A block stages its candidates'
+// triangles (vertices, tN, voxel box, both edge-function sets, the normal)
+// in shared memory once.
+
 #include "vxb_common.cuh"
 #include "vxb_device.cuh"
 #include "vxb_kernels.cuh"
-
-#include <cfloat>
 
 namespace vxb {
 
@@ -12,9 +25,8 @@ using namespace detail;
 namespace {
 
 constexpr double kDblMin = 2.2250738585072014e-308;  // DBL_MIN, src/voxelizer.cu:1443
-
-// ---------------------------------------------------------------------------
-// Solid voxelization.
+constexpr int kBlock = 256;
+constexpr uint32_t kSlots = 96;
 
 __device__ __forceinline__ void loadTriD(const float* __restrict__ V, const uint32_t* __restrict__ I, uint32_t t,
                                          D3* v) {
@@ -88,97 +100,144 @@ __global__ void solidCountKernel(const float* __restrict__ V, const uint32_t* __
     }
 }
 
-// One thread per (triangle, subspace, 4x4 tile) candidate.  The candidate is
-// a member of the tile's work list iff one voxel centre of the tile inside
-// the triangle's clipped bounding box passes the inclusive edge test with
-// tN-oriented normals (traverseTilesForOverlaps, src/voxelizer.cu:980-1033).
-// A member then runs generateVoxelization's per-centre work
-// (src/voxelizer.cu:1344-1462) on all 16 centres of the tile inside the
-// subspace and toggles bit voxelX of the centre's row.
-__global__ void solidToggleKernel(const float* __restrict__ V, const uint32_t* __restrict__ I, uint32_t nT,
-                                  PassGeom g, const SplitYZ* __restrict__ splits, uint32_t nSplits,
-                                  const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ totalPtr,
-                                  uint32_t* __restrict__ toggles) {
-    const uint32_t total = *totalPtr;
+// Staged triangle: binning data plus the generation edge functions.
+struct SolidStage {
+    BinTri b;
+    double bnx[3], bny[3], bd[3];   // binning edges (oriented by tN)
+    D3 n;                           // cross(v0 - v2, v1 - v0)
+    double ex[3], ey[3], ed[3];     // generation edges (oriented by n.x)
+    uint32_t tl;                    // top-left flags of the generation edges
+};
+
+__device__ __forceinline__ void stageSolid(SolidStage& st, const float* V, const uint32_t* I, uint32_t t,
+                                           const PassGeom& g) {
+    binSetup(V, I, t, g, st.b);
+    const D3* v = st.b.v;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const D3& p = v[i];
+        const D3& q = v[(i + 1) % 3];
+        if (st.b.tN > 0.0) { st.bnx[i] = __dsub_rn(p.z, q.z); st.bny[i] = __dsub_rn(q.y, p.y); }
+        else { st.bnx[i] = __dsub_rn(q.z, p.z); st.bny[i] = __dsub_rn(p.y, q.y); }
+        st.bd[i] = -sum2<site::D_BIN>(st.bnx[i], p.y, st.bny[i], p.z);
+    }
+    const D3 U{__dsub_rn(v[0].x, v[2].x), __dsub_rn(v[0].y, v[2].y), __dsub_rn(v[0].z, v[2].z)};
+    const D3 W{__dsub_rn(v[1].x, v[0].x), __dsub_rn(v[1].y, v[0].y), __dsub_rn(v[1].z, v[0].z)};
+    st.n = D3{diff2<site::CR_GEN>(U.y, W.z, U.z, W.y), diff2<site::CR_GEN>(U.z, W.x, U.x, W.z),
+              diff2<site::CR_GEN>(U.x, W.y, U.y, W.x)};
+    st.tl = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const D3& p = v[i];
+        const D3& q = v[(i + 1) % 3];
+        if (st.n.x > 0.0) { st.ex[i] = __dsub_rn(p.z, q.z); st.ey[i] = __dsub_rn(q.y, p.y); }
+        else { st.ex[i] = __dsub_rn(q.z, p.z); st.ey[i] = __dsub_rn(p.y, q.y); }
+        st.ed[i] = -sum2<site::D_GEN>(st.ex[i], p.y, st.ey[i], p.z);
+        if (st.ex[i] > 0.0 || (st.ex[i] == 0.0 && st.ey[i] < 0.0)) st.tl |= 1u << i;
+    }
+}
+
+// One (triangle, subspace, tile) candidate: binning membership
+// (traverseTilesForOverlaps, src/voxelizer.cu:980-1033), then
+// generateVoxelization's per-centre work (1344-1462) for the tile's centres
+// inside the subspace.
+__device__ __forceinline__ void solidCandidate(const SolidStage& st, const SplitYZ* __restrict__ splits,
+                                               uint32_t nSplits, uint32_t local, const PassGeom& g,
+                                               uint32_t* __restrict__ toggles) {
     const double d = g.d;
-    for (uint32_t item = blockIdx.x * blockDim.x + threadIdx.x; item < total; item += gridDim.x * blockDim.x) {
-        const uint32_t t = findOwner(offsets, nT, item);
-        uint32_t local = item - __ldg(offsets + t);
-        BinTri b;
-        binSetup(V, I, t, g, b);
-        uint32_t lo[2] = {0, 0}, hi[2] = {0, 0};
-        SplitYZ sp = splits[0];
-        for (uint32_t s = 0; s < nSplits; ++s) {
-            if (!commonSpace(b, splits[s], lo, hi)) continue;
-            uint32_t nty = (hi[0] - 1) / 4 - lo[0] / 4 + 1, ntz = (hi[1] - 1) / 4 - lo[1] / 4 + 1;
-            if (local < nty * ntz) { sp = splits[s]; break; }
-            local -= nty * ntz;
+    uint32_t lo[2] = {0, 0}, hi[2] = {0, 0};
+    SplitYZ sp = splits[0];
+    for (uint32_t s = 0; s < nSplits; ++s) {
+        if (!commonSpace(st.b, splits[s], lo, hi)) continue;
+        const uint32_t nty = (hi[0] - 1) / 4 - lo[0] / 4 + 1, ntz = (hi[1] - 1) / 4 - lo[1] / 4 + 1;
+        if (local < nty * ntz) { sp = splits[s]; break; }
+        local -= nty * ntz;
+    }
+    const uint32_t nty = (hi[0] - 1) / 4 - lo[0] / 4 + 1;
+    const uint32_t tileY = lo[0] / 4 + local % nty, tileZ = lo[1] / 4 + local / nty;
+    bool member = false;
+    for (uint32_t iy = tileY * 4; iy < tileY * 4 + 4 && iy < hi[0] && !member; ++iy) {
+        if (iy < lo[0]) continue;
+        const double py = lin<site::P_BIN>((double)iy, d, g.mn[1]);
+        for (uint32_t iz = tileZ * 4; iz < tileZ * 4 + 4 && iz < hi[1]; ++iz) {
+            if (iz < lo[1]) continue;
+            const double pz = lin<site::P_BIN>((double)iz, d, g.mn[2]);
+            bool ok = true;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) ok &= sum2p1<site::E_BIN>(st.bnx[k], py, st.bny[k], pz, st.bd[k]) >= 0.0;
+            if (ok) { member = true; break; }
         }
-        const uint32_t nty = (hi[0] - 1) / 4 - lo[0] / 4 + 1;
-        const uint32_t tileY = lo[0] / 4 + local % nty, tileZ = lo[1] / 4 + local / nty;
-        const D3* v = b.v;
-        // Binning edge functions (orientation by the sign of tN).
-        double bnx[3], bny[3], bd[3];
+    }
+    if (!member) return;
+    const D3* v = st.b.v;
+    for (uint32_t c = 0; c < 16; ++c) {
+        const uint32_t vz = tileZ * 4 + c / 4, vy = tileY * 4 + c % 4;
+        if (vy < sp.y0 || vy >= sp.y1 || vz < sp.z0 || vz >= sp.z1) continue;
+        const double py = lin<site::P_GEN>((double)vy, d, g.mn[1]);
+        const double pz = lin<site::P_GEN>((double)vz, d, g.mn[2]);
+        int pass = 0;
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            const D3& p = v[i];
-            const D3& q = v[(i + 1) % 3];
-            if (b.tN > 0.0) { bnx[i] = __dsub_rn(p.z, q.z); bny[i] = __dsub_rn(q.y, p.y); }
-            else { bnx[i] = __dsub_rn(q.z, p.z); bny[i] = __dsub_rn(p.y, q.y); }
-            bd[i] = -sum2<site::D_BIN>(bnx[i], p.y, bny[i], p.z);
+            double r = sum2p1<site::E_GEN>(st.ex[i], py, st.ey[i], pz, st.ed[i]);
+            if ((st.tl >> i) & 1u) r = __dadd_rn(r, kDblMin);
+            pass += r > 0.0;
         }
-        bool member = false;
-        for (uint32_t iy = tileY * 4; iy < tileY * 4 + 4 && iy < hi[0] && !member; ++iy) {
-            if (iy < lo[0]) continue;
-            const double py = lin<site::P_BIN>((double)iy, d, g.mn[1]);
-            for (uint32_t iz = tileZ * 4; iz < tileZ * 4 + 4 && iz < hi[1]; ++iz) {
-                if (iz < lo[1]) continue;
-                const double pz = lin<site::P_BIN>((double)iz, d, g.mn[2]);
-                bool ok = true;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) ok &= sum2p1<site::E_BIN>(bnx[k], py, bny[k], pz, bd[k]) >= 0.0;
-                if (ok) { member = true; break; }
+        if (pass != 3) continue;
+        const double ax = __dsub_rn(v[0].x, g.mn[0]), ay = __dsub_rn(v[0].y, py), az = __dsub_rn(v[0].z, pz);
+        const double B = sum3<site::B_GEN>(ax, st.n.x, ay, st.n.y, az, st.n.z);
+        double px = __ddiv_rn(B, st.n.x);
+        px = px < 0.0 ? 0.0 : px;
+        const uint32_t vx = __double2uint_rz(ceil(__ddiv_rn(px, d))) + 1u;
+        if (vx >= g.X) continue;
+        const uint32_t row = (vz + 1) * g.AY + (vy + 1);
+        atomicXor(toggles + (size_t)row * g.ipx + (vx >> 5), 0x80000000u >> (vx & 31u));
+    }
+}
+
+__global__ void __launch_bounds__(kBlock, 3) solidToggleKernel(const float* __restrict__ V,
+                                                            const uint32_t* __restrict__ I, uint32_t nT, PassGeom g,
+                                                            const SplitYZ* __restrict__ splits, uint32_t nSplits,
+                                                            const uint32_t* __restrict__ offsets,
+                                                            const uint32_t* __restrict__ totalPtr,
+                                                            uint32_t* __restrict__ toggles) {
+    __shared__ SolidStage stage[kSlots];
+    __shared__ uint32_t stOff[kSlots + 1];
+    __shared__ uint32_t tFirst, nStage;
+    const uint32_t total = *totalPtr;
+    for (uint32_t base = blockIdx.x * kBlock; base < total; base += gridDim.x * kBlock) {
+        const uint32_t last = min(base + kBlock, total) - 1;
+        if (threadIdx.x == 0) {
+            const uint32_t t0 = findOwner(offsets, nT, base);
+            const uint32_t t1 = findOwner(offsets, nT, last);
+            tFirst = t0;
+            nStage = min(t1 - t0 + 1, kSlots);
+        }
+        __syncthreads();
+        const uint32_t t0 = tFirst, ns = nStage;
+        if (threadIdx.x < ns) {
+            stageSolid(stage[threadIdx.x], V, I, t0 + threadIdx.x, g);
+            stOff[threadIdx.x] = __ldg(offsets + t0 + threadIdx.x);
+        }
+        if (threadIdx.x == 0) stOff[ns] = __ldg(offsets + t0 + ns);
+        __syncthreads();
+        const uint32_t item = base + threadIdx.x;
+        if (item <= last) {
+            if (item < stOff[ns]) {
+                uint32_t lo = 0, hi = ns;  // stOff[lo] <= item < stOff[hi]
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (stOff[mid] <= item) lo = mid;
+                    else hi = mid;
+                }
+                solidCandidate(stage[lo], splits, nSplits, item - stOff[lo], g, toggles);
+            } else {
+                const uint32_t t = findOwner(offsets, nT, item);
+                SolidStage st;
+                stageSolid(st, V, I, t, g);
+                solidCandidate(st, splits, nSplits, item - __ldg(offsets + t), g, toggles);
             }
         }
-        if (!member) continue;
-        // Generation: normal cross(v0 - v2, v1 - v0), edges oriented by n.x.
-        const D3 U{__dsub_rn(v[0].x, v[2].x), __dsub_rn(v[0].y, v[2].y), __dsub_rn(v[0].z, v[2].z)};
-        const D3 W{__dsub_rn(v[1].x, v[0].x), __dsub_rn(v[1].y, v[0].y), __dsub_rn(v[1].z, v[0].z)};
-        const D3 n{diff2<site::CR_GEN>(U.y, W.z, U.z, W.y), diff2<site::CR_GEN>(U.z, W.x, U.x, W.z),
-                   diff2<site::CR_GEN>(U.x, W.y, U.y, W.x)};
-        double ex[3], ey[3], ed[3];
-        bool tl[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            const D3& p = v[i];
-            const D3& q = v[(i + 1) % 3];
-            if (n.x > 0.0) { ex[i] = __dsub_rn(p.z, q.z); ey[i] = __dsub_rn(q.y, p.y); }
-            else { ex[i] = __dsub_rn(q.z, p.z); ey[i] = __dsub_rn(p.y, q.y); }
-            ed[i] = -sum2<site::D_GEN>(ex[i], p.y, ey[i], p.z);
-            tl[i] = ex[i] > 0.0 || (ex[i] == 0.0 && ey[i] < 0.0);
-        }
-        for (uint32_t c = 0; c < 16; ++c) {
-            const uint32_t vz = tileZ * 4 + c / 4, vy = tileY * 4 + c % 4;
-            if (vy < sp.y0 || vy >= sp.y1 || vz < sp.z0 || vz >= sp.z1) continue;
-            const double py = lin<site::P_GEN>((double)vy, d, g.mn[1]);
-            const double pz = lin<site::P_GEN>((double)vz, d, g.mn[2]);
-            int pass = 0;
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                double r = sum2p1<site::E_GEN>(ex[i], py, ey[i], pz, ed[i]);
-                if (tl[i]) r = __dadd_rn(r, kDblMin);
-                pass += r > 0.0;
-            }
-            if (pass != 3) continue;
-            const double ax = __dsub_rn(v[0].x, g.mn[0]), ay = __dsub_rn(v[0].y, py), az = __dsub_rn(v[0].z, pz);
-            const double B = sum3<site::B_GEN>(ax, n.x, ay, n.y, az, n.z);
-            double px = __ddiv_rn(B, n.x);
-            px = px < 0.0 ? 0.0 : px;
-            const uint32_t vx = __double2uint_rz(ceil(__ddiv_rn(px, d))) + 1u;
-            if (vx >= g.X) continue;
-            const uint32_t row = (vz + 1) * g.AY + (vy + 1);
-            atomicXor(toggles + (size_t)row * g.ipx + (vx >> 5), 0x80000000u >> (vx & 31u));
-        }
+        __syncthreads();
     }
 }
 
@@ -202,6 +261,7 @@ __global__ void rowFillKernel(uint32_t* __restrict__ words, uint32_t rows, uint3
         }
     }
 }
+
 }  // namespace
 
 void launch_solid_count(const float* V, const uint32_t* I, uint32_t nT, PassGeom g, const SplitYZ* splits,
@@ -213,7 +273,7 @@ void launch_solid_count(const float* V, const uint32_t* I, uint32_t nT, PassGeom
 void launch_solid_toggle(const float* V, const uint32_t* I, uint32_t nT, PassGeom g, const SplitYZ* splits,
                          uint32_t nSplits, const uint32_t* offsets, const uint32_t* total, uint32_t* toggles,
                          cudaStream_t s, uint32_t* launches) {
-    solidToggleKernel<<<148 * 8, 256, 0, s>>>(V, I, nT, g, splits, nSplits, offsets, total, toggles);
+    solidToggleKernel<<<148 * 3, kBlock, 0, s>>>(V, I, nT, g, splits, nSplits, offsets, total, toggles);
     *launches += 1;
 }
 
@@ -221,4 +281,5 @@ void launch_row_fill(uint32_t* words, uint32_t rows, uint32_t ipx, cudaStream_t 
     rowFillKernel<<<gridFor((uint64_t)rows * 32, 256), 256, 0, s>>>(words, rows, ipx);
     *launches += 1;
 }
+
 }  // namespace vxb
