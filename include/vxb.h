@@ -132,6 +132,27 @@ vxb_status vxb_last_launch_count(vxb_voxelizer* v, uint32_t* launches);
 vxb_status vxb_set_profiling(vxb_voxelizer* v, int enable);
 vxb_status vxb_stage_times(vxb_voxelizer* v, float* ms, uint32_t n);
 
+/* No counterpart in the reference.  The plain voxelization of
+ * vxb_voxelize_to_device(v, 0, ...) for callers that cannot allocate device
+ * memory: solvers that reserve the whole GPU for their own pool, or that
+ * cannot let cudaFree / cudaMalloc synchronize the device mid-step.  It
+ * allocates nothing: the mesh (dev_vertices: 3 floats per vertex,
+ * dev_indices: 3 indices < n_vertices per triangle) and dev_out are the
+ * caller's device buffers, and its work lists live in a fixed device array
+ * of 16,796,672 bytes inside the library, which every GPU that loads the
+ * library holds until exit.  min_vertex / max_vertex: the mesh's bounding
+ * box, the component-wise min / max of the vertices (vxb_plan reports it).
+ * Limits: at most 2,097,152 triangles and 1024 yz subspaces (vox_split_res
+ * parts in y times z); larger requests return VXB_EINVAL.  Runs on the
+ * current device, stream-ordered on `stream`.  The first call on a device
+ * looks up the array's address (one-time set-up); make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race
+ * and must be serialized by the caller. */
+vxb_status vxb_voxelize_bits_noalloc(const float* dev_vertices, const uint32_t* dev_indices, uint32_t n_vertices,
+                                     uint32_t n_triangles, const double min_vertex[3], const double max_vertex[3],
+                                     const vxb_request* req, void* dev_out, uint64_t dev_bytes, void* stream,
+                                     vxb_grid_info* info);
+
 #ifdef __cplusplus
 }
 #endif

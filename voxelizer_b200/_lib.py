@@ -24,7 +24,7 @@ NODE_BYTES = {SHORT: 1, LONG: 2, PARTIAL: 8, SHORT_FCC: 2, LONG_FCC: 4}
 EXPORTS = ["vxb_last_error", "vxb_version", "vxb_create", "vxb_destroy", "vxb_set_materials",
            "vxb_set_material_output", "vxb_verbose_output", "vxb_plan", "vxb_get_array_dimensions",
            "vxb_voxelize_to_host", "vxb_voxelize_to_device", "vxb_last_launch_count", "vxb_set_profiling",
-           "vxb_stage_times"]
+           "vxb_stage_times", "vxb_voxelize_bits_noalloc"]
 
 
 class VxbError(RuntimeError):
@@ -82,6 +82,9 @@ def lib():
         "vxb_last_launch_count": (ctypes.c_int, [vp, P(ctypes.c_uint32)]),
         "vxb_set_profiling": (ctypes.c_int, [vp, ctypes.c_int]),
         "vxb_stage_times": (ctypes.c_int, [vp, P(ctypes.c_float), ctypes.c_uint32]),
+        "vxb_voxelize_bits_noalloc": (ctypes.c_int, [vp, vp, ctypes.c_uint32, ctypes.c_uint32, P(ctypes.c_double),
+                                                     P(ctypes.c_double), P(Request), vp, ctypes.c_uint64, vp,
+                                                     P(GridInfo)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -76,6 +76,12 @@ enum : int { kSolidTotal = 0, kSolidOverflow = 1, kSurfTotal = 2, kSurfOverflow 
 
 }  // namespace
 
+namespace vxb {
+// Stores `msg` as the calling thread's vxb_last_error message and returns
+// `code`; for entry points defined in other files.
+int recordError(int code, const char* msg) { return fail(code, "%s", msg); }
+}  // namespace vxb
+
 struct vxb_voxelizer {
     int nodeType = 0;
     int device = 0;

@@ -1,0 +1,267 @@
+// vxb_voxelize_bits_noalloc: the plain (solid) voxelization of
+// vxb_voxelize_to_device(v, 0, ...) for callers that cannot allocate device
+// memory.  Such callers exist because the FDTD codes this library feeds
+// often reserve all of a GPU's memory for their field arrays up front and
+// hand out slices of that pool themselves, and because cudaFree (and at
+// times cudaMalloc) synchronizes the whole device, which a caller that keeps
+// several streams busy cannot afford in the middle of a time step.  The
+// caller passes the mesh and the output already in device memory; the work
+// lists this path needs (per-triangle candidate counts, their scan and the
+// yz subspace table) live in a fixed, statically sized array in device
+// memory instead of buffers allocated per call.  The call itself allocates
+// nothing, on the device or on the host (its subspace table is built on the
+// stack); the array is placed by the CUDA driver when it loads this
+// library's device code.
+//
+// Limits: at most kMaxTriangles triangles and kMaxSubspaces yz subspaces
+// per call; larger requests are rejected with VXB_EINVAL.
+//
+// The first call on a device looks up the array's device address (a
+// one-time set-up per device, made with that device current); make that
+// first call before any stream capture.
+//
+// The array is shared by every call on a device and keeps the previous
+// call's contents; each call overwrites everything it reads before reading
+// it, so nothing has to be cleared.  Calls whose work overlaps on the GPU
+// (two host threads, or two streams without ordering between them) race on
+// the array and give undefined results: serialize them.
+
+#include "vxb.h"
+#include "vxb_kernels.cuh"
+#include "vxb_plan.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+namespace vxb {
+int recordError(int code, const char* msg);  // vxb_engine.cu
+}
+
+namespace {
+
+constexpr uint32_t kMaxTriangles = 1u << 21;  // 2,097,152
+constexpr uint32_t kMaxSubspaces = 1024;
+constexpr uint32_t kScanTile = 4096;          // items per tile of launch_scan
+constexpr int kMaxDevices = 64;
+
+constexpr size_t roundUp(size_t v) { return (v + 255) / 256 * 256; }
+
+// Layout of the scratch array (byte offsets).
+constexpr size_t kStatusOff = 0;  // [0] candidate total, [1] overflow flag
+constexpr size_t kSubspaceOff = kStatusOff + 256;
+constexpr size_t kTileOff = kSubspaceOff + roundUp(kMaxSubspaces * sizeof(vxb::SplitYZ));
+constexpr size_t kCountOff = kTileOff + roundUp(4 * (kMaxTriangles / kScanTile + 2));
+constexpr size_t kOffsetOff = kCountOff + roundUp(4 * ((size_t)kMaxTriangles + 1));
+constexpr size_t kScratchBytes = kOffsetOff + roundUp(4 * ((size_t)kMaxTriangles + 2));
+static_assert(kScratchBytes == 16796672, "scratch layout changed: update the stated size");
+
+}  // namespace
+
+// 16,796,672 bytes (about 16.0 MiB) of device memory, held by every GPU that
+// loads this library until the process exits.
+static __device__ __align__(256) unsigned char g_noallocScratch[kScratchBytes];
+
+namespace {
+
+void* g_scratchAddress[kMaxDevices] = {};
+std::mutex g_setupLock;
+
+int failf(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+int failf(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    return vxb::recordError(code, buf);
+}
+
+// Device address of the scratch array on `device` (the current device).  In
+// host code g_noallocScratch names a host-side shadow, not device memory, so
+// the address is looked up once per device and cached.
+int scratchAddress(int device, unsigned char** out) {
+    std::lock_guard<std::mutex> lock(g_setupLock);
+    if (!g_scratchAddress[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noallocScratch);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return failf(VXB_ECUDA, "cudaGetSymbolAddress of the scratch array failed on device %d: %s", device,
+                         cudaGetErrorString(e));
+        }
+        g_scratchAddress[device] = p;
+    }
+    *out = static_cast<unsigned char*>(g_scratchAddress[device]);
+    return 0;
+}
+
+// The grid arithmetic of vxb::makePlan (determineDimensions and the x
+// rounding of src/host_side.cpp:2497-2634) without its split vectors.
+struct BitGrid {
+    double d;
+    uint32_t res[3], alloc[3], xSplits;
+};
+
+int sizeGrid(const double* mn, const double* mx, const vxb_request* r, BitGrid& g) {
+    const double dx = mx[0] - mn[0], dy = mx[1] - mn[1], dz = mx[2] - mn[2];
+    uint32_t res[3];
+    double d;
+    if (r->by_cube_length) {
+        if (!(r->cube_length > 0.0)) return -1;
+        d = r->cube_length;
+        res[0] = vxb::toUint(std::ceil(dx / d)) + 1;
+        res[1] = vxb::toUint(std::ceil(dy / d)) + 1;
+        res[2] = vxb::toUint(std::ceil(dz / d)) + 1;
+    } else {
+        if (r->max_dimension < 2) return -1;
+        const uint32_t m = r->max_dimension;
+        if (dx > dy && dx > dz) {
+            d = dx / double(m - 1);
+            res[0] = m; res[1] = vxb::toUint(std::ceil(dy / d)) + 1; res[2] = vxb::toUint(std::ceil(dz / d)) + 1;
+        } else if (dx > dy) {
+            d = dz / double(m - 1);
+            res[2] = m; res[0] = vxb::toUint(std::ceil(dx / d)) + 1; res[1] = vxb::toUint(std::ceil(dy / d)) + 1;
+        } else if (dy > dz) {
+            d = dy / double(m - 1);
+            res[1] = m; res[0] = vxb::toUint(std::ceil(dx / d)) + 1; res[2] = vxb::toUint(std::ceil(dz / d)) + 1;
+        } else {
+            d = dz / double(m - 1);
+            res[2] = m; res[0] = vxb::toUint(std::ceil(dx / d)) + 1; res[1] = vxb::toUint(std::ceil(dy / d)) + 1;
+        }
+        if (!(d > 0.0)) return -1;
+    }
+    res[0] += 2;
+    const uint32_t vs[3] = {r->vox_split_res.x, r->vox_split_res.y, r->vox_split_res.z};
+    for (int a = 0; a < 3; ++a)
+        if (vs[a] == 0) return -1;
+    g.d = d;
+    g.xSplits = (res[0] + vs[0] - 1) / vs[0];
+    const uint32_t xMod = 32u * g.xSplits;
+    if (res[0] % xMod != 0) res[0] += xMod - res[0] % xMod;
+    if (res[0] / g.xSplits > 1024) return -1;
+    for (int a = 0; a < 3; ++a) g.res[a] = res[a];
+    g.alloc[0] = res[0];
+    g.alloc[1] = res[1] + 2;
+    g.alloc[2] = res[2] + 2;
+    return 0;
+}
+
+// Parts of splitResolutionByNrOfParts (vxb::splitLength) into `out`.
+uint32_t splitInto(uint32_t len, uint32_t maxPart, vxb::Range* out) {
+    const uint32_t n = (len + maxPart - 1) / maxPart;
+    uint32_t prev = len;
+    for (uint32_t i = n; i > 0; --i) {
+        out[i - 1].hi = prev;
+        out[i - 1].lo = prev - prev / i;
+        prev = out[i - 1].lo;
+    }
+    return n;
+}
+
+}  // namespace
+
+extern "C" vxb_status vxb_voxelize_bits_noalloc(const float* dev_vertices, const uint32_t* dev_indices,
+                                                uint32_t n_vertices, uint32_t n_triangles,
+                                                const double* min_vertex, const double* max_vertex,
+                                                const vxb_request* req, void* dev_out, uint64_t dev_bytes,
+                                                void* stream, vxb_grid_info* info) {
+    if (!dev_vertices || !dev_indices || !min_vertex || !max_vertex || !req || !dev_out)
+        return failf(VXB_EINVAL, "NULL argument");
+    if (n_vertices == 0 || n_triangles == 0) return failf(VXB_EINVAL, "empty mesh");
+    if (n_triangles > kMaxTriangles)
+        return failf(VXB_EINVAL,
+                     "%u triangles exceed the %u that the allocation-free path's fixed scratch array holds; "
+                     "use vxb_voxelize_to_device",
+                     n_triangles, kMaxTriangles);
+    BitGrid bg;
+    if (sizeGrid(min_vertex, max_vertex, req, bg))
+        return failf(VXB_EINVAL, "invalid request (maxDimension >= 2 or cubeLength > 0, split sizes > 0 and an x "
+                                 "pass of at most 1024 voxels are required)");
+    const uint64_t voxels = (uint64_t)bg.alloc[0] * bg.alloc[1] * bg.alloc[2];
+    if (voxels > 0xFFFFFFFFull) return failf(VXB_EOVERFLOW, "voxel grid exceeds 32-bit indexing");
+    const uint32_t ny = (bg.res[1] + req->vox_split_res.y - 1) / req->vox_split_res.y;
+    const uint32_t nz = (bg.res[2] + req->vox_split_res.z - 1) / req->vox_split_res.z;
+    if ((uint64_t)ny * nz > kMaxSubspaces)
+        return failf(VXB_EINVAL,
+                     "%llu yz subspaces exceed the %u that the allocation-free path's fixed scratch array holds; "
+                     "use larger split sizes",
+                     (unsigned long long)ny * nz, kMaxSubspaces);
+    vxb_grid_info gi;
+    memset(&gi, 0, sizeof(gi));
+    gi.dim.x = bg.alloc[0];
+    gi.dim.y = bg.alloc[1];
+    gi.dim.z = bg.alloc[2];
+    gi.count = voxels / 32;
+    gi.bytes = gi.count * 4;
+    gi.voxel_length = bg.d;
+    for (int a = 0; a < 3; ++a) {
+        gi.min_vertex[a] = min_vertex[a];
+        gi.max_vertex[a] = max_vertex[a];
+    }
+    gi.resolution.x = bg.res[0];
+    gi.resolution.y = bg.res[1];
+    gi.resolution.z = bg.res[2];
+    gi.x_splits = bg.xSplits;
+    if (info) *info = gi;
+    if (dev_bytes < gi.bytes)
+        return failf(VXB_EINVAL, "output buffer holds %llu bytes, %llu needed", (unsigned long long)dev_bytes,
+                     (unsigned long long)gi.bytes);
+
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return failf(VXB_ECUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+    if (device < 0 || device >= kMaxDevices) return failf(VXB_EINVAL, "device %d is not supported", device);
+    unsigned char* scratch = nullptr;
+    if (int rc = scratchAddress(device, &scratch)) return rc;
+
+    // yz subspaces of the solid pass in the reference's order (z outer).
+    vxb::Range ys[kMaxSubspaces], zs[kMaxSubspaces];
+    vxb::SplitYZ sub[kMaxSubspaces];
+    splitInto(bg.res[1], req->vox_split_res.y, ys);
+    splitInto(bg.res[2], req->vox_split_res.z, zs);
+    uint32_t nSub = 0;
+    for (uint32_t z = 0; z < nz; ++z)
+        for (uint32_t y = 0; y < ny; ++y) sub[nSub++] = vxb::SplitYZ{ys[y].lo, ys[y].hi, zs[z].lo, zs[z].hi};
+
+    vxb::PassGeom g;
+    for (int a = 0; a < 3; ++a) {
+        g.mn[a] = min_vertex[a];
+        g.mnf[a] = (float)min_vertex[a];
+    }
+    g.d = bg.d;
+    g.df = (float)bg.d;
+    g.X = bg.res[0];
+    g.resY = bg.res[1];
+    g.resZ = bg.res[2];
+    g.AY = bg.alloc[1];
+    g.AZ = bg.alloc[2];
+    g.ipx = bg.res[0] / 32;
+
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    uint32_t* status = reinterpret_cast<uint32_t*>(scratch + kStatusOff);
+    vxb::SplitYZ* dsub = reinterpret_cast<vxb::SplitYZ*>(scratch + kSubspaceOff);
+    uint32_t* tiles = reinterpret_cast<uint32_t*>(scratch + kTileOff);
+    uint32_t* counts = reinterpret_cast<uint32_t*>(scratch + kCountOff);
+    uint32_t* offsets = reinterpret_cast<uint32_t*>(scratch + kOffsetOff);
+    uint32_t* grid = static_cast<uint32_t*>(dev_out);
+    uint32_t launches = 0;
+    e = cudaMemsetAsync(grid, 0, gi.bytes, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dsub, sub, nSub * sizeof(vxb::SplitYZ), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return failf(VXB_ECUDA, "%s", cudaGetErrorString(e));
+    }
+    vxb::launch_solid_count(dev_vertices, dev_indices, n_triangles, g, dsub, nSub, counts, s, &launches);
+    vxb::launch_scan(counts, offsets, n_triangles, tiles, status, status + 1, s, &launches);
+    vxb::launch_solid_toggle(dev_vertices, dev_indices, n_triangles, g, dsub, nSub, offsets, status, grid, s,
+                             &launches);
+    vxb::launch_row_fill(grid, g.AY * g.AZ, g.ipx, s, &launches);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return failf(VXB_ECUDA, "%s", cudaGetErrorString(e));
+    return VXB_OK;
+}
