@@ -14,8 +14,11 @@ value: Gvoxels/s of node grid, device resident (mesh already on the GPU,
 e2e: the same metric through the reference-facing C ABI with host buffers:
   each step constructs the voxelizer from pinned host arrays, uploads the
   mesh, voxelizes and copies the node grid back into pinned host memory.
---impl reference: the reference algorithm's CPU restatement (oracle/) on
-  all host cores, on a bounded sample of the same workload.
+--impl reference: the reference's own implementation of the path.  It has
+  no CPU code: its kernels are CUDA (src/voxelizer.cu), built from its
+  sources into oracle/_ref/ and run on cuda:0 with host arrays in and out,
+  on the full workload.  Where that library or a GPU is missing, the CPU
+  restatement (oracle/) runs on all host cores on a bounded sample.
 Multi-GPU: replicas only (the path does not shard); under torchrun every
 rank voxelizes its own copy and value sums the voxels of all ranks over the
 slowest rank's time.
@@ -120,9 +123,93 @@ def dist_setup():
     return world, rank, local
 
 
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libvoxref.so")
+
+
+def _reference_cuda():
+    """The reference's own CUDA kernels (src/voxelizer.cu compiled from its
+    sources by oracle/Makefile) with the driver of oracle/ref_driver.cu, or
+    None where that library or a GPU is missing."""
+    if not os.path.exists(REF_LIB):
+        return None
+    try:
+        import torch
+
+        if not torch.cuda.is_available():
+            return None
+    except ImportError:
+        return None
+    import ctypes
+
+    lib = ctypes.CDLL(REF_LIB)
+    f = lib.ref_voxelize
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_double,
+                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                  ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint64,
+                  ctypes.c_void_p, ctypes.c_void_p]
+    lib.ref_last_error.restype = ctypes.c_char_p
+    return f, lib
+
+
+def run_reference_cuda(args, world, ref):
+    """Full workload through the reference's CUDA path on cuda:0: host arrays
+    in, node grid back in host memory, wall clock per call (the reference's
+    voxelizeToNodesToRAM allocates, uploads, computes and copies back inside
+    the call)."""
+    import ctypes
+
+    from voxelizer_b200 import scenes
+
+    f, lib = ref
+    mesh = scenes.room_scene()
+    vox = np.array([1024, 512, 512], dtype=np.uint32)
+    mat = np.array([512, 512, 512], dtype=np.uint32)
+    dims = np.zeros(3, dtype=np.uint32)
+    ms = ctypes.c_double(0.0)
+    v = np.ascontiguousarray(mesh.vertices.reshape(-1))
+    i = np.ascontiguousarray(mesh.indices.reshape(-1))
+    m = np.ascontiguousarray(mesh.materials)
+    args_common = (1, 1, 1, 0, MAX_DIM, 0.0, vox.ctypes.data, mat.ctypes.data, v.ctypes.data, mesh.n_vertices,
+                   i.ctypes.data, mesh.n_triangles, m.ctypes.data, mesh.n_materials)
+    rc = f(*args_common, None, 0, dims.ctypes.data, None)
+    if rc != 0:
+        raise RuntimeError(f"reference plan failed ({rc}): {lib.ref_last_error().decode()}")
+    n_nodes = int(dims[0]) * int(dims[1]) * int(dims[2])
+    out = np.empty(n_nodes, dtype=np.uint16)
+    times = []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        rc = f(*args_common, out.ctypes.data, out.nbytes, dims.ctypes.data, ctypes.byref(ms))
+        dt = time.perf_counter() - t0
+        if rc != 0:
+            raise RuntimeError(f"reference run failed ({rc}): {lib.ref_last_error().decode()}")
+        if k >= args.warmup:
+            times.append(dt)
+    t = sum(times)
+    value = n_nodes * len(times) / t / 1e9
+    sample = (f"full workload, {int(dims[0])}x{int(dims[1])}x{int(dims[2])} nodes per step: the reference's own "
+              f"CUDA kernels (src/voxelizer.cu built from its sources for sm_100a) on cuda:0, host arrays in and "
+              f"out, wall clock per call")
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t / len(times), 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32+u32",
+            "data": "synthetic (seeded room scene)", "device": "cuda:0",
+            "config": {"workload": WORKLOAD, "sample": sample},
+            "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": 1, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, world, rank):
-    """CPU restatement of the reference (oracle/) on all host cores."""
+    """The reference's implementation of the path: its CUDA build where it
+    was compiled, else its CPU restatement (oracle/) on all host cores."""
     if rank != 0:
+        return
+    ref = _reference_cuda()
+    if ref is not None:
+        run_reference_cuda(args, world, ref)
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
@@ -156,17 +243,20 @@ def run_reference(args, world, rank):
 
 
 def cpu_baseline(mesh):
+    """One run of the CPU restatement (oracle/) of the reference's kernels on
+    the full workload, all host cores."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
     cores = os.cpu_count() or 1
     t0 = time.perf_counter()
-    out, info, _ = O.voxelize(mesh, 1, 1, 1, CPU_SAMPLE_DIM, threads=cores)
+    out, info, _ = O.voxelize(mesh, 1, 1, 1, MAX_DIM, threads=cores)
     dt = time.perf_counter() - t0
     n = info.dims[0] * info.dims[1] * info.dims[2]
+    del out
     return {"value": round(n / dt / 1e9, 6), "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"same scene at maxDimension {CPU_SAMPLE_DIM} ({info.dims[0]}x{info.dims[1]}x{info.dims[2]} "
-                      f"nodes), one full path, {dt:.1f} s"}
+            "sample": f"the full workload ({info.dims[0]}x{info.dims[1]}x{info.dims[2]} nodes), one run of the "
+                      f"whole path, {dt:.1f} s on {cores} threads"}
 
 
 def main():
@@ -270,7 +360,7 @@ def main():
             "vs_baseline": None, "dtype": "f64+f32+u32", "data": "synthetic (seeded room scene)",
             "config": {"workload": WORKLOAD, "l2": "256 MB flush before every timed step",
                        "parallelism": f"replicas x{world}"},
-            "roofline": {"bound": "hbm", "kernel": "emitCartesianKernel<LongNode>",
+            "roofline": {"bound": "hbm", "kernel": "emitNarrowKernel<LongNode>",
                          "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
                          "peak_kind": peak_kind, "frac": round(achieved / peak, 4) if achieved else None,
                          "traffic": traffic, "algorithmic_bytes": int(emit_bytes), "ms": round(emit_ms, 4)},

@@ -24,7 +24,7 @@ NODE_BYTES = {SHORT: 1, LONG: 2, PARTIAL: 8, SHORT_FCC: 2, LONG_FCC: 4}
 EXPORTS = ["vxb_last_error", "vxb_version", "vxb_create", "vxb_destroy", "vxb_set_materials",
            "vxb_set_material_output", "vxb_verbose_output", "vxb_plan", "vxb_get_array_dimensions",
            "vxb_voxelize_to_host", "vxb_voxelize_to_device", "vxb_last_launch_count", "vxb_set_profiling",
-           "vxb_stage_times", "vxb_voxelize_bits_noalloc"]
+           "vxb_stage_times", "vxb_voxelize_bits_noalloc", "vxb_trim_cache"]
 
 
 class VxbError(RuntimeError):
@@ -70,6 +70,7 @@ def lib():
         "vxb_version": (ctypes.c_char_p, []),
         "vxb_create": (ctypes.c_int, [P(vp), ctypes.c_int, vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int]),
         "vxb_destroy": (ctypes.c_int, [vp]),
+        "vxb_trim_cache": (ctypes.c_int, []),
         "vxb_set_materials": (ctypes.c_int, [vp, vp, ctypes.c_uint32]),
         "vxb_set_material_output": (ctypes.c_int, [vp, ctypes.c_int]),
         "vxb_verbose_output": (ctypes.c_int, [vp, ctypes.c_int]),

@@ -18,7 +18,9 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -48,20 +50,90 @@ const uint32_t kMaxMat[5] = {7, 255, 255, 15, 255};
 
 bool isFcc(int t) { return t == VXB_SHORT_FCC_NODE || t == VXB_LONG_FCC_NODE; }
 
-// A device buffer that only grows.
+// Process-wide cache of idle device blocks.  Buffers of destroyed
+// voxelizers (and buffers outgrown by a larger request) go here instead of
+// cudaFree, and the next allocation of a similar size takes them back, so a
+// caller that builds one voxelizer per mesh pays cudaMalloc / cudaFree once.
+// Blocks enter the cache only after the device has finished all work, which
+// keeps them free of in-flight kernels.  Idle bytes are capped; vxb_trim_cache
+// returns them all to the driver.
+struct BlockCache {
+    std::mutex mu;
+    std::multimap<size_t, std::pair<int, void*>> idle;   // bytes -> (device, block)
+    size_t idleBytes = 0;
+    static constexpr size_t kBudget = 16ull << 30;
+};
+
+BlockCache& blockCache() {
+    static BlockCache* c = new BlockCache;   // never destroyed: blocks outlive static destructors
+    return *c;
+}
+
+void* cacheTake(int device, size_t bytes, size_t* got) {
+    BlockCache& c = blockCache();
+    std::lock_guard<std::mutex> lock(c.mu);
+    for (auto it = c.idle.lower_bound(bytes); it != c.idle.end() && it->first <= 2 * bytes + (1u << 20); ++it) {
+        if (it->second.first != device) continue;
+        void* p = it->second.second;
+        *got = it->first;
+        c.idleBytes -= it->first;
+        c.idle.erase(it);
+        return p;
+    }
+    return nullptr;
+}
+
+// `p` must no longer be used by any queued work.
+void cacheGive(int device, void* p, size_t bytes) {
+    BlockCache& c = blockCache();
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        if (c.idleBytes + bytes <= BlockCache::kBudget) {
+            c.idle.emplace(bytes, std::make_pair(device, p));
+            c.idleBytes += bytes;
+            return;
+        }
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != device) cudaSetDevice(device);
+    cudaFree(p);
+    if (cur != device) cudaSetDevice(cur);
+}
+
+// A device buffer that only grows, backed by the block cache.
 struct DevBuf {
     void* p = nullptr;
     size_t cap = 0;
-    ~DevBuf() { if (p) cudaFree(p); }
-    int ensure(size_t bytes) {
-        if (bytes <= cap) return 0;
-        if (p) cudaFree(p);
+    int dev = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    // Owners call this after the device has drained their work.
+    void release() {
+        if (p) cacheGive(dev, p, cap);
         p = nullptr;
         cap = 0;
+    }
+    ~DevBuf() { release(); }
+    int ensure(size_t bytes) {
+        if (bytes <= cap) return 0;
+        if (p) {
+            cudaError_t e = cudaDeviceSynchronize();
+            if (e != cudaSuccess) return fail(VXB_ECUDA, "%s", cudaGetErrorString(e));
+            release();
+        }
+        cudaGetDevice(&dev);
+        size_t got = 0;
+        if ((p = cacheTake(dev, bytes, &got))) {
+            cap = got;
+            return 0;
+        }
         size_t want = bytes + bytes / 8 + 256;
         cudaError_t e = cudaMalloc(&p, want);
         if (e != cudaSuccess) {
             cudaGetLastError();
+            p = nullptr;
             return fail(VXB_ENOMEM, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
         }
         cap = want;
@@ -97,6 +169,7 @@ struct vxb_voxelizer {
     DevBuf dV, dI, dM;
     // scratch
     DevBuf counts, offsets, tileSums, small, codes, splitsBuf, matSplitsBuf, laterFlags, outStage;
+    DevBuf units, perm, buckets, recs, ovl;  // surface pass partition and set-up records
     DevBuf fill[4], surfAll, fin, ranks, rankTiles, hitList, keys;
     uint32_t launches = 0;
     // Optional per-stage CUDA-event timing (vxb_set_profiling): stage k is
@@ -255,23 +328,30 @@ int vxb_voxelizer::surfacePass(const vxb::Plan& p, const vxb::PassGeom& g, int l
                                cudaStream_t s) {
     uint32_t* bits = surfAll.as<uint32_t>() + lattice * gridWords;
     if (mode == 0) VXB_CUDA(cudaMemsetAsync(bits, 0, gridWords * 4, s));
-    std::vector<vxb::Split3> sp;
-    for (const auto& z : p.zMat)
-        for (const auto& y : p.yMat)
-            for (const auto& x : p.xMat) sp.push_back(vxb::Split3{x.lo, x.hi, y.lo, y.hi, z.lo, z.hi});
+    // Material subspace slices per axis (src/host_side.cpp:2301-2337 passes
+    // matSplitRes to the surface launches).
+    std::vector<uint32_t> sl;
+    vxb::SliceTable st;
+    const std::vector<vxb::Range>* axes[3] = {&p.xMat, &p.yMat, &p.zMat};
+    for (int a = 0; a < 3; ++a) {
+        st.off[a] = (uint32_t)(sl.size() / 2);
+        st.n[a] = (uint32_t)axes[a]->size();
+        for (const auto& r : *axes[a]) { sl.push_back(r.lo); sl.push_back(r.hi); }
+    }
     int rc;
-    if ((rc = matSplitsBuf.ensure(sp.size() * sizeof(vxb::Split3) + 64))) return rc;
-    VXB_CUDA(cudaMemcpyAsync(matSplitsBuf.p, sp.data(), sp.size() * sizeof(vxb::Split3), cudaMemcpyHostToDevice, s));
-    uint32_t* cnt = counts.as<uint32_t>();
-    uint32_t* off = offsets.as<uint32_t>();
+    if ((rc = matSplitsBuf.ensure(sl.size() * 4 + 64))) return rc;
+    VXB_CUDA(cudaMemcpyAsync(matSplitsBuf.p, sl.data(), sl.size() * 4, cudaMemcpyHostToDevice, s));
     uint32_t* sm = small.as<uint32_t>();
-    const vxb::Split3* dsp = matSplitsBuf.as<vxb::Split3>();
-    vxb::launch_surface_count(dV.as<float>(), dI.as<uint32_t>(), nT, g, dsp, (uint32_t)sp.size(), codes.as<uint32_t>(),
-                              cnt, s, &launches);
-    vxb::launch_scan(cnt, off, nT, tileSums.as<uint32_t>(), sm + kSurfTotal, sm + kSurfOverflow, s, &launches);
-    vxb::launch_surface_work(mode, nodeType == VXB_PARTIAL_NODE ? 1 : 0, dV.as<float>(), dI.as<uint32_t>(),
-                             dM.as<uint8_t>(), nT, g, dsp, (uint32_t)sp.size(), codes.as<uint32_t>(), off,
-                             sm + kSurfTotal, bits, (uint64_t)lattice * gridWords * 32, ranks.as<uint32_t>(), keys.p,
+    VXB_CUDA(cudaMemsetAsync(buckets.p, 0, 2 * vxb::kSurfaceBuckets * 4, s));
+    VXB_CUDA(cudaMemsetAsync(counts.p, 0, 4 * ((size_t)nT + 1), s));
+    vxb::launch_surface_prepare(dV.as<float>(), dI.as<uint32_t>(), dM.as<uint8_t>(), nT, g, codes.as<uint32_t>(),
+                                units.as<uint32_t>(), buckets.as<uint32_t>(), perm.as<uint32_t>(), counts.as<uint32_t>(),
+                                recs.p, ovl.p, s, &launches);
+    vxb::launch_scan(counts.as<uint32_t>(), offsets.as<uint32_t>(), nT, tileSums.as<uint32_t>(), sm + kSurfTotal,
+                     sm + kSurfOverflow, s, &launches);
+    vxb::launch_surface_work(mode, nodeType == VXB_PARTIAL_NODE ? 1 : 0, recs.p, ovl.p, offsets.as<uint32_t>(), nT,
+                             sm + kSurfTotal, buckets.as<uint32_t>(), g, matSplitsBuf.as<uint32_t>(), st, bits,
+                             (uint64_t)lattice * gridWords * 32, ranks.as<uint32_t>(), keys.p,
                              hitList.as<unsigned long long>(), sm + kHitCount, listCap, s, &launches);
     VXB_CUDA(cudaGetLastError());
     return 0;
@@ -329,6 +409,11 @@ int vxb_voxelizer::run(int nodes, const vxb_request* r, void* dout, uint64_t byt
     const int lattices = isFcc(nodeType) ? 4 : 1;
     if (mats) {
         if ((rc = codes.ensure(4 * (size_t)nT))) return rc;
+        if ((rc = units.ensure(4 * (size_t)nT))) return rc;
+        if ((rc = perm.ensure(4 * (size_t)nT))) return rc;
+        if ((rc = buckets.ensure(4 * 2 * vxb::kSurfaceBuckets))) return rc;
+        if ((rc = recs.ensure(vxb::kSurfRecBytes * (size_t)nT))) return rc;
+        if ((rc = ovl.ensure(vxb::kSurfOvlBytes * (size_t)nT))) return rc;
         if ((rc = surfAll.ensure(gridBytes * lattices))) return rc;
         if ((rc = ranks.ensure(gridBytes * lattices))) return rc;
         if ((rc = rankTiles.ensure(4 * (gridWords * lattices / 2048 + 2)))) return rc;
@@ -485,7 +570,34 @@ vxb_status vxb_create(vxb_voxelizer** out, int node_type, const float* vertices,
 }
 
 vxb_status vxb_destroy(vxb_voxelizer* v) {
+    if (!v) return VXB_OK;
+    // The instance's buffers go back to the block cache: wait for queued
+    // work that may still use them.
+    const int dev = v->device;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != dev) cudaSetDevice(dev);
+    cudaDeviceSynchronize();
     delete v;
+    if (cur != dev) cudaSetDevice(cur);
+    return VXB_OK;
+}
+
+vxb_status vxb_trim_cache(void) {
+    BlockCache& c = blockCache();
+    std::multimap<size_t, std::pair<int, void*>> idle;
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        idle.swap(c.idle);
+        c.idleBytes = 0;
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (auto& e : idle) {
+        cudaSetDevice(e.second.first);
+        cudaFree(e.second.second);
+    }
+    cudaSetDevice(cur);
     return VXB_OK;
 }
 

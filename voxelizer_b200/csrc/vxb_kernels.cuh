@@ -35,19 +35,33 @@ void launch_solid_toggle(const float* V, const uint32_t* I, uint32_t nT, PassGeo
 void launch_row_fill(uint32_t* words, uint32_t rows, uint32_t ipx, cudaStream_t s, uint32_t* launches);
 
 // ---- Surface voxelization: src/voxelizer.cu:2358-2989, 3040-4201 ----
-void launch_surface_count(const float* V, const uint32_t* I, uint32_t nT, PassGeom g, const Split3* splits,
-                          uint32_t nSplits, uint32_t* codes, uint32_t* counts, cudaStream_t s, uint32_t* launches);
-// Surface work, one thread per (triangle, material subspace, column).
-// mode 0: set surface bits in `surfBits` and append (bit position << 24 |
-// key) to `list` (entries past listCap are counted, not stored); mode 1:
-// merge every hit's key at its rank (needs complete bits and `ranks`).
-// posBase is the bit position of surfBits[0] in the rank space (FCC
-// sub-lattices are stacked).  wide: 64-bit keys (PartialNode).
-void launch_surface_work(int mode, int wide, const float* V, const uint32_t* I, const uint8_t* M, uint32_t nT,
-                         PassGeom g, const Split3* splits, uint32_t nSplits, const uint32_t* codes,
-                         const uint32_t* offsets, const uint32_t* total, uint32_t* surfBits, uint64_t posBase,
-                         const uint32_t* ranks, void* keys, unsigned long long* list, uint32_t* listCount,
-                         uint32_t listCap, cudaStream_t s, uint32_t* launches);
+// Triangles with surface work are partitioned into kSurfaceBuckets buckets
+// by (class, axis); each gets a kSurfRecBytes record and a kSurfOvlBytes
+// block of projection edge functions.
+constexpr uint32_t kSurfaceBuckets = 9;
+constexpr size_t kSurfRecBytes = 64;
+constexpr size_t kSurfOvlBytes = 112;
+
+// Material subspace slices along each axis: (lo, hi) pairs, axis a at pair
+// offset off[a], n[a] of them.
+struct SliceTable { uint32_t off[3], n[3]; };
+
+// Classify (codes / units in mesh order, per-bucket counts in buckets[0..9)),
+// partition (perm, unitsP in partitioned order; buckets[9..18) are cursors)
+// and set up (records).  buckets and unitsP[0..nT] must be zero on entry.
+void launch_surface_prepare(const float* V, const uint32_t* I, const uint8_t* M, uint32_t nT, PassGeom g,
+                            uint32_t* codes, uint32_t* units, uint32_t* buckets, uint32_t* perm, uint32_t* unitsP,
+                            void* recs, void* ovl, cudaStream_t s, uint32_t* launches);
+// Surface work over the exclusive scan `offsets` of unitsP (nT + 1 entries),
+// one thread per column.  mode 0: set surface bits in `surfBits` and append
+// (bit position << 24 | key) to `list` (entries past listCap are counted,
+// not stored); mode 1: merge every hit's key at its rank (needs complete
+// bits and `ranks`).  posBase is the bit position of surfBits[0] in the rank
+// space (FCC sub-lattices are stacked).  wide: 64-bit keys (PartialNode).
+void launch_surface_work(int mode, int wide, const void* recs, const void* ovl, const uint32_t* offsets, uint32_t nT,
+                         const uint32_t* total, const uint32_t* buckets, PassGeom g, const uint32_t* slices,
+                         SliceTable st, uint32_t* surfBits, uint64_t posBase, const uint32_t* ranks, void* keys, unsigned long long* list,
+                         uint32_t* listCount, uint32_t listCap, cudaStream_t s, uint32_t* launches);
 // Exclusive popcount prefix over `words` surface words; *total = surface voxels.
 void launch_surface_rank(const uint32_t* bits, uint64_t words, uint32_t* ranks, uint32_t* tileSums, uint32_t* total,
                          cudaStream_t s, uint32_t* launches);

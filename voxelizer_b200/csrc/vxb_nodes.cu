@@ -40,15 +40,17 @@ __global__ void combineKernel(const uint4* __restrict__ a, const uint4* __restri
 __global__ void pruneKernel(uint32_t* solid, const uint32_t* __restrict__ fill, const uint32_t* __restrict__ surf,
                             const uint8_t* __restrict__ yLater, const uint8_t* __restrict__ zLater, PassGeom g,
                             SplitYZ sp, uint32_t* changed) {
+    // Grids hold fewer than 2^32 voxels, so word indices fit 32 bits.
     const uint32_t ny = sp.y1 - sp.y0;
-    const uint64_t nWords = (uint64_t)ny * (sp.z1 - sp.z0) * g.ipx;
-    const size_t plane = (size_t)g.ipx * g.AY;
+    const uint32_t nWords = ny * (sp.z1 - sp.z0) * g.ipx;
+    const uint32_t plane = g.ipx * g.AY;
     bool any = false;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nWords; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t k = (uint32_t)(i % g.ipx);
-        const uint64_t r = i / g.ipx;
-        const uint32_t y = sp.y0 + (uint32_t)(r % ny), z = sp.z0 + (uint32_t)(r / ny);
-        const size_t idx = ((size_t)z * g.AY + y) * g.ipx + k;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nWords; i += gridDim.x * blockDim.x) {
+        const uint32_t r = i / g.ipx;
+        const uint32_t k = i - r * g.ipx;
+        const uint32_t zz = r / ny;
+        const uint32_t y = sp.y0 + (r - zz * ny), z = sp.z0 + zz;
+        const uint32_t idx = (z * g.AY + y) * g.ipx + k;
         const uint32_t w = solid[idx];
         if (w == 0) continue;
         const uint32_t prev = k > 0 ? solid[idx - 1] : 0u;
@@ -92,112 +94,167 @@ struct EmitArgs {
 // grid (its subspace was still unpruned when this one converged), every
 // other neighbour from the final grid.  Pruned surface nodes keep their
 // material (node.bid(0) keeps mat, include/node_types.h).
+
+// The seven words around word w and its coordinates.  Grids hold fewer than
+// 2^32 voxels, so word indices fit 32 bits.
+struct WordNbrs {
+    uint32_t c, s0, f0, L, R, In, Out, Dn, Up;
+};
+
 template <int K>
-__global__ void __launch_bounds__(256) emitCartesianKernel(EmitArgs a) {
+__device__ __forceinline__ WordNbrs loadNbrs(const EmitArgs& a, uint32_t w) {
     typedef NodeT<K> NT;
-    constexpr int WB = 32 * NT::bytes;           // bytes of one word's nodes
+    const PassGeom& g = a.g;
+    WordNbrs n;
+    n.c = __ldg(a.fin + w);
+    n.s0 = a.materials ? __ldg(a.surf + w) : 0u;
+    n.f0 = NT::bytes == 8 ? __ldg(a.fill + w) : 0u;
+    n.L = n.R = n.In = n.Out = n.Dn = n.Up = 0u;
+    if (n.c | n.s0 | n.f0) {
+        const uint32_t row = w / g.ipx;
+        const uint32_t k = w - row * g.ipx;
+        const uint32_t z = row / g.AY, y = row - z * g.AY;
+        const uint32_t plane = g.ipx * g.AY;
+        const uint32_t prev = k > 0 ? __ldg(a.fin + w - 1) : 0u;
+        const uint32_t next = k + 1 < g.ipx ? __ldg(a.fin + w + 1) : 0u;
+        n.L = (n.c >> 1) | (prev << 31);
+        n.R = (n.c << 1) | (next >> 31);
+        n.In = y > 0 ? __ldg(a.fin + w - g.ipx) : 0u;
+        if (y + 1 < g.AY)
+            n.Out = a.yLater[y] ? (__ldg(a.fill + w + g.ipx) | (a.materials ? __ldg(a.surf + w + g.ipx) : 0u))
+                                : __ldg(a.fin + w + g.ipx);
+        n.Dn = z > 0 ? __ldg(a.fin + w - plane) : 0u;
+        if (z + 1 < g.AZ)
+            n.Up = a.zLater[z] ? (__ldg(a.fill + w + plane) | (a.materials ? __ldg(a.surf + w + plane) : 0u))
+                               : __ldg(a.fin + w + plane);
+    }
+    return n;
+}
+
+__device__ __forceinline__ uint32_t permOf(const WordNbrs& n, uint32_t q) {
+    return ((n.L >> q) & 1u) | (((n.R >> q) & 1u) << 1) | (((n.In >> q) & 1u) << 2) | (((n.Out >> q) & 1u) << 3) |
+           (((n.Dn >> q) & 1u) << 4) | (((n.Up >> q) & 1u) << 5);
+}
+
+// 1- and 2-byte nodes.  Each lane owns one word and builds its 32 nodes in
+// its own shared-memory row: nodes whose six neighbours are all solid and
+// that carry no material (id 27) come from a bit expansion, and only the
+// remaining set bits (solid next to empty, surface nodes) are visited one by
+// one.  The warp's 32 rows are then stored as one contiguous span.
+template <int K>
+__global__ void __launch_bounds__(256) emitNarrowKernel(EmitArgs a) {
+    typedef NodeT<K> NT;
+    static_assert(NT::bytes <= 2, "narrow nodes only");
+    constexpr int NB = NT::bytes;
+    constexpr int WB = 32 * NB;                  // bytes of one word's nodes
     constexpr int CH = WB / 16;                  // 16-byte chunks per word
     constexpr int PITCH = (CH + 1) * 16;         // padded smem row (conflict-free)
-    constexpr bool kStaged = NT::bytes <= 2;     // wider nodes store straight from registers
-    __shared__ __align__(16) uint8_t stage[8][kStaged ? 32 * PITCH : 16];
+    __shared__ __align__(16) uint8_t stage[8][32 * PITCH];
     __shared__ uint8_t lut[64];
     if (threadIdx.x < 64) lut[threadIdx.x] = kOrientTable[threadIdx.x];
     __syncthreads();
     const PassGeom& g = a.g;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint64_t nWords = (uint64_t)g.ipx * g.AY * g.AZ;
-    const size_t plane = (size_t)g.ipx * g.AY;
-    uint8_t* my = kStaged ? stage[warp] + lane * PITCH : nullptr;
-    for (uint64_t wbase = ((uint64_t)blockIdx.x * 8 + warp) * 32; wbase < nWords;
-         wbase += (uint64_t)gridDim.x * 8 * 32) {
-        const uint64_t w = wbase + lane;
-        uint4 val[CH];
+    const uint32_t nWords = g.ipx * g.AY * g.AZ;
+    uint8_t* my = stage[warp] + lane * PITCH;
+    const uint32_t v27 = (uint32_t)NT::pack(27u, 0u, 0.0f);
+    for (uint32_t wbase = (blockIdx.x * 8u + warp) * 32u; wbase < nWords; wbase += gridDim.x * 8u * 32u) {
+        const uint32_t w = wbase + lane;
+        WordNbrs n{};
+        if (w < nWords) n = loadNbrs<K>(a, w);
+        const uint32_t interior = n.c & n.L & n.R & n.In & n.Out & n.Dn & n.Up & ~n.s0;
+        uint32_t rest = (n.c & ~interior) | n.s0;
+        uint32_t v[CH * 4];
+        if (interior == 0u) {
 #pragma unroll
-        for (int i = 0; i < CH; ++i) val[i] = make_uint4(0, 0, 0, 0);
-        if (w < nWords) {
-            const uint32_t k = (uint32_t)(w % g.ipx);
-            const uint64_t row = w / g.ipx;
-            const uint32_t y = (uint32_t)(row % g.AY), z = (uint32_t)(row / g.AY);
-            const uint32_t c = __ldg(a.fin + w);
-            const uint32_t s0 = a.materials ? __ldg(a.surf + w) : 0u;
-            const uint32_t f0 = NT::bytes == 8 ? __ldg(a.fill + w) : 0u;
-            if (c | s0 | f0) {
-                const uint32_t prev = k > 0 ? __ldg(a.fin + w - 1) : 0u;
-                const uint32_t next = k + 1 < g.ipx ? __ldg(a.fin + w + 1) : 0u;
-                const uint32_t L = (c >> 1) | (prev << 31), R = (c << 1) | (next >> 31);
-                const uint32_t In = y > 0 ? __ldg(a.fin + w - g.ipx) : 0u;
-                uint32_t Out = 0u, Up = 0u;
-                if (y + 1 < g.AY)
-                    Out = a.yLater[y] ? (__ldg(a.fill + w + g.ipx) | (a.materials ? __ldg(a.surf + w + g.ipx) : 0u))
-                                      : __ldg(a.fin + w + g.ipx);
-                const uint32_t Dn = z > 0 ? __ldg(a.fin + w - plane) : 0u;
-                if (z + 1 < g.AZ)
-                    Up = a.zLater[z] ? (__ldg(a.fill + w + plane) | (a.materials ? __ldg(a.surf + w + plane) : 0u))
-                                     : __ldg(a.fin + w + plane);
-                const uint32_t full = c & L & R & In & Out & Dn & Up;
-                if (full == 0xFFFFFFFFu && s0 == 0u && NT::bytes != 8) {
-                    // All 32 nodes interior: id 27, material 0.
-                    const uint64_t v27 = NT::pack(27u, 0u, 0.0f);
-                    uint32_t rep;
-                    if (NT::bytes == 1) rep = (uint32_t)v27 * 0x01010101u;
-                    else if (NT::bytes == 2) rep = (uint32_t)v27 * 0x00010001u;
-                    else rep = (uint32_t)v27;
+            for (int i = 0; i < CH * 4; ++i) v[i] = 0u;
+        } else if (interior == 0xFFFFFFFFu) {
+            const uint32_t rep = NB == 1 ? v27 * 0x01010101u : v27 * 0x00010001u;
 #pragma unroll
-                    for (int i = 0; i < CH; ++i) val[i] = make_uint4(rep, rep, rep, rep);
-                } else {
-                    uint32_t matRank = 0;
-                    if (s0) matRank = __ldg(a.ranks + w);
-                    uint32_t* v32 = reinterpret_cast<uint32_t*>(val);
+            for (int i = 0; i < CH * 4; ++i) v[i] = rep;
+        } else {
 #pragma unroll
-                    for (int b = 0; b < 32; ++b) {
-                        const uint32_t q = 31u - b;
-                        uint32_t bid = 0;
-                        if ((c >> q) & 1u) {
-                            const uint32_t perm = ((L >> q) & 1u) | (((R >> q) & 1u) << 1) | (((In >> q) & 1u) << 2) |
-                                                  (((Out >> q) & 1u) << 3) | (((Dn >> q) & 1u) << 4) |
-                                                  (((Up >> q) & 1u) << 5);
-                            bid = lut[perm];
-                        }
-                        uint32_t mat = 0;
-                        if ((s0 >> q) & 1u) {
-                            const uint64_t key = NT::bytes == 8
-                                                     ? reinterpret_cast<const unsigned long long*>(a.keys)[matRank]
-                                                     : reinterpret_cast<const uint32_t*>(a.keys)[matRank];
-                            mat = NT::keyMat(key);
-                            ++matRank;
-                        }
-                        const float r = ((f0 >> q) & 1u) && !((s0 >> q) & 1u) ? 1.0f : 0.0f;
-                        const uint64_t nv = NT::pack(bid, mat, r);
-                        if (NT::bytes == 1) {
-                            v32[b >> 2] |= (uint32_t)(nv & 0xFFu) << ((b & 3) * 8);
-                        } else if (NT::bytes == 2) {
-                            v32[b >> 1] |= (uint32_t)(nv & 0xFFFFu) << ((b & 1) * 16);
-                        } else {
-                            v32[2 * b] = (uint32_t)nv;
-                            v32[2 * b + 1] = (uint32_t)(nv >> 32);
-                        }
-                    }
+            for (int i = 0; i < CH * 4; ++i) {
+                uint32_t x = 0u;
+#pragma unroll
+                for (int j = 0; j < 4 / NB; ++j) {
+                    const uint32_t b = (uint32_t)(i * (4 / NB) + j);
+                    x |= ((interior >> (31u - b)) & 1u) * (v27 << (8 * NB * j));
                 }
+                v[i] = x;
             }
         }
-        if constexpr (kStaged) {
-            // Stage the warp's 32 words and store them as contiguous rows.
 #pragma unroll
-            for (int i = 0; i < CH; ++i) *reinterpret_cast<uint4*>(my + 16 * i) = val[i];
-            __syncwarp();
-            const uint64_t wend = wbase + 32 <= nWords ? 32 : nWords - wbase;
-            uint4* out = reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(a.nodes) + wbase * WB);
+        for (int i = 0; i < CH; ++i)
+            *reinterpret_cast<uint4*>(my + 16 * i) = make_uint4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+        if (rest) {
+            const uint32_t rank0 = n.s0 ? __ldg(a.ranks + w) : 0u;
+            do {
+                const uint32_t b = __clz(rest);        // node index in the word
+                const uint32_t q = 31u - b;           // its bit
+                uint32_t bid = 0u, mat = 0u;
+                if ((n.c >> q) & 1u) bid = lut[permOf(n, q)];
+                if ((n.s0 >> q) & 1u) {
+                    const uint32_t r = rank0 + (b ? __popc(n.s0 >> (32u - b)) : 0u);
+                    mat = NT::keyMat(reinterpret_cast<const uint32_t*>(a.keys)[r]);
+                }
+                const uint32_t nv = (uint32_t)NT::pack(bid, mat, 0.0f);
+                if (NB == 1) my[b] = (uint8_t)nv;
+                else reinterpret_cast<uint16_t*>(my)[b] = (uint16_t)nv;
+                rest &= ~(0x80000000u >> b);
+            } while (rest);
+        }
+        __syncwarp();
+        const uint32_t wend = wbase + 32u <= nWords ? 32u : nWords - wbase;
+        uint4* out = reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(a.nodes) + (size_t)wbase * WB);
 #pragma unroll
-            for (int i = 0; i < CH; ++i) {
-                const uint32_t chunk = i * 32 + lane;       // 16-byte chunk of the warp's span
-                const uint32_t wi = chunk / CH, ci = chunk % CH;
-                if (wi < wend) out[chunk] = *reinterpret_cast<const uint4*>(stage[warp] + wi * PITCH + 16 * ci);
+        for (int i = 0; i < CH; ++i) {
+            const uint32_t chunk = i * 32 + lane;       // 16-byte chunk of the warp's span
+            const uint32_t wi = chunk / CH, ci = chunk % CH;
+            if (wi < wend) out[chunk] = *reinterpret_cast<const uint4*>(stage[warp] + wi * PITCH + 16 * ci);
+        }
+        __syncwarp();
+    }
+}
+
+// 8-byte PartialNodes: one lane per word, nodes stored from registers.  The
+// ratio of a node is 1 where the parity fill is set and the node is not a
+// surface node.
+__global__ void __launch_bounds__(256) emitPartialKernel(EmitArgs a) {
+    typedef NodeT<kPartial> NT;
+    __shared__ uint8_t lut[64];
+    if (threadIdx.x < 64) lut[threadIdx.x] = kOrientTable[threadIdx.x];
+    __syncthreads();
+    const PassGeom& g = a.g;
+    const uint32_t nWords = g.ipx * g.AY * g.AZ;
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < nWords; w += gridDim.x * blockDim.x) {
+        const WordNbrs n = loadNbrs<kPartial>(a, w);
+        uint4* out = reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(a.nodes) + (size_t)w * 32 * 8);
+        if ((n.c | n.s0 | n.f0) == 0u) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) out[i] = make_uint4(0, 0, 0, 0);
+            continue;
+        }
+        const uint32_t rank0 = n.s0 ? __ldg(a.ranks + w) : 0u;
+        uint32_t matRank = rank0;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            uint32_t v32[4];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const uint32_t b = 2 * i + j, q = 31u - b;
+                uint32_t bid = 0, mat = 0;
+                if ((n.c >> q) & 1u) bid = lut[permOf(n, q)];
+                if ((n.s0 >> q) & 1u) {
+                    mat = NT::keyMat(reinterpret_cast<const unsigned long long*>(a.keys)[matRank]);
+                    ++matRank;
+                }
+                const float r = ((n.f0 >> q) & 1u) && !((n.s0 >> q) & 1u) ? 1.0f : 0.0f;
+                const uint64_t nv = NT::pack(bid, mat, r);
+                v32[2 * j] = (uint32_t)nv;
+                v32[2 * j + 1] = (uint32_t)(nv >> 32);
             }
-            __syncwarp();
-        } else if (w < nWords) {
-            uint4* out = reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(a.nodes) + w * WB);
-#pragma unroll
-            for (int i = 0; i < CH; ++i) out[i] = val[i];
+            out[i] = make_uint4(v32[0], v32[1], v32[2], v32[3]);
         }
     }
 }
@@ -322,9 +379,9 @@ void launch_emit_cartesian(int nodeKind, const uint32_t* finalSolid, const uint3
     const uint64_t words = (uint64_t)g.ipx * g.AY * g.AZ;
     const uint32_t grid = gridFor(words, 256, 148u * 16u);
     switch (nodeKind) {
-    case kShort: emitCartesianKernel<kShort><<<grid, 256, 0, s>>>(a); break;
-    case kLong: emitCartesianKernel<kLong><<<grid, 256, 0, s>>>(a); break;
-    default: emitCartesianKernel<kPartial><<<gridFor(words, 256, 148u * 8u), 256, 0, s>>>(a); break;
+    case kShort: emitNarrowKernel<kShort><<<grid, 256, 0, s>>>(a); break;
+    case kLong: emitNarrowKernel<kLong><<<grid, 256, 0, s>>>(a); break;
+    default: emitPartialKernel<<<gridFor(words, 256, 148u * 8u), 256, 0, s>>>(a); break;
     }
     *launches += 1;
 }

@@ -2,12 +2,21 @@
 // / encodeTriangleType (src/voxelizer.cu:3040-3221) and the 1D / 2D / 3D
 // processing kernels (3306-3955) with processVoxel (2946-2989).
 //
-// Work is a flat list of (triangle, material subspace, column) items over an
-// exclusive scan of per-triangle column counts, one thread per column (per
-// voxel of a 1D line).  A block stages the triangles its 256 items belong to
-// in shared memory first: vertices, class code, voxel box, normal and the
-// edge functions of the three projections are computed once per triangle,
-// not once per column.
+// Per pass: classify every triangle (class, dominant axis, voxel box clamped
+// to the grid, work units), partition the triangles with work by (class,
+// axis) as the reference's sort by triangle type does, write one set-up
+// record per partitioned triangle (box, normal, the edge functions of the
+// projections it tests), scan the unit counts and run the work list: one
+// thread per column of the dominant projection (per voxel of a 1D line).
+// Warps find the triangle of each of their 32 items with one coalesced load
+// of 32 offsets, so the work kernel has no block-wide barrier.
+//
+// The reference runs the surface kernels once per material subspace on
+// boxes clamped to it.  Subspaces tile the grid, so the columns of the
+// grid-clamped box are the union of the subspaces' columns; along the depth
+// axis a column still visits each subspace's slice separately, because the
+// single-voxel shortcut (no further tests when the clamped depth range is
+// one voxel) depends on the slice.
 //
 // Hits set the voxel's bit in the surface grid and append (bit position,
 // material key) to a hit list.  Once all surface bits exist, every surface
@@ -29,7 +38,9 @@ using namespace detail;
 namespace {
 
 constexpr int kBlock = 256;
-constexpr uint32_t kSlots = 144;  // staged triangles per block (27 KB of shared memory)
+constexpr uint32_t kFull = 0xffffffffu;
+constexpr uint32_t kBatch = 16;  // 32-item chunks per owner search
+constexpr uint32_t kNone = 0xFFu;
 
 __device__ __forceinline__ void loadTriF(const float* __restrict__ V, const uint32_t* __restrict__ I, uint32_t t,
                                          F3* v) {
@@ -72,79 +83,135 @@ __device__ __forceinline__ IBox voxBoundsHalf(const F3* v, const PassGeom& g) {
     return b;
 }
 
-__device__ __forceinline__ uint32_t classifyTri(const F3* v, const PassGeom& g) {
+// Class (bits 30-31: 0 degenerate, 1 / 2 / 3 for 1D / 2D / 3D boxes) and
+// axis (bits 28-29: the line's axis for 1D, the flat axis for 2D, the
+// dominant normal axis for 3D) of a triangle, from its unclamped box.
+__device__ __forceinline__ uint32_t classifyTri(const F3* v, const IBox& b) {
     const F3 n = crossF<site::CRF_CLS>(subF(v[0], v[2]), subF(v[1], v[0]));
     if (!(n.x != 0.0f || n.y != 0.0f || n.z != 0.0f)) return 0u;
-    const IBox b = voxBoundsHalf(v, g);
     const int dx = b.hi[0] - b.lo[0], dy = b.hi[1] - b.lo[1], dz = b.hi[2] - b.lo[2];
-    uint32_t bb, axis, cols;
+    uint32_t bb, axis;
     if (dx == 0) {
-        if (dy == 0) {
-            if (dz == 0) { bb = 1; axis = 0; cols = 1; }
-            else { bb = 1; axis = 2; cols = (uint32_t)dz; }
-        } else if (dz == 0) { bb = 1; axis = 1; cols = (uint32_t)dy; }
-        else { bb = 2; axis = 0; cols = (uint32_t)(dy * dz); }
+        if (dy == 0) { bb = 1; axis = dz == 0 ? 0 : 2; }
+        else if (dz == 0) { bb = 1; axis = 1; }
+        else { bb = 2; axis = 0; }
     } else if (dy == 0) {
-        if (dz == 0) { bb = 1; axis = 0; cols = (uint32_t)dx; }
-        else { bb = 2; axis = 1; cols = (uint32_t)(dx * dz); }
-    } else if (dz == 0) { bb = 2; axis = 2; cols = (uint32_t)(dx * dy); }
+        if (dz == 0) { bb = 1; axis = 0; }
+        else { bb = 2; axis = 1; }
+    } else if (dz == 0) { bb = 2; axis = 2; }
     else {
         bb = 3;
         const float ax = fabsf(n.x), ay = fabsf(n.y), az = fabsf(n.z);
         if (ax > ay && ax > az) axis = 0;
         else if (ay > ax && ay > az) axis = 1;
         else axis = 2;
-        cols = axis == 0 ? (uint32_t)(dy * dz) : axis == 1 ? (uint32_t)(dx * dz) : (uint32_t)(dx * dy);
     }
-    return cols | (axis << 28) | (bb << 30);
+    return (axis << 28) | (bb << 30);
 }
 
-// adjustVoxelRange, src/voxelizer.cu:3963-3993.
-__device__ __forceinline__ bool clampBox(IBox& b, const Split3& s) {
-    const int lo[3] = {(int)s.x0, (int)s.y0, (int)s.z0};
-    const int hi[3] = {(int)s.x1 - 1, (int)s.y1 - 1, (int)s.z1 - 1};
-    if (lo[0] > b.hi[0] || lo[1] > b.hi[1] || lo[2] > b.hi[2]) return false;
-    if (b.lo[0] > hi[0] || b.lo[1] > hi[1] || b.lo[2] > hi[2]) return false;
+// The box clamped to the grid, i.e. to the union of the material subspaces
+// (adjustVoxelRange, src/voxelizer.cu:3963-3993, over all of them).
+__device__ __forceinline__ IBox gridClamp(IBox b, const PassGeom& g) {
+    const int hi[3] = {(int)g.X - 1, (int)g.resY - 1, (int)g.resZ - 1};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        b.lo[a] = max(b.lo[a], lo[a]);
+        b.lo[a] = max(b.lo[a], 0);
         b.hi[a] = min(b.hi[a], hi[a]);
     }
-    return true;
+    return b;
 }
 
-// Work units of one (triangle, material subspace): voxels along the axis for
-// 1D boxes, columns of the dominant projection otherwise.
+// Work units: voxels along the axis for 1D boxes, columns of the dominant
+// projection otherwise; 0 for an empty (fully outside) box.
 __device__ __forceinline__ uint32_t surfUnits(const IBox& b, uint32_t code) {
+    if (b.lo[0] > b.hi[0] || b.lo[1] > b.hi[1] || b.lo[2] > b.hi[2]) return 0u;
     const uint32_t bb = code >> 30, axis = (code >> 28) & 3u;
     const uint32_t ex = (uint32_t)(b.hi[0] - b.lo[0] + 1), ey = (uint32_t)(b.hi[1] - b.lo[1] + 1),
                    ez = (uint32_t)(b.hi[2] - b.lo[2] + 1);
+    if (bb == 0) return 0u;
     if (bb == 1) return axis == 0 ? ex : axis == 1 ? ey : ez;
     return axis == 0 ? ey * ez : axis == 1 ? ex * ez : ex * ey;
 }
 
-__global__ void surfaceCountKernel(const float* __restrict__ V, const uint32_t* __restrict__ I, uint32_t nT,
-                                   PassGeom g, const Split3* __restrict__ splits, uint32_t nSplits,
-                                   uint32_t* __restrict__ codes, uint32_t* __restrict__ counts) {
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nT; t += gridDim.x * blockDim.x) {
-        F3 v[3];
-        loadTriF(V, I, t, v);
-        const uint32_t code = classifyTri(v, g);
-        codes[t] = code;
-        uint32_t c = 0;
-        if ((code >> 30) != 0) {
+__device__ __forceinline__ uint32_t bucketOf(uint32_t code, uint32_t units) {
+    return units ? ((code >> 30) - 1u) * 3u + ((code >> 28) & 3u) : kNone;
+}
+
+// Pass 1 (mesh order): code and units per triangle, triangles per bucket.
+__global__ void surfaceClassifyKernel(const float* __restrict__ V, const uint32_t* __restrict__ I, uint32_t nT,
+                                      PassGeom g, uint32_t* __restrict__ codes, uint32_t* __restrict__ units,
+                                      uint32_t* __restrict__ bucketCount) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < nT; base += stride) {
+        const uint32_t t = base + lane;
+        uint32_t code = 0, u = 0;
+        if (t < nT) {
+            F3 v[3];
+            loadTriF(V, I, t, v);
             const IBox full = voxBoundsHalf(v, g);
-            for (uint32_t s = 0; s < nSplits; ++s) {
-                IBox b = full;
-                if (!clampBox(b, splits[s])) continue;
-                c += surfUnits(b, code);
-            }
+            code = classifyTri(v, full);
+            u = surfUnits(gridClamp(full, g), code);
+            codes[t] = code;
+            units[t] = u;
         }
-        counts[t] = c;
+        const uint32_t b = bucketOf(code, u);
+        const uint32_t peers = __match_any_sync(kFull, b);
+        if (b != kNone && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(bucketCount + b, (uint32_t)__popc(peers));
+    }
+}
+
+// Pass 2 (mesh order): position of every triangle with work in the
+// partitioned order; unitsP holds its units there (zero past the end).
+__global__ void surfaceScatterKernel(const uint32_t* __restrict__ codes, const uint32_t* __restrict__ units,
+                                     uint32_t nT, const uint32_t* __restrict__ bucketCount,
+                                     uint32_t* __restrict__ bucketCursor, uint32_t* __restrict__ perm,
+                                     uint32_t* __restrict__ unitsP) {
+    __shared__ uint32_t bucketBase[kSurfaceBuckets];
+    if (threadIdx.x < kSurfaceBuckets) {
+        uint32_t s = 0;
+        for (uint32_t k = 0; k < threadIdx.x; ++k) s += bucketCount[k];
+        bucketBase[threadIdx.x] = s;
+    }
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < nT; base += stride) {
+        const uint32_t t = base + lane;
+        const uint32_t u = t < nT ? __ldg(units + t) : 0u;
+        const uint32_t b = t < nT ? bucketOf(__ldg(codes + t), u) : kNone;
+        const uint32_t peers = __match_any_sync(kFull, b);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t start = 0;
+        if (b != kNone && lane == leader) start = atomicAdd(bucketCursor + b, (uint32_t)__popc(peers));
+        start = __shfl_sync(kFull, start, leader);
+        if (b != kNone) {
+            const uint32_t pos = bucketBase[b] + start + __popc(peers & laneMaskLt());
+            perm[pos] = t;
+            unitsP[pos] = u;
+        }
     }
 }
 
 struct Overlap { float nx[3], ny[3], de[3]; };
+
+// Set-up record of one partitioned triangle (64 bytes) and its projection
+// edge functions (o[axis] for 2D boxes, all three for 3D boxes).
+struct __align__(16) SurfRec {
+    int lo[3], hi[3];   // voxel box clamped to the grid
+    uint32_t code;      // class << 30 | axis << 28
+    uint32_t key;       // class << 8 | material
+    uint32_t tri;       // mesh index (PartialNode keys)
+    float v0[3];        // first vertex (3D depth range)
+    float n[3];         // normal (3D depth range)
+    uint32_t pad;
+};
+struct __align__(16) SurfOvl {
+    Overlap o[3];
+    uint32_t pad;
+};
+static_assert(sizeof(SurfRec) == kSurfRecBytes, "record size");
+static_assert(sizeof(SurfOvl) == kSurfOvlBytes, "record size");
 
 // Per-edge contraction modes: the three edge expressions of a test are
 // separate (unrolled) expressions in the reference, so a site's mode packs
@@ -184,15 +251,60 @@ template <int OT> __device__ __forceinline__ bool overlapTest(const Overlap& o, 
     return r;
 }
 
+// Pass 3 (partitioned order): the set-up record of every triangle with work.
+__global__ void surfaceSetupKernel(const float* __restrict__ V, const uint32_t* __restrict__ I,
+                                   const uint8_t* __restrict__ M, const uint32_t* __restrict__ perm,
+                                   const uint32_t* __restrict__ codes, const uint32_t* __restrict__ bucketCount,
+                                   PassGeom g, SurfRec* __restrict__ recs, SurfOvl* __restrict__ ovl) {
+    uint32_t nP = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < kSurfaceBuckets; ++k) nP += __ldg(bucketCount + k);
+    for (uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x; pos < nP; pos += gridDim.x * blockDim.x) {
+        const uint32_t t = __ldg(perm + pos);
+        F3 v[3];
+        loadTriF(V, I, t, v);
+        const uint32_t code = __ldg(codes + t);
+        const uint32_t bb = code >> 30, axis = (code >> 28) & 3u;
+        const IBox b = gridClamp(voxBoundsHalf(v, g), g);
+        SurfRec r;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) { r.lo[a] = b.lo[a]; r.hi[a] = b.hi[a]; }
+        r.code = code;
+        r.key = (bb << 8) | (M ? __ldg(M + t) : 0u);
+        r.tri = t;
+        r.v0[0] = v[0].x; r.v0[1] = v[0].y; r.v0[2] = v[0].z;
+        r.n[0] = r.n[1] = r.n[2] = 0.0f;
+        r.pad = 0;
+        const float d = g.df;
+        if (bb == 2) {
+            const F3 n = crossF<site::CRF_2D>(subF(v[0], v[2]), subF(v[1], v[0]));
+            r.n[0] = n.x; r.n[1] = n.y; r.n[2] = n.z;
+            if (axis == 0) ovl[pos].o[0] = setupOverlap<0, site::DE_2D_YZ>(v, n, d);
+            else if (axis == 1) ovl[pos].o[1] = setupOverlap<1, site::DE_2D_ZX>(v, n, d);
+            else ovl[pos].o[2] = setupOverlap<2, site::DE_2D_XY>(v, n, d);
+        } else if (bb == 3) {
+            const F3 n = crossF<site::CRF_3D>(subF(v[0], v[2]), subF(v[1], v[0]));
+            r.n[0] = n.x; r.n[1] = n.y; r.n[2] = n.z;
+            SurfOvl o;
+            o.o[0] = setupOverlap<0, site::DE_3D_YZ>(v, n, d);
+            o.o[1] = setupOverlap<1, site::DE_3D_ZX>(v, n, d);
+            o.o[2] = setupOverlap<2, site::DE_3D_XY>(v, n, d);
+            o.pad = 0;
+            ovl[pos] = o;
+        }
+        recs[pos] = r;
+    }
+}
+
 // getSingleVoxelBoundsComponent, src/voxelizer.cu:2575-2586.
 template <int M> __device__ __forceinline__ float vbComp(int c, float m, float d) {
     return linf<M>(__fsub_rn((float)c, 0.5f), d, m);
 }
 
 // determineDepthRange{X,Y,Z} (src/voxelizer.cu:3994-4119) with
-// intersectWithPlane* and boundsCheck.
-template <int A, int DT> __device__ __forceinline__ void depthRange(const F3* t, F3 p, F3 n, const PassGeom& g,
-                                                                    int& lo, int& hi) {
+// intersectWithPlane* and boundsCheck; t0 is the triangle's first vertex.
+template <int A, int DT> __device__ __forceinline__ void depthRange(F3 t0, F3 p, F3 n, const PassGeom& g, int& lo,
+                                                                    int& hi) {
     const float d = g.df;
     F3 pmin, pmax;
     float a, b;
@@ -200,21 +312,21 @@ template <int A, int DT> __device__ __forceinline__ void depthRange(const F3* t,
         const float sy = n.y > 0.0f ? 1.0f : 0.0f, sz = n.z > 0.0f ? 1.0f : 0.0f;
         pmin = F3{0.0f, __fadd_rn(p.y, __fmul_rn(sy, d)), __fadd_rn(p.z, __fmul_rn(sz, d))};
         pmax = F3{0.0f, __fadd_rn(p.y, __fmul_rn(1.0f - sy, d)), __fadd_rn(p.z, __fmul_rn(1.0f - sz, d))};
-        const F3 u = subF(t[0], pmin), w = subF(t[0], pmax);
+        const F3 u = subF(t0, pmin), w = subF(t0, pmax);
         a = __fdiv_rn(sum3f<DT>(u.x, n.x, u.y, n.y, u.z, n.z), n.x);
         b = __fdiv_rn(sum3f<DT>(w.x, n.x, w.y, n.y, w.z, n.z), n.x);
     } else if (A == 1) {
         const float sx = n.x > 0.0f ? 1.0f : 0.0f, sz = n.z > 0.0f ? 1.0f : 0.0f;
         pmin = F3{__fadd_rn(p.x, __fmul_rn(sx, d)), 0.0f, __fadd_rn(p.z, __fmul_rn(sz, d))};
         pmax = F3{__fadd_rn(p.x, __fmul_rn(1.0f - sx, d)), 0.0f, __fadd_rn(p.z, __fmul_rn(1.0f - sz, d))};
-        const F3 u = subF(t[0], pmin), w = subF(t[0], pmax);
+        const F3 u = subF(t0, pmin), w = subF(t0, pmax);
         a = __fdiv_rn(sum3f<DT>(u.x, n.x, u.y, n.y, u.z, n.z), n.y);
         b = __fdiv_rn(sum3f<DT>(w.x, n.x, w.y, n.y, w.z, n.z), n.y);
     } else {
         const float sx = n.x > 0.0f ? 1.0f : 0.0f, sy = n.y > 0.0f ? 1.0f : 0.0f;
         pmin = F3{__fadd_rn(p.x, __fmul_rn(sx, d)), __fadd_rn(p.y, __fmul_rn(sy, d)), 0.0f};
         pmax = F3{__fadd_rn(p.x, __fmul_rn(1.0f - sx, d)), __fadd_rn(p.y, __fmul_rn(1.0f - sy, d)), 0.0f};
-        const F3 u = subF(t[0], pmin), w = subF(t[0], pmax);
+        const F3 u = subF(t0, pmin), w = subF(t0, pmax);
         a = __fdiv_rn(sum3f<DT>(u.x, n.x, u.y, n.y, u.z, n.z), n.z);
         b = __fdiv_rn(sum3f<DT>(w.x, n.x, w.y, n.y, w.z, n.z), n.z);
     }
@@ -224,39 +336,15 @@ template <int A, int DT> __device__ __forceinline__ void depthRange(const F3* t,
     hi = __float2int_rz(floorf(__fadd_rn(__fdiv_rn(__fsub_rn(b, m), d), 0.5f)));
 }
 
-// Triangle setup shared by the columns of a block.
-struct TriStage {
-    F3 v[3];
-    F3 n;
-    IBox full;
-    uint32_t code;
-    uint32_t key;      // class << 8 | material (32-bit key types)
-    uint32_t tri;
-    Overlap o[3];
+// Hits of one warp staged in shared memory before they go to the global
+// hit list, so that the list takes one atomic per flush instead of one per
+// hit.
+constexpr uint32_t kStageHits = 256;
+constexpr uint32_t kFlushAt = kStageHits - 96;
+struct WarpStage {
+    unsigned long long* buf;
+    uint32_t* count;
 };
-
-__device__ __forceinline__ void stageTriangle(TriStage& st, const float* V, const uint32_t* I, const uint8_t* M,
-                                              const uint32_t* codes, uint32_t t, const PassGeom& g) {
-    loadTriF(V, I, t, st.v);
-    st.code = __ldg(codes + t);
-    st.tri = t;
-    st.full = voxBoundsHalf(st.v, g);
-    const uint32_t bb = st.code >> 30;
-    st.key = (bb << 8) | __ldg(M + t);
-    const float d = g.df;
-    if (bb == 2) {
-        st.n = crossF<site::CRF_2D>(subF(st.v[0], st.v[2]), subF(st.v[1], st.v[0]));
-        const uint32_t axis = (st.code >> 28) & 3u;
-        if (axis == 0) st.o[0] = setupOverlap<0, site::DE_2D_YZ>(st.v, st.n, d);
-        else if (axis == 1) st.o[1] = setupOverlap<1, site::DE_2D_ZX>(st.v, st.n, d);
-        else st.o[2] = setupOverlap<2, site::DE_2D_XY>(st.v, st.n, d);
-    } else if (bb == 3) {
-        st.n = crossF<site::CRF_3D>(subF(st.v[0], st.v[2]), subF(st.v[1], st.v[0]));
-        st.o[0] = setupOverlap<0, site::DE_3D_YZ>(st.v, st.n, d);
-        st.o[1] = setupOverlap<1, site::DE_3D_ZX>(st.v, st.n, d);
-        st.o[2] = setupOverlap<2, site::DE_3D_XY>(st.v, st.n, d);
-    }
-}
 
 // processVoxel of the surface pass, coordinates with the 1-voxel padding.
 // mode 0: set the bit and append (bit position << 24 | key) to the hit list;
@@ -272,22 +360,22 @@ struct Sink {
     int mode;
     int wide;                // 64-bit keys (PartialNode)
     PassGeom g;
-    __device__ __forceinline__ void operator()(int xi, int yi, int zi, uint64_t key) const {
+    __device__ __forceinline__ void operator()(int xi, int yi, int zi, uint64_t key, const WarpStage& ws) const {
         const uint32_t x = (uint32_t)xi, y = (uint32_t)yi, z = (uint32_t)zi;
         const size_t w = ((size_t)z * g.AY + y) * g.ipx + (x >> 5);
         const uint32_t b = x & 31u;
         const uint32_t bit = 0x80000000u >> b;
         if (mode == 0) {
             atomicOr(bits + w, bit);
-            const uint32_t active = __activemask();
-            const uint32_t lane = threadIdx.x & 31u;
-            const uint32_t leader = __ffs(active) - 1;
-            uint32_t base = 0;
-            if (lane == leader) base = atomicAdd(listCount, (uint32_t)__popc(active));
-            base = __shfl_sync(active, base, leader);
-            const uint32_t at = base + __popc(active & laneMaskLt());
-            if (at < listCap)
-                list[at] = ((unsigned long long)(posBase + (uint64_t)w * 32 + b) << 24) | (key & 0xFFFFFFull);
+            const unsigned long long e = ((unsigned long long)(posBase + (uint64_t)w * 32 + b) << 24) |
+                                         (key & 0xFFFFFFull);
+            const uint32_t at = atomicAdd(ws.count, 1u);
+            if (at < kStageHits) {
+                ws.buf[at] = e;
+            } else {
+                const uint32_t gat = atomicAdd(listCount, 1u);
+                if (gat < listCap) list[gat] = e;
+            }
         } else {
             const uint32_t word = __ldg(bits + w);
             const uint32_t r = __ldg(wordRank + (posBase >> 5) + w) + (b ? __popc(word >> (32 - b)) : 0u);
@@ -295,161 +383,204 @@ struct Sink {
             else atomicMax(reinterpret_cast<uint32_t*>(keys) + r, (uint32_t)key);
         }
     }
+    // Moves the warp's staged hits to the global list (whole warp, converged).
+    __device__ __forceinline__ void flush(const WarpStage& ws, uint32_t lane) const {
+        __syncwarp();
+        const uint32_t n = min(*ws.count, kStageHits);
+        uint32_t base = 0;
+        if (lane == 0 && n) base = atomicAdd(listCount, n);
+        base = __shfl_sync(kFull, base, 0);
+        for (uint32_t i = lane; i < n; i += 32u)
+            if (base + i < listCap) list[base + i] = ws.buf[i];
+        __syncwarp();
+        if (lane == 0) *ws.count = 0;
+        __syncwarp();
+    }
 };
 
-// Columns of one staged triangle (process1D/2D/3DTriangles).
-__device__ __forceinline__ void surfaceColumn(const TriStage& st, const IBox& b, uint32_t u, const PassGeom& g,
-                                              uint64_t key, const Sink& sink) {
-    const uint32_t bb = st.code >> 30, axis = (st.code >> 28) & 3u;
+// One column (one voxel for 1D boxes) of a partitioned triangle
+// (process1D/2D/3DTriangles).  xr / yr / zr: the material subspace slices
+// along each axis ((lo, hi) pairs).
+__device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const SurfRec& r, const Overlap& od,
+                                            const SurfOvl* __restrict__ ov, uint32_t u, const PassGeom& g,
+                                            const uint32_t* __restrict__ slices, const uint32_t* sliceOff,
+                                            const uint32_t* sliceN, uint64_t key, const Sink& sink,
+                                            const WarpStage& ws) {
     const float d = g.df;
-    const uint32_t ex = (uint32_t)(b.hi[0] - b.lo[0] + 1), ey = (uint32_t)(b.hi[1] - b.lo[1] + 1);
-    const F3* v = st.v;
+    const uint32_t ex = (uint32_t)(r.hi[0] - r.lo[0] + 1), ey = (uint32_t)(r.hi[1] - r.lo[1] + 1);
     if (bb == 1) {
         // process1DTriangles (3306-3411): every voxel of the line, no test.
-        if (axis == 0) sink(b.lo[0] + (int)u + 1, b.lo[1] + 1, b.lo[2] + 1, key);
-        else if (axis == 1) sink(b.lo[0] + 1, b.lo[1] + (int)u + 1, b.lo[2] + 1, key);
-        else sink(b.lo[0] + 1, b.lo[1] + 1, b.lo[2] + (int)u + 1, key);
+        if (axis == 0) sink(r.lo[0] + (int)u + 1, r.lo[1] + 1, r.lo[2] + 1, key, ws);
+        else if (axis == 1) sink(r.lo[0] + 1, r.lo[1] + (int)u + 1, r.lo[2] + 1, key, ws);
+        else sink(r.lo[0] + 1, r.lo[1] + 1, r.lo[2] + (int)u + 1, key, ws);
         return;
     }
     if (bb == 2) {
         // process2DTriangles (3418-3596): the dominant projection only.
         if (axis == 0) {
-            const int j = b.lo[1] + (int)(u % ey), k = b.lo[2] + (int)(u / ey);
-            if (overlapTest<site::OT_2D_YZ>(st.o[0], vbComp<site::PC_2D>(j, g.mnf[1], d), vbComp<site::PC_2D>(k, g.mnf[2], d)))
-                sink(b.lo[0] + 1, j + 1, k + 1, key);
+            const int j = r.lo[1] + (int)(u % ey), k = r.lo[2] + (int)(u / ey);
+            if (overlapTest<site::OT_2D_YZ>(od, vbComp<site::PC_2D>(j, g.mnf[1], d),
+                                            vbComp<site::PC_2D>(k, g.mnf[2], d)))
+                sink(r.lo[0] + 1, j + 1, k + 1, key, ws);
         } else if (axis == 1) {
-            const int i = b.lo[0] + (int)(u % ex), k = b.lo[2] + (int)(u / ex);
-            if (overlapTest<site::OT_2D_ZX>(st.o[1], vbComp<site::PC_2D>(k, g.mnf[2], d), vbComp<site::PC_2D>(i, g.mnf[0], d)))
-                sink(i + 1, b.lo[1] + 1, k + 1, key);
+            const int i = r.lo[0] + (int)(u % ex), k = r.lo[2] + (int)(u / ex);
+            if (overlapTest<site::OT_2D_ZX>(od, vbComp<site::PC_2D>(k, g.mnf[2], d),
+                                            vbComp<site::PC_2D>(i, g.mnf[0], d)))
+                sink(i + 1, r.lo[1] + 1, k + 1, key, ws);
         } else {
-            const int i = b.lo[0] + (int)(u % ex), j = b.lo[1] + (int)(u / ex);
-            if (overlapTest<site::OT_2D_XY>(st.o[2], vbComp<site::PC_2D>(i, g.mnf[0], d), vbComp<site::PC_2D>(j, g.mnf[1], d)))
-                sink(i + 1, j + 1, b.lo[2] + 1, key);
+            const int i = r.lo[0] + (int)(u % ex), j = r.lo[1] + (int)(u / ex);
+            if (overlapTest<site::OT_2D_XY>(od, vbComp<site::PC_2D>(i, g.mnf[0], d),
+                                            vbComp<site::PC_2D>(j, g.mnf[1], d)))
+                sink(i + 1, j + 1, r.lo[2] + 1, key, ws);
         }
         return;
     }
     // process3DTriangles (3603-3955): dominant projection, depth range from
-    // the plane, then the other two projections per voxel unless the range
-    // is a single voxel.
-    const F3 n = st.n;
+    // the plane, then per subspace slice of the depth axis either the single
+    // voxel or the other two projections per voxel.
+    const F3 n{r.n[0], r.n[1], r.n[2]};
+    const F3 t0{r.v0[0], r.v0[1], r.v0[2]};
     if (axis == 0) {
-        const int j = b.lo[1] + (int)(u % ey), k = b.lo[2] + (int)(u / ey);
+        const int j = r.lo[1] + (int)(u % ey), k = r.lo[2] + (int)(u / ey);
         F3 p{0.0f, vbComp<site::PC_3D>(j, g.mnf[1], d), vbComp<site::PC_3D>(k, g.mnf[2], d)};
-        if (!overlapTest<site::OT_3D_YZ>(st.o[0], p.y, p.z)) return;
-        int r0, r1;
-        depthRange<0, site::DT_3DX>(v, p, n, g, r0, r1);
-        if (r0 > b.hi[0] || r1 < b.lo[0]) return;
-        r0 = r0 < b.lo[0] ? b.lo[0] : r0;
-        r1 = r1 > b.hi[0] ? b.hi[0] : r1;
-        if (r0 == r1) { sink(r0 + 1, j + 1, k + 1, key); return; }
-        for (int i = r0; i <= r1; ++i) {
-            p.x = vbComp<site::PC_3DL>(i, g.mnf[0], d);
-            if (overlapTest<site::OT_3DX_ZX>(st.o[1], p.z, p.x) && overlapTest<site::OT_3DX_XY>(st.o[2], p.x, p.y))
-                sink(i + 1, j + 1, k + 1, key);
-        }
-    } else if (axis == 1) {
-        const int i = b.lo[0] + (int)(u % ex), k = b.lo[2] + (int)(u / ex);
-        F3 p{vbComp<site::PC_3D>(i, g.mnf[0], d), 0.0f, vbComp<site::PC_3D>(k, g.mnf[2], d)};
-        if (!overlapTest<site::OT_3D_ZX>(st.o[1], p.z, p.x)) return;
-        int r0, r1;
-        depthRange<1, site::DT_3DY>(v, p, n, g, r0, r1);
-        if (r0 > b.hi[1] || r1 < b.lo[1]) return;
-        r0 = r0 < b.lo[1] ? b.lo[1] : r0;
-        r1 = r1 > b.hi[1] ? b.hi[1] : r1;
-        if (r0 == r1) { sink(i + 1, r0 + 1, k + 1, key); return; }
-        for (int j = r0; j <= r1; ++j) {
-            p.y = vbComp<site::PC_3DL>(j, g.mnf[1], d);
-            if (overlapTest<site::OT_3DY_XY>(st.o[2], p.x, p.y) && overlapTest<site::OT_3DY_YZ>(st.o[0], p.y, p.z))
-                sink(i + 1, j + 1, k + 1, key);
-        }
-    } else {
-        const int i = b.lo[0] + (int)(u % ex), j = b.lo[1] + (int)(u / ex);
-        F3 p{vbComp<site::PC_3D>(i, g.mnf[0], d), vbComp<site::PC_3D>(j, g.mnf[1], d), 0.0f};
-        if (!overlapTest<site::OT_3D_XY>(st.o[2], p.x, p.y)) return;
-        int r0, r1;
-        depthRange<2, site::DT_3DZ>(v, p, n, g, r0, r1);
-        if (r0 > b.hi[2] || r1 < b.lo[2]) return;
-        r0 = r0 < b.lo[2] ? b.lo[2] : r0;
-        r1 = r1 > b.hi[2] ? b.hi[2] : r1;
-        if (r0 == r1) { sink(i + 1, j + 1, r0 + 1, key); return; }
-        for (int k = r0; k <= r1; ++k) {
-            p.z = vbComp<site::PC_3DL>(k, g.mnf[2], d);
-            if (overlapTest<site::OT_3DZ_YZ>(st.o[0], p.y, p.z) && overlapTest<site::OT_3DZ_ZX>(st.o[1], p.z, p.x))
-                sink(i + 1, j + 1, k + 1, key);
-        }
-    }
-}
-
-// The (split, column) of a staged triangle for its `local` work unit.
-__device__ __forceinline__ IBox locateUnit(const TriStage& st, const Split3* __restrict__ splits, uint32_t nSplits,
-                                           uint32_t& local) {
-    IBox b = st.full;
-    for (uint32_t s = 0; s < nSplits; ++s) {
-        b = st.full;
-        if (!clampBox(b, splits[s])) continue;
-        const uint32_t n = surfUnits(b, st.code);
-        if (local < n) break;
-        local -= n;
-    }
-    return b;
-}
-
-__global__ void __launch_bounds__(kBlock) surfaceWorkKernel(
-    Sink sink, const float* __restrict__ V, const uint32_t* __restrict__ I, const uint8_t* __restrict__ M, uint32_t nT,
-    PassGeom g, const Split3* __restrict__ splits, uint32_t nSplits, const uint32_t* __restrict__ codes,
-    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ totalPtr) {
-    __shared__ TriStage stage[kSlots];
-    __shared__ uint32_t stOff[kSlots + 1];
-    __shared__ uint32_t tFirst, nStage;
-    const uint32_t total = *totalPtr;
-    for (uint32_t base = blockIdx.x * kBlock; base < total; base += gridDim.x * kBlock) {
-        const uint32_t last = min(base + kBlock, total) - 1;
-        if (threadIdx.x == 0) {
-            const uint32_t t0 = findOwner(offsets, nT, base);
-            const uint32_t t1 = findOwner(offsets, nT, last);
-            tFirst = t0;
-            nStage = min(t1 - t0 + 1, kSlots);
-        }
-        __syncthreads();
-        const uint32_t t0 = tFirst, ns = nStage;
-        if (threadIdx.x < ns) {
-            stageTriangle(stage[threadIdx.x], V, I, M, codes, t0 + threadIdx.x, g);
-            stOff[threadIdx.x] = __ldg(offsets + t0 + threadIdx.x);
-        }
-        if (threadIdx.x == 0) stOff[ns] = __ldg(offsets + t0 + ns);
-        __syncthreads();
-        const uint32_t item = base + threadIdx.x;
-        if (item <= last) {
-            if (item < stOff[ns]) {
-                uint32_t lo = 0, hi = ns;  // stOff[lo] <= item < stOff[hi]
-                while (hi - lo > 1) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if (stOff[mid] <= item) lo = mid;
-                    else hi = mid;
-                }
-                const TriStage& st = stage[lo];
-                uint32_t local = item - stOff[lo];
-                const IBox b = locateUnit(st, splits, nSplits, local);
-                const uint64_t key = sink.wide ? (((uint64_t)(st.code >> 30) << 40) |
-                                                  ((uint64_t)(st.key & 255u) << 32) | st.tri)
-                                               : (uint64_t)st.key;
-                surfaceColumn(st, b, local, g, key, sink);
-            } else {
-                // More triangles than staging slots (runs of zero-unit
-                // triangles): stage privately.
-                const uint32_t t = findOwner(offsets, nT, item);
-                TriStage st;
-                stageTriangle(st, V, I, M, codes, t, g);
-                uint32_t local = item - __ldg(offsets + t);
-                const IBox b = locateUnit(st, splits, nSplits, local);
-                const uint64_t key = sink.wide ? (((uint64_t)(st.code >> 30) << 40) |
-                                                  ((uint64_t)(st.key & 255u) << 32) | st.tri)
-                                               : (uint64_t)st.key;
-                surfaceColumn(st, b, local, g, key, sink);
+        if (!overlapTest<site::OT_3D_YZ>(od, p.y, p.z)) return;
+        int d0, d1;
+        depthRange<0, site::DT_3DX>(t0, p, n, g, d0, d1);
+        const uint32_t* sl = slices + 2 * sliceOff[0];
+        for (uint32_t s = 0; s < sliceN[0]; ++s) {
+            const int lo = max(r.lo[0], (int)__ldg(sl + 2 * s)), hi = min(r.hi[0], (int)__ldg(sl + 2 * s + 1) - 1);
+            if (lo > hi || d0 > hi || d1 < lo) continue;
+            const int a = d0 < lo ? lo : d0, c = d1 > hi ? hi : d1;
+            if (a == c) { sink(a + 1, j + 1, k + 1, key, ws); continue; }
+            for (int i = a; i <= c; ++i) {
+                p.x = vbComp<site::PC_3DL>(i, g.mnf[0], d);
+                if (overlapTest<site::OT_3DX_ZX>(ov->o[1], p.z, p.x) && overlapTest<site::OT_3DX_XY>(ov->o[2], p.x, p.y))
+                    sink(i + 1, j + 1, k + 1, key, ws);
             }
         }
-        __syncthreads();
+    } else if (axis == 1) {
+        const int i = r.lo[0] + (int)(u % ex), k = r.lo[2] + (int)(u / ex);
+        F3 p{vbComp<site::PC_3D>(i, g.mnf[0], d), 0.0f, vbComp<site::PC_3D>(k, g.mnf[2], d)};
+        if (!overlapTest<site::OT_3D_ZX>(od, p.z, p.x)) return;
+        int d0, d1;
+        depthRange<1, site::DT_3DY>(t0, p, n, g, d0, d1);
+        const uint32_t* sl = slices + 2 * sliceOff[1];
+        for (uint32_t s = 0; s < sliceN[1]; ++s) {
+            const int lo = max(r.lo[1], (int)__ldg(sl + 2 * s)), hi = min(r.hi[1], (int)__ldg(sl + 2 * s + 1) - 1);
+            if (lo > hi || d0 > hi || d1 < lo) continue;
+            const int a = d0 < lo ? lo : d0, c = d1 > hi ? hi : d1;
+            if (a == c) { sink(i + 1, a + 1, k + 1, key, ws); continue; }
+            for (int j = a; j <= c; ++j) {
+                p.y = vbComp<site::PC_3DL>(j, g.mnf[1], d);
+                if (overlapTest<site::OT_3DY_XY>(ov->o[2], p.x, p.y) && overlapTest<site::OT_3DY_YZ>(ov->o[0], p.y, p.z))
+                    sink(i + 1, j + 1, k + 1, key, ws);
+            }
+        }
+    } else {
+        const int i = r.lo[0] + (int)(u % ex), j = r.lo[1] + (int)(u / ex);
+        F3 p{vbComp<site::PC_3D>(i, g.mnf[0], d), vbComp<site::PC_3D>(j, g.mnf[1], d), 0.0f};
+        if (!overlapTest<site::OT_3D_XY>(od, p.x, p.y)) return;
+        int d0, d1;
+        depthRange<2, site::DT_3DZ>(t0, p, n, g, d0, d1);
+        const uint32_t* sl = slices + 2 * sliceOff[2];
+        for (uint32_t s = 0; s < sliceN[2]; ++s) {
+            const int lo = max(r.lo[2], (int)__ldg(sl + 2 * s)), hi = min(r.hi[2], (int)__ldg(sl + 2 * s + 1) - 1);
+            if (lo > hi || d0 > hi || d1 < lo) continue;
+            const int a = d0 < lo ? lo : d0, c = d1 > hi ? hi : d1;
+            if (a == c) { sink(i + 1, j + 1, a + 1, key, ws); continue; }
+            for (int k = a; k <= c; ++k) {
+                p.z = vbComp<site::PC_3DL>(k, g.mnf[2], d);
+                if (overlapTest<site::OT_3DZ_YZ>(ov->o[0], p.y, p.z) && overlapTest<site::OT_3DZ_ZX>(ov->o[1], p.z, p.x))
+                    sink(i + 1, j + 1, k + 1, key, ws);
+            }
+        }
     }
+}
+
+// Largest t < n with off[t] <= item (off[n] > item), by a 32-way search of
+// the whole warp: ceil(log32 n) dependent loads.
+__device__ __forceinline__ uint32_t warpFindOwner(const uint32_t* __restrict__ off, uint32_t n, uint32_t item,
+                                                  uint32_t lane) {
+    uint32_t lo = 0, hi = n;  // off[lo] <= item < off[hi]
+    while (hi - lo > 1) {
+        const uint32_t step = (hi - lo + 31u) / 32u;
+        const uint32_t p = lo + lane * step;
+        const bool ok = p < hi && __ldg(off + p) <= item;
+        const uint32_t m = __ballot_sync(kFull, ok);
+        const uint32_t nlo = lo + (31u - (uint32_t)__clz(m)) * step;
+        hi = min(nlo + step, hi);
+        lo = nlo;
+    }
+    return lo;
+}
+
+// Pass 4: the work list.  Warps take batches of kBatch consecutive 32-item
+// chunks; within a batch the owner of each chunk's first item follows from
+// the previous chunk.  Every partitioned triangle has at least one unit, so
+// a chunk's 32 items belong to at most 32 consecutive triangles: lane l
+// loads off[t0 + l] and a bit mask of the triangle starts inside the chunk
+// gives every lane its owner.  The class and axis of a position follow from
+// the bucket bounds, so the projection edge functions load together with
+// the record.
+__global__ void __launch_bounds__(kBlock) surfaceWorkKernel(Sink sink, const SurfRec* __restrict__ recs,
+                                                            const SurfOvl* __restrict__ ovl,
+                                                            const uint32_t* __restrict__ off, uint32_t n,
+                                                            const uint32_t* __restrict__ totalPtr,
+                                                            const uint32_t* __restrict__ bucketCount, PassGeom g,
+                                                            const uint32_t* __restrict__ slices, SliceTable st) {
+    __shared__ unsigned long long stageBuf[kBlock / 32][kStageHits];
+    __shared__ uint32_t stageCount[kBlock / 32];
+    __shared__ uint32_t bucketEnd[kSurfaceBuckets];
+    const uint32_t total = *totalPtr;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t wib = threadIdx.x >> 5;
+    const WarpStage ws{stageBuf[wib], stageCount + wib};
+    if (lane == 0) stageCount[wib] = 0;
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (uint32_t k = 0; k < kSurfaceBuckets; ++k) {
+            acc += __ldg(bucketCount + k);
+            bucketEnd[k] = acc;
+        }
+    }
+    __syncthreads();
+    const uint32_t chunks = (total + 31u) / 32u;
+    const uint32_t batches = (chunks + kBatch - 1) / kBatch;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nWarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t bt = warp; bt < batches; bt += nWarps) {
+        const uint32_t c1 = min((bt + 1) * kBatch, chunks);
+        uint32_t t0 = warpFindOwner(off, n, bt * kBatch * 32u, lane);
+        for (uint32_t c = bt * kBatch; c < c1; ++c) {
+            const uint32_t base = c * 32u;
+            const uint32_t ol = t0 + lane <= n ? __ldg(off + t0 + lane) : 0xFFFFFFFFu;
+            const uint32_t o32 = t0 + 32u <= n ? __ldg(off + t0 + 32u) : 0xFFFFFFFFu;
+            const uint32_t starts = __reduce_or_sync(kFull, (lane >= 1u && ol < base + 32u) ? 1u << (ol - base) : 0u);
+            const uint32_t k = __popc(starts & ((2u << lane) - 1u));
+            const uint32_t ok = __shfl_sync(kFull, ol, k);
+            const uint32_t k31 = __popc(starts);
+            const uint32_t next = __shfl_sync(kFull, ol, (k31 + 1u) & 31u);
+            const uint32_t nextOff = k31 < 31u ? next : o32;
+            const uint32_t item = base + lane;
+            if (item < total) {
+                const uint32_t pos = t0 + k;
+                uint32_t bucket = 0;
+#pragma unroll
+                for (uint32_t q = 0; q + 1 < kSurfaceBuckets; ++q) bucket += pos >= bucketEnd[q] ? 1u : 0u;
+                const uint32_t bb = bucket / 3u + 1u, axis = bucket % 3u;
+                Overlap od;
+                if (bb >= 2) od = ovl[pos].o[axis];
+                const SurfRec r = recs[pos];
+                const uint64_t key = sink.wide ? (((uint64_t)bb << 40) | ((uint64_t)(r.key & 255u) << 32) | r.tri)
+                                               : (uint64_t)r.key;
+                surfaceItem(bb, axis, r, od, ovl + pos, item - ok, g, slices, st.off, st.n, key, sink, ws);
+            }
+            __syncwarp();
+            if (sink.mode == 0 && *ws.count >= kFlushAt) sink.flush(ws, lane);
+            t0 += k31 + (nextOff == base + 32u ? 1u : 0u);
+        }
+    }
+    if (sink.mode == 0) sink.flush(ws, lane);
 }
 
 // Exclusive popcount prefix over the surface words (ranks of surface voxels).
@@ -562,17 +693,21 @@ __global__ void mergeKeysKernel(const unsigned long long* __restrict__ list, con
 
 }  // namespace
 
-void launch_surface_count(const float* V, const uint32_t* I, uint32_t nT, PassGeom g, const Split3* splits,
-                          uint32_t nSplits, uint32_t* codes, uint32_t* counts, cudaStream_t s, uint32_t* launches) {
-    surfaceCountKernel<<<gridFor(nT, 256), 256, 0, s>>>(V, I, nT, g, splits, nSplits, codes, counts);
-    *launches += 1;
+void launch_surface_prepare(const float* V, const uint32_t* I, const uint8_t* M, uint32_t nT, PassGeom g,
+                            uint32_t* codes, uint32_t* units, uint32_t* buckets, uint32_t* perm, uint32_t* unitsP,
+                            void* recs, void* ovl, cudaStream_t s, uint32_t* launches) {
+    const uint32_t grid = gridFor(nT, 256);
+    surfaceClassifyKernel<<<grid, 256, 0, s>>>(V, I, nT, g, codes, units, buckets);
+    surfaceScatterKernel<<<grid, 256, 0, s>>>(codes, units, nT, buckets, buckets + kSurfaceBuckets, perm, unitsP);
+    surfaceSetupKernel<<<grid, 256, 0, s>>>(V, I, M, perm, codes, buckets, g, static_cast<SurfRec*>(recs),
+                                            static_cast<SurfOvl*>(ovl));
+    *launches += 3;
 }
 
-void launch_surface_work(int mode, int wide, const float* V, const uint32_t* I, const uint8_t* M, uint32_t nT,
-                         PassGeom g, const Split3* splits, uint32_t nSplits, const uint32_t* codes,
-                         const uint32_t* offsets, const uint32_t* total, uint32_t* surfBits, uint64_t posBase,
-                         const uint32_t* ranks, void* keys, unsigned long long* list, uint32_t* listCount,
-                         uint32_t listCap, cudaStream_t s, uint32_t* launches) {
+void launch_surface_work(int mode, int wide, const void* recs, const void* ovl, const uint32_t* offsets, uint32_t nT,
+                         const uint32_t* total, const uint32_t* buckets, PassGeom g, const uint32_t* slices, SliceTable st, uint32_t* surfBits,
+                         uint64_t posBase, const uint32_t* ranks, void* keys, unsigned long long* list,
+                         uint32_t* listCount, uint32_t listCap, cudaStream_t s, uint32_t* launches) {
     Sink sink;
     sink.bits = surfBits;
     sink.posBase = posBase;
@@ -584,7 +719,9 @@ void launch_surface_work(int mode, int wide, const float* V, const uint32_t* I, 
     sink.mode = mode;
     sink.wide = wide;
     sink.g = g;
-    surfaceWorkKernel<<<148 * 4, kBlock, 0, s>>>(sink, V, I, M, nT, g, splits, nSplits, codes, offsets, total);
+    surfaceWorkKernel<<<148 * 8, kBlock, 0, s>>>(sink, static_cast<const SurfRec*>(recs),
+                                                  static_cast<const SurfOvl*>(ovl), offsets, nT, total, buckets, g,
+                                                  slices, st);
     *launches += 1;
 }
 
