@@ -259,6 +259,23 @@ def cpu_baseline(mesh):
                       f"whole path, {dt:.1f} s on {cores} threads"}
 
 
+def profile_run(args):
+    """The workload's launches and nothing else, for a profiler to capture."""
+    import torch
+
+    from voxelizer_b200 import scenes
+    from voxelizer_b200.api import LONG, Voxelizer
+
+    mesh = scenes.room_scene()
+    with Voxelizer(mesh.vertices, mesh.indices, mesh.materials, mesh.n_materials, node_type=LONG) as vx:
+        info = vx.plan(1, args.profile_run)
+        out = torch.empty(int(info.bytes), dtype=torch.uint8, device="cuda")
+        for _ in range(args.steps):
+            vx.voxelize_device(1, args.profile_run, out)
+        torch.cuda.synchronize()
+        print(f"profile run: {args.steps} x {info.dims}, {vx.last_launch_count()} launches each", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -267,11 +284,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--profile-run", type=int, default=0, metavar="MAXDIM",
+                    help="no timing: voxelize the room scene at this maxDimension --steps times (a target for ncu)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.profile_run:
+        profile_run(args)
         return
 
     import torch

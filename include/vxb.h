@@ -121,8 +121,9 @@ vxb_status vxb_voxelize_to_host(vxb_voxelizer* v, int nodes, const vxb_request* 
 /* voxelize / voxelizeToNodes with devConfig (1,1), include/voxelizer.h:718-770:
  * writes the result into the caller's device buffer `dev_out`, stream-ordered
  * on `stream` (a cudaStream_t, NULL for the default stream).  The mesh is
- * uploaded on the first call and stays resident.  Returns once the work is
- * enqueued unless a split needs a host decision (none on the default path). */
+ * uploaded on the first call and stays resident.  Returns when the result is
+ * complete (as the reference's calls do); the host reads a few status words
+ * once, after all launches. */
 vxb_status vxb_voxelize_to_device(vxb_voxelizer* v, int nodes, const vxb_request* req, void* dev_out,
                                   uint64_t dev_bytes, void* stream, vxb_grid_info* info);
 
@@ -137,6 +138,29 @@ vxb_status vxb_last_launch_count(vxb_voxelizer* v, uint32_t* launches);
 vxb_status vxb_set_profiling(vxb_voxelizer* v, int enable);
 vxb_status vxb_stage_times(vxb_voxelizer* v, float* ms, uint32_t n);
 
+/* Batches (no reference counterpart; the reference voxelizes one mesh per
+ * call).  A batch runs the meshes of several voxelizers through one sequence
+ * of launches: every kernel covers all meshes at once, so many small meshes
+ * cost about as much as one large one.  All meshes of a batch share the
+ * node type and output kind (node grid or plain bit array) and the device;
+ * each gets its own request and device output.  Results are identical to
+ * vxb_voxelize_to_device on each mesh alone.  The voxelizers must outlive
+ * the batch's runs.  vxb_batch_run returns when every result is complete.
+ * With VXB_BATCH_GRAPH the launches are captured once into a CUDA graph and
+ * replayed on later runs of the same batch (until vxb_batch_add /
+ * vxb_batch_clear change it); a NULL stream then means a stream the batch
+ * owns, ordered after the default stream. */
+typedef struct vxb_batch vxb_batch;
+#define VXB_BATCH_GRAPH 1
+vxb_status vxb_batch_create(vxb_batch** out, int device);
+vxb_status vxb_batch_destroy(vxb_batch* b);
+vxb_status vxb_batch_add(vxb_batch* b, vxb_voxelizer* v, int nodes, const vxb_request* req, void* dev_out,
+                         uint64_t dev_bytes, vxb_grid_info* info);
+vxb_status vxb_batch_clear(vxb_batch* b);
+vxb_status vxb_batch_run(vxb_batch* b, void* stream, int flags);
+/* Kernels of the last run (graph replays count the captured kernels). */
+vxb_status vxb_batch_last_launch_count(vxb_batch* b, uint32_t* launches);
+
 /* No counterpart in the reference.  The plain voxelization of
  * vxb_voxelize_to_device(v, 0, ...) for callers that cannot allocate device
  * memory: solvers that reserve the whole GPU for their own pool, or that
@@ -144,7 +168,7 @@ vxb_status vxb_stage_times(vxb_voxelizer* v, float* ms, uint32_t n);
  * allocates nothing: the mesh (dev_vertices: 3 floats per vertex,
  * dev_indices: 3 indices < n_vertices per triangle) and dev_out are the
  * caller's device buffers, and its work lists live in a fixed device array
- * of 16,796,672 bytes inside the library, which every GPU that loads the
+ * of 16,797,440 bytes inside the library, which every GPU that loads the
  * library holds until exit.  min_vertex / max_vertex: the mesh's bounding
  * box, the component-wise min / max of the vertices (vxb_plan reports it).
  * Limits: at most 2,097,152 triangles and 1024 yz subspaces (vox_split_res

@@ -24,7 +24,10 @@ NODE_BYTES = {SHORT: 1, LONG: 2, PARTIAL: 8, SHORT_FCC: 2, LONG_FCC: 4}
 EXPORTS = ["vxb_last_error", "vxb_version", "vxb_create", "vxb_destroy", "vxb_set_materials",
            "vxb_set_material_output", "vxb_verbose_output", "vxb_plan", "vxb_get_array_dimensions",
            "vxb_voxelize_to_host", "vxb_voxelize_to_device", "vxb_last_launch_count", "vxb_set_profiling",
-           "vxb_stage_times", "vxb_voxelize_bits_noalloc", "vxb_trim_cache"]
+           "vxb_stage_times", "vxb_voxelize_bits_noalloc", "vxb_trim_cache", "vxb_batch_create",
+           "vxb_batch_destroy", "vxb_batch_add", "vxb_batch_clear", "vxb_batch_run", "vxb_batch_last_launch_count"]
+
+BATCH_GRAPH = 1
 
 
 class VxbError(RuntimeError):
@@ -71,6 +74,12 @@ def lib():
         "vxb_create": (ctypes.c_int, [P(vp), ctypes.c_int, vp, vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int]),
         "vxb_destroy": (ctypes.c_int, [vp]),
         "vxb_trim_cache": (ctypes.c_int, []),
+        "vxb_batch_create": (ctypes.c_int, [P(vp), ctypes.c_int]),
+        "vxb_batch_destroy": (ctypes.c_int, [vp]),
+        "vxb_batch_add": (ctypes.c_int, [vp, vp, ctypes.c_int, P(Request), vp, ctypes.c_uint64, P(GridInfo)]),
+        "vxb_batch_clear": (ctypes.c_int, [vp]),
+        "vxb_batch_run": (ctypes.c_int, [vp, vp, ctypes.c_int]),
+        "vxb_batch_last_launch_count": (ctypes.c_int, [vp, P(ctypes.c_uint32)]),
         "vxb_set_materials": (ctypes.c_int, [vp, vp, ctypes.c_uint32]),
         "vxb_set_material_output": (ctypes.c_int, [vp, ctypes.c_int]),
         "vxb_verbose_output": (ctypes.c_int, [vp, ctypes.c_int]),

@@ -137,3 +137,55 @@ class Voxelizer:
         n = ctypes.c_uint32()
         check(lib().vxb_last_launch_count(self._h, ctypes.byref(n)))
         return int(n.value)
+
+
+class VoxelizerBatch:
+    """Several voxelizers' meshes run through one sequence of launches
+    (vxb_batch_*).  Every mesh gets its own request and device output;
+    results equal the single-mesh calls.  ``graph=True`` captures the
+    launches once and replays them on later runs of the same batch."""
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        check(lib().vxb_batch_create(ctypes.byref(h), int(device)))
+        self._h = h
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().vxb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def add(self, voxelizer, nodes, size, out, voxSplitRes=DEFAULT_VOX, matSplitRes=DEFAULT_MAT):
+        """Adds one mesh; ``out`` exposes data_ptr() (a device tensor)."""
+        info = _lib.GridInfo()
+        r = make_request(size, voxSplitRes, matSplitRes)
+        nbytes = out.numel() * out.element_size() if hasattr(out, "element_size") else int(out.nbytes)
+        check(lib().vxb_batch_add(self._h, voxelizer._h, int(bool(nodes)), ctypes.byref(r),
+                                  ctypes.c_void_p(out.data_ptr()), nbytes, ctypes.byref(info)))
+        self._keep.append((voxelizer, out))
+        return info
+
+    def clear(self):
+        check(lib().vxb_batch_clear(self._h))
+        self._keep = []
+
+    def run(self, stream=None, graph=False):
+        check(lib().vxb_batch_run(self._h, ctypes.c_void_p(stream or 0), _lib.BATCH_GRAPH if graph else 0))
+
+    def last_launch_count(self):
+        n = ctypes.c_uint32()
+        check(lib().vxb_batch_last_launch_count(self._h, ctypes.byref(n)))
+        return int(n.value)

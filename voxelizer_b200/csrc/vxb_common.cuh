@@ -27,6 +27,18 @@ __device__ __forceinline__ uint32_t findOwner(const uint32_t* __restrict__ offse
     return lo;
 }
 
+// Unit of element x: the largest u < n with base[u] <= x (base[0] = 0).
+template <class T>
+__device__ __forceinline__ uint32_t unitOf(const T* __restrict__ base, uint32_t n, T x) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(base + mid) <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
 // Blocks for `work` items at `threads` per block, capped (grid-stride loops).
 inline uint32_t gridFor(uint64_t work, uint32_t threads, uint32_t cap = 148u * 32u) {
     uint64_t b = (work + threads - 1) / threads;

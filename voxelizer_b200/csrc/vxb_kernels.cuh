@@ -1,4 +1,13 @@
 // Kernel declarations and the plain structs the host engine passes to them.
+//
+// Every kernel works on a batch of units.  A unit is one mesh voxelized on
+// one lattice (a Cartesian mesh is one unit, an FCC mesh four: one per
+// shifted sub-lattice).  The batch concatenates what its units need into
+// shared arrays: work triangles (the units' triangle lists back to back, so
+// an FCC mesh's triangles appear once per sub-lattice), bit-grid words (each
+// unit's grids start at a multiple of 32 words), subspace tables and flags.
+// Meshes stay in their own device arrays.  A single voxelization is a batch
+// of one mesh.
 #pragma once
 
 #include <cstdint>
@@ -6,8 +15,8 @@
 
 namespace vxb {
 
-// Geometry of one solid / surface pass.  For FCC lattices each of the four
-// sub-lattices is one pass with its own shifted minimum corner.
+// Geometry of one unit.  For FCC lattices each of the four sub-lattices has
+// its own shifted minimum corner.
 struct PassGeom {
     double mn[3];        // minimum corner (FP64, as the reference's extMinVertex)
     double d;            // voxel length
@@ -20,19 +29,47 @@ struct PassGeom {
 };
 
 struct SplitYZ { uint32_t y0, y1, z0, z1; };
-struct Split3 { uint32_t x0, x1, y0, y1, z0, z1; };
+
+struct Unit {
+    PassGeom g;
+    const float* V;       // the mesh: vertices (3 floats each),
+    const uint32_t* I;    // indices into V (3 per triangle),
+    const uint8_t* M;     // material per triangle (NULL without materials)
+    uint32_t nT;          // triangles of the mesh
+    uint32_t splitBase;   // solid yz subspaces: SplitYZ entries [splitBase, splitBase + nSplits)
+    uint32_t nSplits;
+    uint32_t sliceBase;   // material subspace slices: (lo, hi) pairs, x then y then z
+    uint32_t sliceN[3];
+    uint32_t laterBase;   // AY + AZ flags: row y + 1 / plane z + 1 starts a later pruning subspace
+    uint32_t materials;   // surface pass and material output enabled
+    uint64_t wordBase;    // first word of the unit's bit grids (a multiple of 32)
+    void* out;            // node output (Cartesian units)
+};
+
+// Device tables of a batch.  Bases have nUnits + 1 entries (the last one is
+// the total), so that the unit of an element is a binary search away.
+struct Batch {
+    const Unit* units;
+    uint32_t nUnits;
+    const uint32_t* workBase;   // first work triangle of each unit
+    const uint64_t* rowBase;    // first grid row (y, z) of each unit
+    const uint64_t* wordBase;   // first grid word of each unit
+    const SplitYZ* splits;
+    const uint32_t* slices;
+    const uint8_t* later;
+};
 
 // Work-list scan: exclusive offsets (n + 1 entries) and the grand total.
 void launch_scan(const uint32_t* in, uint32_t* offsets, uint32_t n, uint32_t* blockSums, uint32_t* total,
                  uint32_t* overflow, cudaStream_t s, uint32_t* launches);
 
 // ---- Solid (parity) voxelization: src/voxelizer.cu:840-1617 ----
-void launch_solid_count(const float* V, const uint32_t* I, uint32_t nT, PassGeom g, const SplitYZ* splits,
-                        uint32_t nSplits, uint32_t* counts, cudaStream_t s, uint32_t* launches);
-void launch_solid_toggle(const float* V, const uint32_t* I, uint32_t nT, PassGeom g, const SplitYZ* splits,
-                         uint32_t nSplits, const uint32_t* offsets, const uint32_t* total, uint32_t* toggles,
-                         cudaStream_t s, uint32_t* launches);
-void launch_row_fill(uint32_t* words, uint32_t rows, uint32_t ipx, cudaStream_t s, uint32_t* launches);
+// Candidates per work triangle, the toggles of the listed candidates into
+// the `fill` arena, then the row prefix XOR over all rows of the batch.
+void launch_solid_count(const Batch& b, uint32_t nWork, uint32_t* counts, cudaStream_t s, uint32_t* launches);
+void launch_solid_toggle(const Batch& b, uint32_t nWork, const uint32_t* offsets, const uint32_t* total,
+                         uint32_t* fill, cudaStream_t s, uint32_t* launches);
+void launch_row_fill(const Batch& b, uint64_t nRows, uint32_t* fill, cudaStream_t s, uint32_t* launches);
 
 // ---- Surface voxelization: src/voxelizer.cu:2358-2989, 3040-4201 ----
 // Triangles with surface work are partitioned into kSurfaceBuckets buckets
@@ -42,51 +79,68 @@ constexpr uint32_t kSurfaceBuckets = 9;
 constexpr size_t kSurfRecBytes = 64;
 constexpr size_t kSurfOvlBytes = 112;
 
-// Material subspace slices along each axis: (lo, hi) pairs, axis a at pair
-// offset off[a], n[a] of them.
-struct SliceTable { uint32_t off[3], n[3]; };
-
-// Classify (codes / units in mesh order, per-bucket counts in buckets[0..9)),
-// partition (perm, unitsP in partitioned order; buckets[9..18) are cursors)
-// and set up (records).  buckets and unitsP[0..nT] must be zero on entry.
-void launch_surface_prepare(const float* V, const uint32_t* I, const uint8_t* M, uint32_t nT, PassGeom g,
-                            uint32_t* codes, uint32_t* units, uint32_t* buckets, uint32_t* perm, uint32_t* unitsP,
-                            void* recs, void* ovl, cudaStream_t s, uint32_t* launches);
-// Surface work over the exclusive scan `offsets` of unitsP (nT + 1 entries),
-// one thread per column.  mode 0: set surface bits in `surfBits` and append
-// (bit position << 24 | key) to `list` (entries past listCap are counted,
-// not stored); mode 1: merge every hit's key at its rank (needs complete
-// bits and `ranks`).  posBase is the bit position of surfBits[0] in the rank
-// space (FCC sub-lattices are stacked).  wide: 64-bit keys (PartialNode).
-void launch_surface_work(int mode, int wide, const void* recs, const void* ovl, const uint32_t* offsets, uint32_t nT,
-                         const uint32_t* total, const uint32_t* buckets, PassGeom g, const uint32_t* slices,
-                         SliceTable st, uint32_t* surfBits, uint64_t posBase, const uint32_t* ranks, void* keys, unsigned long long* list,
-                         uint32_t* listCount, uint32_t listCap, cudaStream_t s, uint32_t* launches);
+// Classify (codes / units in work-triangle order, per-bucket counts in
+// buckets[0..9)), partition (perm, unitsP in partitioned order;
+// buckets[9..18) are cursors) and set up (records) the work triangles of
+// units with materials.  buckets and unitsP[0..nWork] must be zero on entry.
+void launch_surface_prepare(const Batch& b, uint32_t nWork, uint32_t* codes, uint32_t* units, uint32_t* buckets,
+                            uint32_t* perm, uint32_t* unitsP, void* recs, void* ovl, cudaStream_t s,
+                            uint32_t* launches);
+// Surface work over the exclusive scan `offsets` of unitsP (nWork + 1
+// entries), one thread per column.  mode 0: set bits in the `surf` arena and
+// append (bit position << 24 | key) to `list` (entries past listCap are
+// counted, not stored); mode 1: merge every hit's key at its rank (needs
+// complete bits and `ranks`).  wide: 64-bit keys (PartialNode).
+void launch_surface_work(int mode, int wide, const Batch& b, const void* recs, const void* ovl,
+                         const uint32_t* offsets, uint32_t nWork, const uint32_t* total, const uint32_t* buckets,
+                         uint32_t* surf, const uint32_t* ranks, void* keys, uint32_t keysCap,
+                         unsigned long long* list, uint32_t* listCount, uint32_t listCap, cudaStream_t s,
+                         uint32_t* launches);
 // Exclusive popcount prefix over `words` surface words; *total = surface voxels.
 void launch_surface_rank(const uint32_t* bits, uint64_t words, uint32_t* ranks, uint32_t* tileSums, uint32_t* total,
                          cudaStream_t s, uint32_t* launches);
-void launch_surface_keys_zero(void* keys, const uint32_t* count, int wide, cudaStream_t s, uint32_t* launches);
+// Zeroes min(*count, cap) keys.
+void launch_surface_keys_zero(void* keys, const uint32_t* count, uint32_t cap, int wide, cudaStream_t s,
+                              uint32_t* launches);
+// Keys at ranks >= keysCap are dropped (the host re-merges after growing).
 void launch_surface_merge(const unsigned long long* list, const uint32_t* listCount, uint32_t listCap,
-                          const uint32_t* bits, const uint32_t* ranks, uint32_t* keys, cudaStream_t s,
-                          uint32_t* launches);
+                          const uint32_t* bits, const uint32_t* ranks, uint32_t* keys, uint32_t keysCap,
+                          cudaStream_t s, uint32_t* launches);
 
 // ---- Node classification: src/voxelizer.cu:1626-2048 ----
 void launch_combine(const uint32_t* a, const uint32_t* b, uint32_t* out, uint64_t n, cudaStream_t s,
                     uint32_t* launches);
-// One in-place pruning pass over `split`; neighbours in later subspaces
-// (yLater / zLater) are read from fill | surf.  Sets *changed if any word
-// changed.
-void launch_prune(uint32_t* solid, const uint32_t* fill, const uint32_t* surf, const uint8_t* yLater,
-                  const uint8_t* zLater, PassGeom g, SplitYZ split, uint32_t* changed, cudaStream_t s,
-                  uint32_t* launches);
-// yLater[y] / zLater[z] are 1 where row y + 1 / plane z + 1 starts a later
-// pruning subspace than row y / plane z.  ranks / keys: surface voxel ranks
-// and merged material keys (materials only).
-void launch_emit_cartesian(int nodeKind, const uint32_t* finalSolid, const uint32_t* fill, const uint32_t* surf,
-                           const uint32_t* ranks, const void* keys, PassGeom g, const uint8_t* yLater,
-                           const uint8_t* zLater, void* nodes, int materials, cudaStream_t s, uint32_t* launches);
-void launch_emit_fcc(int nodeKind, const uint32_t* const* fill, const uint32_t* const* surf,
-                     const uint64_t* surfWordBase, const uint32_t* ranks, const void* keys, PassGeom g, void* nodes,
-                     int materials, cudaStream_t s, uint32_t* launches);
+
+// One pruning region: subspace `split` of unit `unit`.  wordStart is the
+// exclusive prefix of region words within one launch.
+struct PruneRegion {
+    uint32_t unit;
+    SplitYZ split;
+    uint32_t wordStart;
+};
+// One in-place pruning pass over `n` regions (totalWords words).  Region r
+// sets flags[(flagBase + r) * passes + pass] if it changed anything; for
+// pass > 0 a region whose previous pass changed nothing is skipped.
+// Neighbours in later subspaces are read from fill | surf (surf may be NULL).
+void launch_prune(const Batch& b, const PruneRegion* regions, uint32_t n, uint32_t totalWords, uint32_t* solid,
+                  const uint32_t* fill, const uint32_t* surf, uint32_t* flags, uint32_t flagBase, uint32_t passes,
+                  uint32_t pass, cudaStream_t s, uint32_t* launches);
+// Cartesian node grids of every unit of the batch (all of one node kind).
+// Keys at ranks >= keysCap read as 0.
+void launch_emit_cartesian(int nodeKind, const Batch& b, uint64_t totalWords, const uint32_t* finalSolid,
+                           const uint32_t* fill, const uint32_t* surf, const uint32_t* ranks, const void* keys,
+                           uint32_t keysCap, cudaStream_t s, uint32_t* launches);
+
+// An FCC mesh: its four sub-lattice units are units [unit0, unit0 + 4).
+struct FccMesh {
+    uint32_t unit0;
+    void* out;
+};
+// FCC node grids; groupBase[m] is the first 16-byte output group of mesh m
+// (nMeshes + 1 entries).
+void launch_emit_fcc(int nodeKind, const Batch& b, const FccMesh* meshes, const uint64_t* groupBase,
+                     uint32_t nMeshes, uint64_t totalGroups, const uint32_t* fill, const uint32_t* surf,
+                     const uint32_t* ranks, const void* keys, uint32_t keysCap, cudaStream_t s,
+                     uint32_t* launches);
 
 }  // namespace vxb

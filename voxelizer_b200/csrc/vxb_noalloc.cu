@@ -39,7 +39,7 @@
 #include <mutex>
 
 namespace vxb {
-int recordError(int code, const char* msg);  // vxb_engine.cu
+int recordError(int code, const char* msg);  // vxb_host.cu
 }
 
 namespace {
@@ -51,18 +51,29 @@ constexpr int kMaxDevices = 64;
 
 constexpr size_t roundUp(size_t v) { return (v + 255) / 256 * 256; }
 
+// The one-unit batch tables the kernels read.
+struct UnitTables {
+    vxb::Unit unit;
+    uint32_t workBase[2];
+    uint32_t pad[2];
+    uint64_t rowBase[2];
+    uint64_t wordBase[2];
+};
+
 // Layout of the scratch array (byte offsets).
 constexpr size_t kStatusOff = 0;  // [0] candidate total, [1] overflow flag
-constexpr size_t kSubspaceOff = kStatusOff + 256;
+constexpr size_t kTablesOff = kStatusOff + 256;
+constexpr size_t kSubspaceOff = kTablesOff + 768;
+static_assert(sizeof(UnitTables) <= 768, "tables region");
 constexpr size_t kTileOff = kSubspaceOff + roundUp(kMaxSubspaces * sizeof(vxb::SplitYZ));
 constexpr size_t kCountOff = kTileOff + roundUp(4 * (kMaxTriangles / kScanTile + 2));
 constexpr size_t kOffsetOff = kCountOff + roundUp(4 * ((size_t)kMaxTriangles + 1));
 constexpr size_t kScratchBytes = kOffsetOff + roundUp(4 * ((size_t)kMaxTriangles + 2));
-static_assert(kScratchBytes == 16796672, "scratch layout changed: update the stated size");
+static_assert(kScratchBytes == 16797440, "scratch layout changed: update the stated size");
 
 }  // namespace
 
-// 16,796,672 bytes (about 16.0 MiB) of device memory, held by every GPU that
+// 16,797,440 bytes (about 16.0 MiB) of device memory, held by every GPU that
 // loads this library until the process exits.
 static __device__ __align__(256) unsigned char g_noallocScratch[kScratchBytes];
 
@@ -228,7 +239,9 @@ extern "C" vxb_status vxb_voxelize_bits_noalloc(const float* dev_vertices, const
     for (uint32_t z = 0; z < nz; ++z)
         for (uint32_t y = 0; y < ny; ++y) sub[nSub++] = vxb::SplitYZ{ys[y].lo, ys[y].hi, zs[z].lo, zs[z].hi};
 
-    vxb::PassGeom g;
+    UnitTables tab;
+    memset(&tab, 0, sizeof(tab));
+    vxb::PassGeom& g = tab.unit.g;
     for (int a = 0; a < 3; ++a) {
         g.mn[a] = min_vertex[a];
         g.mnf[a] = (float)min_vertex[a];
@@ -241,26 +254,43 @@ extern "C" vxb_status vxb_voxelize_bits_noalloc(const float* dev_vertices, const
     g.AY = bg.alloc[1];
     g.AZ = bg.alloc[2];
     g.ipx = bg.res[0] / 32;
+    tab.unit.V = dev_vertices;
+    tab.unit.I = dev_indices;
+    tab.unit.nT = n_triangles;
+    tab.unit.nSplits = nSub;
+    tab.unit.out = dev_out;
+    tab.workBase[1] = n_triangles;
+    tab.rowBase[1] = (uint64_t)g.AY * g.AZ;
+    tab.wordBase[1] = (uint64_t)g.ipx * g.AY * g.AZ;
 
     const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     uint32_t* status = reinterpret_cast<uint32_t*>(scratch + kStatusOff);
+    UnitTables* dtab = reinterpret_cast<UnitTables*>(scratch + kTablesOff);
     vxb::SplitYZ* dsub = reinterpret_cast<vxb::SplitYZ*>(scratch + kSubspaceOff);
     uint32_t* tiles = reinterpret_cast<uint32_t*>(scratch + kTileOff);
     uint32_t* counts = reinterpret_cast<uint32_t*>(scratch + kCountOff);
     uint32_t* offsets = reinterpret_cast<uint32_t*>(scratch + kOffsetOff);
     uint32_t* grid = static_cast<uint32_t*>(dev_out);
+    vxb::Batch b;
+    memset(&b, 0, sizeof(b));
+    b.units = &dtab->unit;
+    b.nUnits = 1;
+    b.workBase = dtab->workBase;
+    b.rowBase = dtab->rowBase;
+    b.wordBase = dtab->wordBase;
+    b.splits = dsub;
     uint32_t launches = 0;
     e = cudaMemsetAsync(grid, 0, gi.bytes, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dtab, &tab, sizeof(tab), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dsub, sub, nSub * sizeof(vxb::SplitYZ), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return failf(VXB_ECUDA, "%s", cudaGetErrorString(e));
     }
-    vxb::launch_solid_count(dev_vertices, dev_indices, n_triangles, g, dsub, nSub, counts, s, &launches);
+    vxb::launch_solid_count(b, n_triangles, counts, s, &launches);
     vxb::launch_scan(counts, offsets, n_triangles, tiles, status, status + 1, s, &launches);
-    vxb::launch_solid_toggle(dev_vertices, dev_indices, n_triangles, g, dsub, nSub, offsets, status, grid, s,
-                             &launches);
-    vxb::launch_row_fill(grid, g.AY * g.AZ, g.ipx, s, &launches);
+    vxb::launch_solid_toggle(b, n_triangles, offsets, status, grid, s, &launches);
+    vxb::launch_row_fill(b, tab.rowBase[1], grid, s, &launches);
     e = cudaGetLastError();
     if (e != cudaSuccess) return failf(VXB_ECUDA, "%s", cudaGetErrorString(e));
     return VXB_OK;

@@ -1,0 +1,89 @@
+// The voxelization pipeline of one batch of meshes (a single voxelization is
+// a batch of one): plan and tables on the host, one stream-ordered sequence
+// of launches for every unit of the batch, and a final check on the host.
+#pragma once
+
+#include "vxb.h"
+#include "vxb_host.h"
+#include "vxb_kernels.cuh"
+#include "vxb_plan.h"
+
+#include <vector>
+
+namespace vxb {
+
+// One mesh of a batch.  The mesh arrays and the output are device memory.
+struct MeshJob {
+    const float* V;
+    const uint32_t* I;
+    const uint8_t* M;        // NULL without material output
+    uint32_t nV, nT;
+    double mn[3], mx[3];     // bounding box of the vertices
+    int nodeType;            // VXB_*_NODE
+    int nodes;               // 1: node grid, 0: plain bit array
+    vxb_request req;
+    void* out;
+    uint64_t outBytes;
+};
+
+// Shape of a job's result (vxb_plan).  Returns 0 or a vxb status.
+int gridInfo(const Plan& p, int nodeType, int nodes, vxb_grid_info* info);
+// Geometry of sub-lattice `lattice` (0 for Cartesian grids).
+PassGeom makeGeom(const Plan& p, int lattice);
+
+// Per-stage CUDA events on the launching stream (vxb_set_profiling).
+struct StageTimer {
+    static constexpr int kStages = 5;   // 0 solid, 1 surface, 2 prune, 3 emit, 4 material merge
+    bool enabled = false;
+    cudaEvent_t ev[2 * kStages] = {};
+    bool used[kStages] = {};
+    void reset() {
+        for (bool& u : used) u = false;
+    }
+    void mark(int stage, bool end, cudaStream_t s);
+    ~StageTimer();
+};
+
+class Pipeline {
+public:
+    // Plans every job, sizes the buffers and uploads the batch tables.
+    int prepare(const std::vector<MeshJob>& jobs, cudaStream_t s);
+    // Queues the whole voxelization of the prepared batch.  It neither
+    // synchronizes nor allocates, so a CUDA graph can capture it.
+    int enqueue(cudaStream_t s, StageTimer* timer);
+    // Waits for the queued work, checks the overflow and convergence flags
+    // and finishes, on the host's lead, the rare batches that need more
+    // work: a hit list that overflowed, or a pruning subspace that needed
+    // more passes than were queued.
+    int finish(cudaStream_t s);
+    // Kernels launched by the last enqueue + finish.
+    uint32_t launches = 0;
+
+    static constexpr uint32_t kPasses = 4;   // pruning passes queued per subspace
+
+private:
+    struct Group {            // pruning regions of one subspace index
+        uint32_t first, count, words, flagBase;
+    };
+    Batch batch();
+    int pruneGroupUntilStable(const Group& gr, cudaStream_t s);
+
+    std::vector<MeshJob> jobs_;
+    std::vector<Unit> units_;
+    std::vector<Group> groups_;
+    uint32_t nWork_ = 0, nRegions_ = 0, nFcc_ = 0;
+    uint64_t totalWords_ = 0, totalRows_ = 0, totalGroups_ = 0;
+    int nodeKind_ = 0, nodes_ = 1;
+    bool anyMaterials_ = false, anyCartesian_ = false, wide_ = false, aliasFill_ = false;
+    uint32_t listCap_ = 0, keysCap_ = 0;
+    // table offsets (bytes) in `tables`
+    size_t oUnits_ = 0, oWork_ = 0, oRow_ = 0, oWord_ = 0, oSplits_ = 0, oSlices_ = 0, oLater_ = 0, oRegions_ = 0,
+           oFcc_ = 0, oGroupBase_ = 0;
+    std::vector<uint8_t> blob_;   // host copy of the tables (alive while the upload runs)
+
+    DevBuf tables, status, counts, offsets, tileSums;
+    DevBuf fill, surf, fin, ranks, rankTiles;
+    DevBuf codes, unitCounts, perm, buckets, recs, ovl, hitList, keys;
+};
+
+}  // namespace vxb

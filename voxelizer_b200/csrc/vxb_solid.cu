@@ -3,8 +3,9 @@
 // FP64 as in the reference.
 //
 // The reference sorts (tile, triangle) pairs and voxelizes one tile per
-// block.  Here the work list is the flat set of (triangle, yz subspace, 4x4
-// tile) candidates over an exclusive scan of per-triangle candidate counts;
+// block.  Here the work list is the flat set of (work triangle, yz subspace,
+// 4x4 tile) candidates of every unit of the batch over an exclusive scan of
+// per-triangle candidate counts;
 // a candidate is a member of the tile's list iff one voxel centre of the
 // tile inside the triangle's clipped bounding box passes the binning test,
 // and a member toggles, for each centre of the tile inside the subspace that
@@ -83,20 +84,30 @@ __device__ __forceinline__ bool commonSpace(const BinTri& b, const SplitYZ& sp, 
     return true;
 }
 
-__global__ void solidCountKernel(const float* __restrict__ V, const uint32_t* __restrict__ I, uint32_t nT, PassGeom g,
-                                 const SplitYZ* __restrict__ splits, uint32_t nSplits, uint32_t* __restrict__ counts) {
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nT; t += gridDim.x * blockDim.x) {
-        BinTri b;
-        binSetup(V, I, t, g, b);
+// The unit and mesh triangle of work triangle wt.
+__device__ __forceinline__ uint32_t workUnit(const Batch& b, uint32_t wt, uint32_t* t) {
+    const uint32_t u = unitOf(b.workBase, b.nUnits, wt);
+    *t = wt - __ldg(b.workBase + u);
+    return u;
+}
+
+__global__ void solidCountKernel(Batch b, uint32_t nWork, uint32_t* __restrict__ counts) {
+    for (uint32_t wt = blockIdx.x * blockDim.x + threadIdx.x; wt < nWork; wt += gridDim.x * blockDim.x) {
+        uint32_t t;
+        const Unit& U = b.units[workUnit(b, wt, &t)];
+        const PassGeom g = U.g;
+        BinTri bt;
+        binSetup(U.V, U.I, t, g, bt);
         uint32_t c = 0;
-        if (!binRejected(b)) {
-            for (uint32_t s = 0; s < nSplits; ++s) {
+        if (!binRejected(bt)) {
+            const SplitYZ* splits = b.splits + U.splitBase;
+            for (uint32_t s = 0; s < U.nSplits; ++s) {
                 uint32_t lo[2], hi[2];
-                if (!commonSpace(b, splits[s], lo, hi)) continue;
+                if (!commonSpace(bt, splits[s], lo, hi)) continue;
                 c += ((hi[0] - 1) / 4 - lo[0] / 4 + 1) * ((hi[1] - 1) / 4 - lo[1] / 4 + 1);
             }
         }
-        counts[t] = c;
+        counts[wt] = c;
     }
 }
 
@@ -107,11 +118,14 @@ struct SolidStage {
     D3 n;                           // cross(v0 - v2, v1 - v0)
     double ex[3], ey[3], ed[3];     // generation edges (oriented by n.x)
     uint32_t tl;                    // top-left flags of the generation edges
+    uint32_t unit;
 };
 
-__device__ __forceinline__ void stageSolid(SolidStage& st, const float* V, const uint32_t* I, uint32_t t,
-                                           const PassGeom& g) {
-    binSetup(V, I, t, g, st.b);
+__device__ __forceinline__ void stageSolid(SolidStage& st, const Batch& b, uint32_t wt) {
+    uint32_t t;
+    st.unit = workUnit(b, wt, &t);
+    const Unit& unit = b.units[st.unit];
+    binSetup(unit.V, unit.I, t, unit.g, st.b);
     const D3* v = st.b.v;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
@@ -141,9 +155,13 @@ __device__ __forceinline__ void stageSolid(SolidStage& st, const float* V, const
 // (traverseTilesForOverlaps, src/voxelizer.cu:980-1033), then
 // generateVoxelization's per-centre work (1344-1462) for the tile's centres
 // inside the subspace.
-__device__ __forceinline__ void solidCandidate(const SolidStage& st, const SplitYZ* __restrict__ splits,
-                                               uint32_t nSplits, uint32_t local, const PassGeom& g,
-                                               uint32_t* __restrict__ toggles) {
+__device__ __forceinline__ void solidCandidate(const SolidStage& st, const Batch& b, uint32_t local,
+                                               uint32_t* __restrict__ fill) {
+    const Unit& U = b.units[st.unit];
+    const PassGeom& g = U.g;
+    const SplitYZ* __restrict__ splits = b.splits + U.splitBase;
+    const uint32_t nSplits = U.nSplits;
+    uint32_t* __restrict__ toggles = fill + U.wordBase;
     const double d = g.d;
     uint32_t lo[2] = {0, 0}, hi[2] = {0, 0};
     SplitYZ sp = splits[0];
@@ -194,12 +212,10 @@ __device__ __forceinline__ void solidCandidate(const SolidStage& st, const Split
     }
 }
 
-__global__ void __launch_bounds__(kBlock, 3) solidToggleKernel(const float* __restrict__ V,
-                                                            const uint32_t* __restrict__ I, uint32_t nT, PassGeom g,
-                                                            const SplitYZ* __restrict__ splits, uint32_t nSplits,
-                                                            const uint32_t* __restrict__ offsets,
-                                                            const uint32_t* __restrict__ totalPtr,
-                                                            uint32_t* __restrict__ toggles) {
+__global__ void __launch_bounds__(kBlock, 3) solidToggleKernel(Batch b, uint32_t nWork,
+                                                               const uint32_t* __restrict__ offsets,
+                                                               const uint32_t* __restrict__ totalPtr,
+                                                               uint32_t* __restrict__ fill) {
     __shared__ SolidStage stage[kSlots];
     __shared__ uint32_t stOff[kSlots + 1];
     __shared__ uint32_t tFirst, nStage;
@@ -207,15 +223,15 @@ __global__ void __launch_bounds__(kBlock, 3) solidToggleKernel(const float* __re
     for (uint32_t base = blockIdx.x * kBlock; base < total; base += gridDim.x * kBlock) {
         const uint32_t last = min(base + kBlock, total) - 1;
         if (threadIdx.x == 0) {
-            const uint32_t t0 = findOwner(offsets, nT, base);
-            const uint32_t t1 = findOwner(offsets, nT, last);
+            const uint32_t t0 = findOwner(offsets, nWork, base);
+            const uint32_t t1 = findOwner(offsets, nWork, last);
             tFirst = t0;
             nStage = min(t1 - t0 + 1, kSlots);
         }
         __syncthreads();
         const uint32_t t0 = tFirst, ns = nStage;
         if (threadIdx.x < ns) {
-            stageSolid(stage[threadIdx.x], V, I, t0 + threadIdx.x, g);
+            stageSolid(stage[threadIdx.x], b, t0 + threadIdx.x);
             stOff[threadIdx.x] = __ldg(offsets + t0 + threadIdx.x);
         }
         if (threadIdx.x == 0) stOff[ns] = __ldg(offsets + t0 + ns);
@@ -229,12 +245,12 @@ __global__ void __launch_bounds__(kBlock, 3) solidToggleKernel(const float* __re
                     if (stOff[mid] <= item) lo = mid;
                     else hi = mid;
                 }
-                solidCandidate(stage[lo], splits, nSplits, item - stOff[lo], g, toggles);
+                solidCandidate(stage[lo], b, item - stOff[lo], fill);
             } else {
-                const uint32_t t = findOwner(offsets, nT, item);
+                const uint32_t wt = findOwner(offsets, nWork, item);
                 SolidStage st;
-                stageSolid(st, V, I, t, g);
-                solidCandidate(st, splits, nSplits, item - __ldg(offsets + t), g, toggles);
+                stageSolid(st, b, wt);
+                solidCandidate(st, b, item - __ldg(offsets + wt), fill);
             }
         }
         __syncthreads();
@@ -242,12 +258,15 @@ __global__ void __launch_bounds__(kBlock, 3) solidToggleKernel(const float* __re
 }
 
 // Toggle bits -> solid runs, one warp per row: bit x = XOR of toggles <= x.
-__global__ void rowFillKernel(uint32_t* __restrict__ words, uint32_t rows, uint32_t ipx) {
+__global__ void rowFillKernel(Batch b, uint64_t nRows, uint32_t* __restrict__ fill) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warpsPerBlock = blockDim.x >> 5;
-    for (uint32_t row = blockIdx.x * warpsPerBlock + (threadIdx.x >> 5); row < rows;
-         row += gridDim.x * warpsPerBlock) {
-        uint32_t* r = words + (size_t)row * ipx;
+    for (uint64_t row = (uint64_t)blockIdx.x * warpsPerBlock + (threadIdx.x >> 5); row < nRows;
+         row += (uint64_t)gridDim.x * warpsPerBlock) {
+        const uint32_t u = unitOf(b.rowBase, b.nUnits, row);
+        const Unit& U = b.units[u];
+        const uint32_t ipx = U.g.ipx;
+        uint32_t* r = fill + U.wordBase + (row - __ldg(b.rowBase + u)) * ipx;
         uint32_t carry = 0;
         for (uint32_t base = 0; base < ipx; base += 32) {
             const uint32_t k = base + lane;
@@ -264,21 +283,19 @@ __global__ void rowFillKernel(uint32_t* __restrict__ words, uint32_t rows, uint3
 
 }  // namespace
 
-void launch_solid_count(const float* V, const uint32_t* I, uint32_t nT, PassGeom g, const SplitYZ* splits,
-                        uint32_t nSplits, uint32_t* counts, cudaStream_t s, uint32_t* launches) {
-    solidCountKernel<<<gridFor(nT, 256), 256, 0, s>>>(V, I, nT, g, splits, nSplits, counts);
+void launch_solid_count(const Batch& b, uint32_t nWork, uint32_t* counts, cudaStream_t s, uint32_t* launches) {
+    solidCountKernel<<<gridFor(nWork, 256), 256, 0, s>>>(b, nWork, counts);
     *launches += 1;
 }
 
-void launch_solid_toggle(const float* V, const uint32_t* I, uint32_t nT, PassGeom g, const SplitYZ* splits,
-                         uint32_t nSplits, const uint32_t* offsets, const uint32_t* total, uint32_t* toggles,
-                         cudaStream_t s, uint32_t* launches) {
-    solidToggleKernel<<<148 * 3, kBlock, 0, s>>>(V, I, nT, g, splits, nSplits, offsets, total, toggles);
+void launch_solid_toggle(const Batch& b, uint32_t nWork, const uint32_t* offsets, const uint32_t* total,
+                         uint32_t* fill, cudaStream_t s, uint32_t* launches) {
+    solidToggleKernel<<<148 * 3, kBlock, 0, s>>>(b, nWork, offsets, total, fill);
     *launches += 1;
 }
 
-void launch_row_fill(uint32_t* words, uint32_t rows, uint32_t ipx, cudaStream_t s, uint32_t* launches) {
-    rowFillKernel<<<gridFor((uint64_t)rows * 32, 256), 256, 0, s>>>(words, rows, ipx);
+void launch_row_fill(const Batch& b, uint64_t nRows, uint32_t* fill, cudaStream_t s, uint32_t* launches) {
+    rowFillKernel<<<gridFor(nRows * 32, 256), 256, 0, s>>>(b, nRows, fill);
     *launches += 1;
 }
 

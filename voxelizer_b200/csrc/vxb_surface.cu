@@ -137,31 +137,43 @@ __device__ __forceinline__ uint32_t bucketOf(uint32_t code, uint32_t units) {
     return units ? ((code >> 30) - 1u) * 3u + ((code >> 28) & 3u) : kNone;
 }
 
-// Pass 1 (mesh order): code and units per triangle, triangles per bucket.
-__global__ void surfaceClassifyKernel(const float* __restrict__ V, const uint32_t* __restrict__ I, uint32_t nT,
-                                      PassGeom g, uint32_t* __restrict__ codes, uint32_t* __restrict__ units,
-                                      uint32_t* __restrict__ bucketCount) {
+// The unit and mesh triangle of work triangle wt.
+__device__ __forceinline__ uint32_t workUnit(const Batch& b, uint32_t wt, uint32_t* t) {
+    const uint32_t u = unitOf(b.workBase, b.nUnits, wt);
+    *t = wt - __ldg(b.workBase + u);
+    return u;
+}
+
+// Pass 1 (work-triangle order): code and units per triangle, triangles per
+// bucket.  Units without materials have no surface pass.
+__global__ void surfaceClassifyKernel(Batch b, uint32_t nWork, uint32_t* __restrict__ codes,
+                                      uint32_t* __restrict__ units, uint32_t* __restrict__ bucketCount) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < nT; base += stride) {
-        const uint32_t t = base + lane;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < nWork; base += stride) {
+        const uint32_t wt = base + lane;
         uint32_t code = 0, u = 0;
-        if (t < nT) {
-            F3 v[3];
-            loadTriF(V, I, t, v);
-            const IBox full = voxBoundsHalf(v, g);
-            code = classifyTri(v, full);
-            u = surfUnits(gridClamp(full, g), code);
-            codes[t] = code;
-            units[t] = u;
+        if (wt < nWork) {
+            uint32_t t;
+            const Unit& U = b.units[workUnit(b, wt, &t)];
+            if (U.materials) {
+                const PassGeom g = U.g;
+                F3 v[3];
+                loadTriF(U.V, U.I, t, v);
+                const IBox full = voxBoundsHalf(v, g);
+                code = classifyTri(v, full);
+                u = surfUnits(gridClamp(full, g), code);
+            }
+            codes[wt] = code;
+            units[wt] = u;
         }
-        const uint32_t b = bucketOf(code, u);
-        const uint32_t peers = __match_any_sync(kFull, b);
-        if (b != kNone && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(bucketCount + b, (uint32_t)__popc(peers));
+        const uint32_t bk = bucketOf(code, u);
+        const uint32_t peers = __match_any_sync(kFull, bk);
+        if (bk != kNone && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(bucketCount + bk, (uint32_t)__popc(peers));
     }
 }
 
-// Pass 2 (mesh order): position of every triangle with work in the
+// Pass 2 (work-triangle order): position of every triangle with work in the
 // partitioned order; unitsP holds its units there (zero past the end).
 __global__ void surfaceScatterKernel(const uint32_t* __restrict__ codes, const uint32_t* __restrict__ units,
                                      uint32_t nT, const uint32_t* __restrict__ bucketCount,
@@ -204,7 +216,7 @@ struct __align__(16) SurfRec {
     uint32_t tri;       // mesh index (PartialNode keys)
     float v0[3];        // first vertex (3D depth range)
     float n[3];         // normal (3D depth range)
-    uint32_t pad;
+    uint32_t unit;      // unit of the batch
 };
 struct __align__(16) SurfOvl {
     Overlap o[3];
@@ -252,29 +264,32 @@ template <int OT> __device__ __forceinline__ bool overlapTest(const Overlap& o, 
 }
 
 // Pass 3 (partitioned order): the set-up record of every triangle with work.
-__global__ void surfaceSetupKernel(const float* __restrict__ V, const uint32_t* __restrict__ I,
-                                   const uint8_t* __restrict__ M, const uint32_t* __restrict__ perm,
-                                   const uint32_t* __restrict__ codes, const uint32_t* __restrict__ bucketCount,
-                                   PassGeom g, SurfRec* __restrict__ recs, SurfOvl* __restrict__ ovl) {
+__global__ void surfaceSetupKernel(Batch b, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ codes,
+                                   const uint32_t* __restrict__ bucketCount, SurfRec* __restrict__ recs,
+                                   SurfOvl* __restrict__ ovl) {
     uint32_t nP = 0;
 #pragma unroll
     for (uint32_t k = 0; k < kSurfaceBuckets; ++k) nP += __ldg(bucketCount + k);
     for (uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x; pos < nP; pos += gridDim.x * blockDim.x) {
-        const uint32_t t = __ldg(perm + pos);
+        const uint32_t wt = __ldg(perm + pos);
+        uint32_t t;
+        const uint32_t unit = workUnit(b, wt, &t);
+        const Unit& U = b.units[unit];
+        const PassGeom g = U.g;
         F3 v[3];
-        loadTriF(V, I, t, v);
-        const uint32_t code = __ldg(codes + t);
+        loadTriF(U.V, U.I, t, v);
+        const uint32_t code = __ldg(codes + wt);
         const uint32_t bb = code >> 30, axis = (code >> 28) & 3u;
-        const IBox b = gridClamp(voxBoundsHalf(v, g), g);
+        const IBox box = gridClamp(voxBoundsHalf(v, g), g);
         SurfRec r;
 #pragma unroll
-        for (int a = 0; a < 3; ++a) { r.lo[a] = b.lo[a]; r.hi[a] = b.hi[a]; }
+        for (int a = 0; a < 3; ++a) { r.lo[a] = box.lo[a]; r.hi[a] = box.hi[a]; }
         r.code = code;
-        r.key = (bb << 8) | (M ? __ldg(M + t) : 0u);
+        r.key = (bb << 8) | (U.M ? __ldg(U.M + t) : 0u);
         r.tri = t;
         r.v0[0] = v[0].x; r.v0[1] = v[0].y; r.v0[2] = v[0].z;
         r.n[0] = r.n[1] = r.n[2] = 0.0f;
-        r.pad = 0;
+        r.unit = unit;
         const float d = g.df;
         if (bb == 2) {
             const F3 n = crossF<site::CRF_2D>(subF(v[0], v[2]), subF(v[1], v[0]));
@@ -346,29 +361,34 @@ struct WarpStage {
     uint32_t* count;
 };
 
+// Where a unit's surface bits live.
+struct UnitGrid {
+    uint64_t wordBase;   // first word of the unit in the surface arena
+    uint32_t AY, ipx;
+};
+
 // processVoxel of the surface pass, coordinates with the 1-voxel padding.
 // mode 0: set the bit and append (bit position << 24 | key) to the hit list;
 // mode 1: merge the key at the voxel's rank (surface bits are complete).
 struct Sink {
-    uint32_t* bits;          // surface grid of this lattice
-    uint64_t posBase;        // bit position of bits[0] in the rank space
+    uint32_t* bits;            // surface arena
     const uint32_t* wordRank;  // exclusive popcount prefix per word (mode 1)
-    void* keys;              // compact key array (mode 1)
+    void* keys;                // compact key array (mode 1)
+    uint32_t keysCap;          // keys at ranks past it are dropped
     unsigned long long* list;
     uint32_t* listCount;
     uint32_t listCap;
     int mode;
-    int wide;                // 64-bit keys (PartialNode)
-    PassGeom g;
-    __device__ __forceinline__ void operator()(int xi, int yi, int zi, uint64_t key, const WarpStage& ws) const {
+    int wide;                  // 64-bit keys (PartialNode)
+    __device__ __forceinline__ void operator()(int xi, int yi, int zi, uint64_t key, const UnitGrid& ug,
+                                               const WarpStage& ws) const {
         const uint32_t x = (uint32_t)xi, y = (uint32_t)yi, z = (uint32_t)zi;
-        const size_t w = ((size_t)z * g.AY + y) * g.ipx + (x >> 5);
+        const uint64_t w = ug.wordBase + ((uint64_t)z * ug.AY + y) * ug.ipx + (x >> 5);
         const uint32_t b = x & 31u;
         const uint32_t bit = 0x80000000u >> b;
         if (mode == 0) {
             atomicOr(bits + w, bit);
-            const unsigned long long e = ((unsigned long long)(posBase + (uint64_t)w * 32 + b) << 24) |
-                                         (key & 0xFFFFFFull);
+            const unsigned long long e = ((unsigned long long)(w * 32 + b) << 24) | (key & 0xFFFFFFull);
             const uint32_t at = atomicAdd(ws.count, 1u);
             if (at < kStageHits) {
                 ws.buf[at] = e;
@@ -378,7 +398,8 @@ struct Sink {
             }
         } else {
             const uint32_t word = __ldg(bits + w);
-            const uint32_t r = __ldg(wordRank + (posBase >> 5) + w) + (b ? __popc(word >> (32 - b)) : 0u);
+            const uint32_t r = __ldg(wordRank + w) + (b ? __popc(word >> (32 - b)) : 0u);
+            if (r >= keysCap) return;
             if (wide) atomicMax(reinterpret_cast<unsigned long long*>(keys) + r, (unsigned long long)key);
             else atomicMax(reinterpret_cast<uint32_t*>(keys) + r, (uint32_t)key);
         }
@@ -405,14 +426,14 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
                                             const SurfOvl* __restrict__ ov, uint32_t u, const PassGeom& g,
                                             const uint32_t* __restrict__ slices, const uint32_t* sliceOff,
                                             const uint32_t* sliceN, uint64_t key, const Sink& sink,
-                                            const WarpStage& ws) {
+                                            const UnitGrid& ug, const WarpStage& ws) {
     const float d = g.df;
     const uint32_t ex = (uint32_t)(r.hi[0] - r.lo[0] + 1), ey = (uint32_t)(r.hi[1] - r.lo[1] + 1);
     if (bb == 1) {
         // process1DTriangles (3306-3411): every voxel of the line, no test.
-        if (axis == 0) sink(r.lo[0] + (int)u + 1, r.lo[1] + 1, r.lo[2] + 1, key, ws);
-        else if (axis == 1) sink(r.lo[0] + 1, r.lo[1] + (int)u + 1, r.lo[2] + 1, key, ws);
-        else sink(r.lo[0] + 1, r.lo[1] + 1, r.lo[2] + (int)u + 1, key, ws);
+        if (axis == 0) sink(r.lo[0] + (int)u + 1, r.lo[1] + 1, r.lo[2] + 1, key, ug, ws);
+        else if (axis == 1) sink(r.lo[0] + 1, r.lo[1] + (int)u + 1, r.lo[2] + 1, key, ug, ws);
+        else sink(r.lo[0] + 1, r.lo[1] + 1, r.lo[2] + (int)u + 1, key, ug, ws);
         return;
     }
     if (bb == 2) {
@@ -421,17 +442,17 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
             const int j = r.lo[1] + (int)(u % ey), k = r.lo[2] + (int)(u / ey);
             if (overlapTest<site::OT_2D_YZ>(od, vbComp<site::PC_2D>(j, g.mnf[1], d),
                                             vbComp<site::PC_2D>(k, g.mnf[2], d)))
-                sink(r.lo[0] + 1, j + 1, k + 1, key, ws);
+                sink(r.lo[0] + 1, j + 1, k + 1, key, ug, ws);
         } else if (axis == 1) {
             const int i = r.lo[0] + (int)(u % ex), k = r.lo[2] + (int)(u / ex);
             if (overlapTest<site::OT_2D_ZX>(od, vbComp<site::PC_2D>(k, g.mnf[2], d),
                                             vbComp<site::PC_2D>(i, g.mnf[0], d)))
-                sink(i + 1, r.lo[1] + 1, k + 1, key, ws);
+                sink(i + 1, r.lo[1] + 1, k + 1, key, ug, ws);
         } else {
             const int i = r.lo[0] + (int)(u % ex), j = r.lo[1] + (int)(u / ex);
             if (overlapTest<site::OT_2D_XY>(od, vbComp<site::PC_2D>(i, g.mnf[0], d),
                                             vbComp<site::PC_2D>(j, g.mnf[1], d)))
-                sink(i + 1, j + 1, r.lo[2] + 1, key, ws);
+                sink(i + 1, j + 1, r.lo[2] + 1, key, ug, ws);
         }
         return;
     }
@@ -451,11 +472,11 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
             const int lo = max(r.lo[0], (int)__ldg(sl + 2 * s)), hi = min(r.hi[0], (int)__ldg(sl + 2 * s + 1) - 1);
             if (lo > hi || d0 > hi || d1 < lo) continue;
             const int a = d0 < lo ? lo : d0, c = d1 > hi ? hi : d1;
-            if (a == c) { sink(a + 1, j + 1, k + 1, key, ws); continue; }
+            if (a == c) { sink(a + 1, j + 1, k + 1, key, ug, ws); continue; }
             for (int i = a; i <= c; ++i) {
                 p.x = vbComp<site::PC_3DL>(i, g.mnf[0], d);
                 if (overlapTest<site::OT_3DX_ZX>(ov->o[1], p.z, p.x) && overlapTest<site::OT_3DX_XY>(ov->o[2], p.x, p.y))
-                    sink(i + 1, j + 1, k + 1, key, ws);
+                    sink(i + 1, j + 1, k + 1, key, ug, ws);
             }
         }
     } else if (axis == 1) {
@@ -469,11 +490,11 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
             const int lo = max(r.lo[1], (int)__ldg(sl + 2 * s)), hi = min(r.hi[1], (int)__ldg(sl + 2 * s + 1) - 1);
             if (lo > hi || d0 > hi || d1 < lo) continue;
             const int a = d0 < lo ? lo : d0, c = d1 > hi ? hi : d1;
-            if (a == c) { sink(i + 1, a + 1, k + 1, key, ws); continue; }
+            if (a == c) { sink(i + 1, a + 1, k + 1, key, ug, ws); continue; }
             for (int j = a; j <= c; ++j) {
                 p.y = vbComp<site::PC_3DL>(j, g.mnf[1], d);
                 if (overlapTest<site::OT_3DY_XY>(ov->o[2], p.x, p.y) && overlapTest<site::OT_3DY_YZ>(ov->o[0], p.y, p.z))
-                    sink(i + 1, j + 1, k + 1, key, ws);
+                    sink(i + 1, j + 1, k + 1, key, ug, ws);
             }
         }
     } else {
@@ -487,11 +508,11 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
             const int lo = max(r.lo[2], (int)__ldg(sl + 2 * s)), hi = min(r.hi[2], (int)__ldg(sl + 2 * s + 1) - 1);
             if (lo > hi || d0 > hi || d1 < lo) continue;
             const int a = d0 < lo ? lo : d0, c = d1 > hi ? hi : d1;
-            if (a == c) { sink(i + 1, j + 1, a + 1, key, ws); continue; }
+            if (a == c) { sink(i + 1, j + 1, a + 1, key, ug, ws); continue; }
             for (int k = a; k <= c; ++k) {
                 p.z = vbComp<site::PC_3DL>(k, g.mnf[2], d);
                 if (overlapTest<site::OT_3DZ_YZ>(ov->o[0], p.y, p.z) && overlapTest<site::OT_3DZ_ZX>(ov->o[1], p.z, p.x))
-                    sink(i + 1, j + 1, k + 1, key, ws);
+                    sink(i + 1, j + 1, k + 1, key, ug, ws);
             }
         }
     }
@@ -522,12 +543,11 @@ __device__ __forceinline__ uint32_t warpFindOwner(const uint32_t* __restrict__ o
 // gives every lane its owner.  The class and axis of a position follow from
 // the bucket bounds, so the projection edge functions load together with
 // the record.
-__global__ void __launch_bounds__(kBlock) surfaceWorkKernel(Sink sink, const SurfRec* __restrict__ recs,
+__global__ void __launch_bounds__(kBlock) surfaceWorkKernel(Sink sink, Batch b, const SurfRec* __restrict__ recs,
                                                             const SurfOvl* __restrict__ ovl,
                                                             const uint32_t* __restrict__ off, uint32_t n,
                                                             const uint32_t* __restrict__ totalPtr,
-                                                            const uint32_t* __restrict__ bucketCount, PassGeom g,
-                                                            const uint32_t* __restrict__ slices, SliceTable st) {
+                                                            const uint32_t* __restrict__ bucketCount) {
     __shared__ unsigned long long stageBuf[kBlock / 32][kStageHits];
     __shared__ uint32_t stageCount[kBlock / 32];
     __shared__ uint32_t bucketEnd[kSurfaceBuckets];
@@ -573,7 +593,14 @@ __global__ void __launch_bounds__(kBlock) surfaceWorkKernel(Sink sink, const Sur
                 const SurfRec r = recs[pos];
                 const uint64_t key = sink.wide ? (((uint64_t)bb << 40) | ((uint64_t)(r.key & 255u) << 32) | r.tri)
                                                : (uint64_t)r.key;
-                surfaceItem(bb, axis, r, od, ovl + pos, item - ok, g, slices, st.off, st.n, key, sink, ws);
+                const Unit& U = b.units[r.unit];
+                const PassGeom g = U.g;
+                const UnitGrid ug{U.wordBase, g.AY, g.ipx};
+                const uint32_t sliceOff[3] = {U.sliceBase, U.sliceBase + U.sliceN[0],
+                                              U.sliceBase + U.sliceN[0] + U.sliceN[1]};
+                const uint32_t sliceN[3] = {U.sliceN[0], U.sliceN[1], U.sliceN[2]};
+                surfaceItem(bb, axis, r, od, ovl + pos, item - ok, g, b.slices, sliceOff, sliceN, key, sink, ug,
+                            ws);
             }
             __syncwarp();
             if (sink.mode == 0 && *ws.count >= kFlushAt) sink.flush(ws, lane);
@@ -667,8 +694,8 @@ __global__ void rankAddKernel(uint32_t* ranks, uint64_t n, const uint32_t* __res
         ranks[i] += tileSums[i / kRankTile];
 }
 
-__global__ void zeroKeysKernel(void* keys, const uint32_t* __restrict__ countPtr, int wide) {
-    const uint32_t n = *countPtr;
+__global__ void zeroKeysKernel(void* keys, const uint32_t* __restrict__ countPtr, uint32_t cap, int wide) {
+    const uint32_t n = min(*countPtr, cap);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         if (wide) reinterpret_cast<unsigned long long*>(keys)[i] = 0ull;
         else reinterpret_cast<uint32_t*>(keys)[i] = 0u;
@@ -678,7 +705,7 @@ __global__ void zeroKeysKernel(void* keys, const uint32_t* __restrict__ countPtr
 // Max-merges the hit list into the rank-indexed key array.
 __global__ void mergeKeysKernel(const unsigned long long* __restrict__ list, const uint32_t* __restrict__ countPtr,
                                 uint32_t cap, const uint32_t* __restrict__ bits, const uint32_t* __restrict__ ranks,
-                                uint32_t* keys) {
+                                uint32_t* keys, uint32_t keysCap) {
     const uint32_t n = min(*countPtr, cap);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const unsigned long long e = list[i];
@@ -687,41 +714,40 @@ __global__ void mergeKeysKernel(const unsigned long long* __restrict__ list, con
         const uint32_t b = (uint32_t)(pos & 31u);
         const uint32_t word = __ldg(bits + w);
         const uint32_t r = __ldg(ranks + w) + (b ? __popc(word >> (32 - b)) : 0u);
-        atomicMax(keys + r, (uint32_t)(e & 0xFFFFFFull));
+        if (r < keysCap) atomicMax(keys + r, (uint32_t)(e & 0xFFFFFFull));
     }
 }
 
 }  // namespace
 
-void launch_surface_prepare(const float* V, const uint32_t* I, const uint8_t* M, uint32_t nT, PassGeom g,
-                            uint32_t* codes, uint32_t* units, uint32_t* buckets, uint32_t* perm, uint32_t* unitsP,
-                            void* recs, void* ovl, cudaStream_t s, uint32_t* launches) {
-    const uint32_t grid = gridFor(nT, 256);
-    surfaceClassifyKernel<<<grid, 256, 0, s>>>(V, I, nT, g, codes, units, buckets);
-    surfaceScatterKernel<<<grid, 256, 0, s>>>(codes, units, nT, buckets, buckets + kSurfaceBuckets, perm, unitsP);
-    surfaceSetupKernel<<<grid, 256, 0, s>>>(V, I, M, perm, codes, buckets, g, static_cast<SurfRec*>(recs),
+void launch_surface_prepare(const Batch& b, uint32_t nWork, uint32_t* codes, uint32_t* units, uint32_t* buckets,
+                            uint32_t* perm, uint32_t* unitsP, void* recs, void* ovl, cudaStream_t s,
+                            uint32_t* launches) {
+    const uint32_t grid = gridFor(nWork, 256);
+    surfaceClassifyKernel<<<grid, 256, 0, s>>>(b, nWork, codes, units, buckets);
+    surfaceScatterKernel<<<grid, 256, 0, s>>>(codes, units, nWork, buckets, buckets + kSurfaceBuckets, perm, unitsP);
+    surfaceSetupKernel<<<grid, 256, 0, s>>>(b, perm, codes, buckets, static_cast<SurfRec*>(recs),
                                             static_cast<SurfOvl*>(ovl));
     *launches += 3;
 }
 
-void launch_surface_work(int mode, int wide, const void* recs, const void* ovl, const uint32_t* offsets, uint32_t nT,
-                         const uint32_t* total, const uint32_t* buckets, PassGeom g, const uint32_t* slices, SliceTable st, uint32_t* surfBits,
-                         uint64_t posBase, const uint32_t* ranks, void* keys, unsigned long long* list,
-                         uint32_t* listCount, uint32_t listCap, cudaStream_t s, uint32_t* launches) {
+void launch_surface_work(int mode, int wide, const Batch& b, const void* recs, const void* ovl,
+                         const uint32_t* offsets, uint32_t nWork, const uint32_t* total, const uint32_t* buckets,
+                         uint32_t* surf, const uint32_t* ranks, void* keys, uint32_t keysCap,
+                         unsigned long long* list, uint32_t* listCount, uint32_t listCap, cudaStream_t s,
+                         uint32_t* launches) {
     Sink sink;
-    sink.bits = surfBits;
-    sink.posBase = posBase;
+    sink.bits = surf;
     sink.wordRank = ranks;
     sink.keys = keys;
+    sink.keysCap = keysCap;
     sink.list = list;
     sink.listCount = listCount;
     sink.listCap = listCap;
     sink.mode = mode;
     sink.wide = wide;
-    sink.g = g;
-    surfaceWorkKernel<<<148 * 8, kBlock, 0, s>>>(sink, static_cast<const SurfRec*>(recs),
-                                                  static_cast<const SurfOvl*>(ovl), offsets, nT, total, buckets, g,
-                                                  slices, st);
+    surfaceWorkKernel<<<148 * 8, kBlock, 0, s>>>(sink, b, static_cast<const SurfRec*>(recs),
+                                                  static_cast<const SurfOvl*>(ovl), offsets, nWork, total, buckets);
     *launches += 1;
 }
 
@@ -734,15 +760,16 @@ void launch_surface_rank(const uint32_t* bits, uint64_t words, uint32_t* ranks, 
     *launches += 3;
 }
 
-void launch_surface_keys_zero(void* keys, const uint32_t* count, int wide, cudaStream_t s, uint32_t* launches) {
-    zeroKeysKernel<<<148 * 8, 256, 0, s>>>(keys, count, wide);
+void launch_surface_keys_zero(void* keys, const uint32_t* count, uint32_t cap, int wide, cudaStream_t s,
+                              uint32_t* launches) {
+    zeroKeysKernel<<<148 * 8, 256, 0, s>>>(keys, count, cap, wide);
     *launches += 1;
 }
 
 void launch_surface_merge(const unsigned long long* list, const uint32_t* listCount, uint32_t listCap,
-                          const uint32_t* bits, const uint32_t* ranks, uint32_t* keys, cudaStream_t s,
-                          uint32_t* launches) {
-    mergeKeysKernel<<<148 * 8, 256, 0, s>>>(list, listCount, listCap, bits, ranks, keys);
+                          const uint32_t* bits, const uint32_t* ranks, uint32_t* keys, uint32_t keysCap,
+                          cudaStream_t s, uint32_t* launches) {
+    mergeKeysKernel<<<148 * 8, 256, 0, s>>>(list, listCount, listCap, bits, ranks, keys, keysCap);
     *launches += 1;
 }
 
