@@ -118,14 +118,22 @@ struct PruneRegion {
     SplitYZ split;
     uint32_t wordStart;
 };
-// One in-place pruning pass over `n` regions (totalWords words).  Region r
-// sets flags[(flagBase + r) * passes + pass] if it changed anything; for
-// pass > 0 a region whose previous pass changed nothing is skipped.
-// Neighbours in later subspaces are read from fill | surf (surf may be NULL).
-void launch_prune(const Batch& b, const PruneRegion* regions, uint32_t n, uint32_t totalWords, uint32_t* solid,
+// Pruning of one subspace index.  launch_prune: the first pass over every
+// word of its `n` regions (groupWords words in all), appending each changed
+// word to `list`; launch_prune_list: a later pass over the words next to the
+// changes listed in `in`, appending its own changes to `out`.  Lists hold
+// (region << 32 | word) entries, at most `cap`; past it *overflow is set and
+// the passes are no longer complete.  A region that changed in pass p sets
+// flags[(flagBase + region) * passes + p].  Neighbours in later subspaces
+// are read from fill | surf (surf may be NULL).
+void launch_prune(const Batch& b, const PruneRegion* regions, uint32_t n, uint32_t groupWords, uint32_t* solid,
                   const uint32_t* fill, const uint32_t* surf, uint32_t* flags, uint32_t flagBase, uint32_t passes,
-                  uint32_t pass, cudaStream_t s, uint32_t* launches);
-// Cartesian node grids of every unit of the batch (all of one node kind).
+                  unsigned long long* list, uint32_t* count, uint32_t cap, uint32_t* overflow, cudaStream_t s,
+                  uint32_t* launches);
+void launch_prune_list(const Batch& b, const PruneRegion* regions, uint32_t* solid, const uint32_t* fill,
+                       const uint32_t* surf, uint32_t* flags, uint32_t flagBase, uint32_t passes, uint32_t pass,
+                       const unsigned long long* in, const uint32_t* inCount, unsigned long long* out,
+                       uint32_t* outCount, uint32_t cap, uint32_t* overflow, cudaStream_t s, uint32_t* launches);
 // Keys at ranks >= keysCap read as 0.
 void launch_emit_cartesian(int nodeKind, const Batch& b, uint64_t totalWords, const uint32_t* finalSolid,
                            const uint32_t* fill, const uint32_t* surf, const uint32_t* ranks, const void* keys,

@@ -30,73 +30,176 @@ __global__ void combineKernel(const uint4* __restrict__ a, const uint4* __restri
     }
 }
 
-// One pruning pass over the regions of one launch (fillNodeList2 and the
-// host loop, src/voxelizer.cu:1790-1913, src/host_side.cpp:1183-1206): a
-// solid node stays solid iff each axis has a solid neighbour.  Words are
-// updated in place; passes repeat until none changes, which reaches the same
-// greatest fixed point as the reference's in-place node passes.  Neighbours
-// in a later subspace are read from the unpruned grid (fill | surf): the
-// reference prunes subspaces in order, so they are still unpruned when this
-// one converges.  Reading them explicitly makes a subspace's result
-// independent of how far later subspaces have been pruned, which lets the
-// host queue passes for all subspaces before checking convergence.
-__global__ void pruneKernel(Batch b, const PruneRegion* __restrict__ regions, uint32_t nRegions, uint32_t totalWords,
+// Pruning (fillNodeList2 and the host loop, src/voxelizer.cu:1790-1913,
+// src/host_side.cpp:1183-1206): a solid node stays solid iff each axis has a
+// solid neighbour.  Passes repeat until nothing changes, which reaches the
+// same greatest fixed point as the reference's in-place node passes.
+// Neighbours in a later subspace are read from the unpruned grid (fill |
+// surf): the reference prunes subspaces in order, so they are still unpruned
+// when this one converges.  Reading them explicitly makes a subspace's
+// result independent of how far later subspaces have been pruned, which lets
+// the host queue passes for all subspaces before checking convergence.
+//
+// The first pass visits every word of the subspace index's regions and lists
+// the words it changed; each later pass revisits only the words next to the
+// previous pass's changes (a word can only change when a neighbour did).
+// Later passes may visit a word from several threads, so they clear bits with
+// atomicAnd: the solid set only shrinks, and every change schedules its
+// neighbours, so the passes converge to the same fixed point.
+
+// The data of one pruning region.
+struct PruneView {
+    uint32_t* S;
+    const uint32_t* F;
+    const uint32_t* Sf;        // NULL without materials
+    const uint8_t* yLater;
+    uint32_t ipx, AY, AZ, y0, y1, z0, z1;
+};
+
+__device__ __forceinline__ PruneView pruneView(const Batch& b, const PruneRegion& R, uint32_t* solid,
+                                               const uint32_t* fill, const uint32_t* surf) {
+    const Unit& U = b.units[R.unit];
+    PruneView v;
+    v.S = solid + U.wordBase;
+    v.F = fill + U.wordBase;
+    v.Sf = (surf && U.materials) ? surf + U.wordBase : nullptr;
+    v.yLater = b.later + U.laterBase;
+    v.ipx = U.g.ipx;
+    v.AY = U.g.AY;
+    v.AZ = U.g.AZ;
+    v.y0 = R.split.y0;
+    v.y1 = R.split.y1;
+    v.z0 = R.split.z0;
+    v.z1 = R.split.z1;
+    return v;
+}
+
+// The pruned value of word (k, y, z) given its current neighbourhood.
+__device__ __forceinline__ uint32_t prunedWord(const PruneView& v, uint32_t w, uint32_t idx, uint32_t k, uint32_t y,
+                                               uint32_t z) {
+    const uint32_t* S = v.S;
+    const uint32_t plane = v.ipx * v.AY;
+    const uint32_t prev = k > 0 ? S[idx - 1] : 0u;
+    const uint32_t next = k + 1 < v.ipx ? S[idx + 1] : 0u;
+    const uint32_t L = (w >> 1) | (prev << 31), Rt = (w << 1) | (next >> 31);
+    const uint32_t In = y > 0 ? S[idx - v.ipx] : 0u;
+    uint32_t Out = 0u, Up = 0u;
+    if (y + 1 < v.AY) {
+        if (v.yLater[y]) Out = __ldg(v.F + idx + v.ipx) | (v.Sf ? __ldg(v.Sf + idx + v.ipx) : 0u);
+        else Out = S[idx + v.ipx];
+    }
+    const uint32_t Dn = z > 0 ? S[idx - plane] : 0u;
+    if (z + 1 < v.AZ) {
+        const uint8_t* zLater = v.yLater + v.AY;
+        if (zLater[z]) Up = __ldg(v.F + idx + plane) | (v.Sf ? __ldg(v.Sf + idx + plane) : 0u);
+        else Up = S[idx + plane];
+    }
+    return w & (L | Rt) & (In | Out) & (Dn | Up);
+}
+
+// Appends (region, word) to a change list; past `cap` it sets *overflow.
+__device__ __forceinline__ void listAppend(unsigned long long* list, uint32_t* count, uint32_t cap,
+                                           uint32_t* overflow, uint32_t rg, uint32_t idx) {
+    const uint32_t at = atomicAdd(count, 1u);
+    if (at < cap) list[at] = ((unsigned long long)rg << 32) | idx;
+    else *overflow = 1u;
+}
+
+// Pass 0: every word of the regions of one subspace index.  Warps walk 32
+// consecutive words; the region of a warp's first word is one search, the
+// others step forward from it.
+__global__ void pruneKernel(Batch b, const PruneRegion* __restrict__ regions, uint32_t n, uint32_t total,
                             uint32_t* solid, const uint32_t* __restrict__ fill, const uint32_t* __restrict__ surf,
-                            uint32_t* flags, uint32_t flagBase, uint32_t passes, uint32_t pass) {
+                            uint32_t* flags, uint32_t flagBase, uint32_t passes, unsigned long long* list,
+                            uint32_t* count, uint32_t cap, uint32_t* overflow) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nWarps = (gridDim.x * blockDim.x) >> 5;
     uint32_t dirty = 0xFFFFFFFFu;   // region this thread changed last (flag not yet set)
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < totalWords; i += gridDim.x * blockDim.x) {
-        uint32_t lo = 0, hi = nRegions;
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (__ldg(&regions[mid].wordStart) <= i) lo = mid;
-            else hi = mid;
+    uint32_t cur = 0xFFFFFFFFu, wordStart = 0, ny = 0;
+    PruneView v{};
+    for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; base < total; base += nWarps * 32u) {
+        uint32_t r0 = 0;
+        if (lane == 0 && n > 1) {
+            uint32_t lo = 0, hi = n;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (__ldg(&regions[mid].wordStart) <= base) lo = mid;
+                else hi = mid;
+            }
+            r0 = lo;
         }
-        const uint32_t r = lo;
-        if (pass > 0 && __ldg(flags + (flagBase + r) * passes + pass - 1) == 0u) continue;
-        const PruneRegion R = regions[r];
-        const Unit& U = b.units[R.unit];
-        const uint32_t ipx = U.g.ipx, AY = U.g.AY, AZ = U.g.AZ;
-        const uint32_t ny = R.split.y1 - R.split.y0;
-        const uint32_t li = i - R.wordStart;
-        const uint32_t row = li / ipx;
-        const uint32_t k = li - row * ipx;
+        r0 = __shfl_sync(0xffffffffu, r0, 0);
+        const uint32_t i = base + lane;
+        if (i >= total) continue;
+        uint32_t r = r0;
+        while (r + 1 < n && __ldg(&regions[r + 1].wordStart) <= i) ++r;
+        if (r != cur) {
+            cur = r;
+            const PruneRegion R = regions[r];
+            v = pruneView(b, R, solid, fill, surf);
+            wordStart = R.wordStart;
+            ny = v.y1 - v.y0;
+        }
+        const uint32_t li = i - wordStart;
+        const uint32_t row = li / v.ipx;
+        const uint32_t k = li - row * v.ipx;
         const uint32_t zz = row / ny;
-        const uint32_t y = R.split.y0 + (row - zz * ny), z = R.split.z0 + zz;
-        const uint32_t plane = ipx * AY;
-        const uint32_t idx = (z * AY + y) * ipx + k;
-        uint32_t* S = solid + U.wordBase;
-        const uint32_t* F = fill + U.wordBase;
-        const uint32_t* Sf = (surf && U.materials) ? surf + U.wordBase : nullptr;
-        const uint8_t* yLater = b.later + U.laterBase;
-        const uint8_t* zLater = yLater + AY;
-        const uint32_t w = S[idx];
+        const uint32_t y = v.y0 + (row - zz * ny), z = v.z0 + zz;
+        const uint32_t idx = (z * v.AY + y) * v.ipx + k;
+        const uint32_t w = v.S[idx];
         if (w == 0) continue;
-        const uint32_t prev = k > 0 ? S[idx - 1] : 0u;
-        const uint32_t next = k + 1 < ipx ? S[idx + 1] : 0u;
-        const uint32_t L = (w >> 1) | (prev << 31), Rt = (w << 1) | (next >> 31);
-        const uint32_t In = y > 0 ? S[idx - ipx] : 0u;
-        uint32_t Out = 0u, Up = 0u;
-        if (y + 1 < AY) {
-            if (yLater[y]) Out = __ldg(F + idx + ipx) | (Sf ? __ldg(Sf + idx + ipx) : 0u);
-            else Out = S[idx + ipx];
-        }
-        const uint32_t Dn = z > 0 ? S[idx - plane] : 0u;
-        if (z + 1 < AZ) {
-            if (zLater[z]) Up = __ldg(F + idx + plane) | (Sf ? __ldg(Sf + idx + plane) : 0u);
-            else Up = S[idx + plane];
-        }
-        const uint32_t nw = w & (L | Rt) & (In | Out) & (Dn | Up);
+        const uint32_t nw = prunedWord(v, w, idx, k, y, z);
         if (nw != w) {
-            S[idx] = nw;
+            v.S[idx] = nw;
+            listAppend(list, count, cap, overflow, r, idx);
             if (dirty != r) {
-                if (dirty != 0xFFFFFFFFu) atomicOr(flags + (flagBase + dirty) * passes + pass, 1u);
+                if (dirty != 0xFFFFFFFFu) atomicOr(flags + (flagBase + dirty) * passes, 1u);
                 dirty = r;
             }
         }
     }
     const uint32_t peers = __match_any_sync(0xffffffffu, dirty);
-    if (dirty != 0xFFFFFFFFu && (threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1))
-        atomicOr(flags + (flagBase + dirty) * passes + pass, 1u);
+    if (dirty != 0xFFFFFFFFu && lane == (uint32_t)(__ffs(peers) - 1)) atomicOr(flags + (flagBase + dirty) * passes, 1u);
+}
+
+// Pass `pass` >= 1: the words next to the previous pass's changes (and the
+// changed words themselves), inside their region's subspace.
+__global__ void pruneListKernel(Batch b, const PruneRegion* __restrict__ regions, uint32_t* solid,
+                                const uint32_t* __restrict__ fill, const uint32_t* __restrict__ surf, uint32_t* flags,
+                                uint32_t flagBase, uint32_t passes, uint32_t pass,
+                                const unsigned long long* __restrict__ in, const uint32_t* __restrict__ inCount,
+                                unsigned long long* out, uint32_t* outCount, uint32_t cap, uint32_t* overflow) {
+    const uint32_t nIn = min(*inCount, cap);
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < nIn; e += gridDim.x * blockDim.x) {
+        const unsigned long long ent = in[e];
+        const uint32_t rg = (uint32_t)(ent >> 32), c = (uint32_t)ent;
+        const PruneView v = pruneView(b, regions[rg], solid, fill, surf);
+        const uint32_t plane = v.ipx * v.AY;
+        const uint32_t cz = c / plane, rem = c - cz * plane, cy = rem / v.ipx, ck = rem - cy * v.ipx;
+        bool changed = false;
+#pragma unroll 1
+        for (int q = 0; q < 7; ++q) {
+            uint32_t k = ck, y = cy, z = cz;
+            if (q == 1) { if (k == 0) continue; --k; }
+            else if (q == 2) { if (k + 1 >= v.ipx) continue; ++k; }
+            else if (q == 3) { if (y == v.y0) continue; --y; }
+            else if (q == 4) { if (y + 1 >= v.y1) continue; ++y; }
+            else if (q == 5) { if (z == v.z0) continue; --z; }
+            else if (q == 6) { if (z + 1 >= v.z1) continue; ++z; }
+            const uint32_t idx = (z * v.AY + y) * v.ipx + k;
+            const uint32_t w = v.S[idx];
+            if (w == 0) continue;
+            const uint32_t nw = prunedWord(v, w, idx, k, y, z);
+            if (nw != w) {
+                const uint32_t old = atomicAnd(v.S + idx, nw);
+                if (old & ~nw) {
+                    listAppend(out, outCount, cap, overflow, rg, idx);
+                    changed = true;
+                }
+            }
+        }
+        if (changed) atomicOr(flags + (flagBase + rg) * passes + pass, 1u);
+    }
 }
 
 // The words of one unit a kernel reads.
@@ -182,7 +285,7 @@ __device__ __forceinline__ uint32_t permOf(const WordNbrs& n, uint32_t q) {
 // one.  The warp's 32 rows are then stored as one contiguous span.  Unit
 // word bases are multiples of 32, so a warp's words belong to one unit.
 template <int K>
-__global__ void __launch_bounds__(256) emitNarrowKernel(EmitArgs a, uint64_t totalWords) {
+__global__ void __launch_bounds__(256, 6) emitNarrowKernel(EmitArgs a, uint64_t totalWords) {
     typedef NodeT<K> NT;
     static_assert(NT::bytes <= 2, "narrow nodes only");
     constexpr int NB = NT::bytes;
@@ -196,14 +299,24 @@ __global__ void __launch_bounds__(256) emitNarrowKernel(EmitArgs a, uint64_t tot
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     uint8_t* my = stage[warp] + lane * PITCH;
     const uint32_t v27 = (uint32_t)NT::pack(27u, 0u, 0.0f);
+    // Data of the unit last visited (a warp's words belong to one unit).
+    uint32_t cur = 0xFFFFFFFFu, nWords = 0;
+    uint64_t uBase = 0;
+    uint8_t* uOut = nullptr;
+    UnitWords uw{};
     for (uint64_t gbase = ((uint64_t)blockIdx.x * 8u + warp) * 32u; gbase < totalWords;
          gbase += (uint64_t)gridDim.x * 8u * 32u) {
-        const uint32_t u = unitOf(a.b.wordBase, a.b.nUnits, gbase);
-        const Unit& U = a.b.units[u];
-        const uint32_t nWords = U.g.ipx * U.g.AY * U.g.AZ;
-        const uint32_t wbase = (uint32_t)(gbase - U.wordBase);
+        const uint32_t u = a.b.nUnits > 1 ? unitOf(a.b.wordBase, a.b.nUnits, gbase) : 0u;
+        if (u != cur) {
+            cur = u;
+            const Unit& U = a.b.units[u];
+            nWords = U.g.ipx * U.g.AY * U.g.AZ;
+            uBase = U.wordBase;
+            uOut = static_cast<uint8_t*>(U.out);
+            uw = unitWords(a, U);
+        }
+        const uint32_t wbase = (uint32_t)(gbase - uBase);
         if (wbase >= nWords) continue;            // padding after the unit's grid (whole warp)
-        const UnitWords uw = unitWords(a, U);
         const uint32_t w = wbase + lane;
         WordNbrs n{};
         if (w < nWords) n = loadNbrs<K>(uw, w);
@@ -233,7 +346,7 @@ __global__ void __launch_bounds__(256) emitNarrowKernel(EmitArgs a, uint64_t tot
         for (int i = 0; i < CH; ++i)
             *reinterpret_cast<uint4*>(my + 16 * i) = make_uint4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
         if (rest) {
-            const uint32_t rank0 = n.s0 ? __ldg(a.ranks + U.wordBase + w) : 0u;
+            const uint32_t rank0 = n.s0 ? __ldg(a.ranks + uBase + w) : 0u;
             do {
                 const uint32_t bt = __clz(rest);       // node index in the word
                 const uint32_t q = 31u - bt;          // its bit
@@ -251,7 +364,7 @@ __global__ void __launch_bounds__(256) emitNarrowKernel(EmitArgs a, uint64_t tot
         }
         __syncwarp();
         const uint32_t wend = wbase + 32u <= nWords ? 32u : nWords - wbase;
-        uint4* out = reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(U.out) + (size_t)wbase * WB);
+        uint4* out = reinterpret_cast<uint4*>(uOut + (size_t)wbase * WB);
 #pragma unroll
         for (int i = 0; i < CH; ++i) {
             const uint32_t chunk = i * 32 + lane;       // 16-byte chunk of the warp's span
@@ -424,11 +537,22 @@ void launch_combine(const uint32_t* a, const uint32_t* b, uint32_t* out, uint64_
     *launches += 1;
 }
 
-void launch_prune(const Batch& b, const PruneRegion* regions, uint32_t n, uint32_t totalWords, uint32_t* solid,
+void launch_prune(const Batch& b, const PruneRegion* regions, uint32_t n, uint32_t groupWords, uint32_t* solid,
                   const uint32_t* fill, const uint32_t* surf, uint32_t* flags, uint32_t flagBase, uint32_t passes,
-                  uint32_t pass, cudaStream_t s, uint32_t* launches) {
-    pruneKernel<<<gridFor(totalWords, 256), 256, 0, s>>>(b, regions, n, totalWords, solid, fill, surf, flags,
-                                                          flagBase, passes, pass);
+                  unsigned long long* list, uint32_t* count, uint32_t cap, uint32_t* overflow, cudaStream_t s,
+                  uint32_t* launches) {
+    pruneKernel<<<gridFor(groupWords, 256, 148u * 8u), 256, 0, s>>>(b, regions, n, groupWords, solid, fill, surf,
+                                                                    flags, flagBase, passes, list, count, cap,
+                                                                    overflow);
+    *launches += 1;
+}
+
+void launch_prune_list(const Batch& b, const PruneRegion* regions, uint32_t* solid, const uint32_t* fill,
+                       const uint32_t* surf, uint32_t* flags, uint32_t flagBase, uint32_t passes, uint32_t pass,
+                       const unsigned long long* in, const uint32_t* inCount, unsigned long long* out,
+                       uint32_t* outCount, uint32_t cap, uint32_t* overflow, cudaStream_t s, uint32_t* launches) {
+    pruneListKernel<<<148 * 8, 256, 0, s>>>(b, regions, solid, fill, surf, flags, flagBase, passes, pass, in, inCount,
+                                            out, outCount, cap, overflow);
     *launches += 1;
 }
 

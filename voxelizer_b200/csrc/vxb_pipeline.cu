@@ -263,6 +263,14 @@ int Pipeline::prepare(const std::vector<MeshJob>& jobs, cudaStream_t s) {
     if ((rc = tileSums.ensure(4 * ((size_t)nWork_ / 4096 + 2)))) return rc;
     if (!aliasFill_ && (rc = fill.ensure(wordBytes))) return rc;
     if (anyCartesian_ && (rc = fin.ensure(wordBytes))) return rc;
+    // Change lists of the pruning passes: the first pass lists every word it
+    // changes (a fraction of the boundary words); past the cap the host
+    // finishes pruning with full passes.
+    uint32_t maxGroupWords = 0;
+    for (const Group& gr : groups_) maxGroupWords = std::max(maxGroupWords, gr.words);
+    pruneCap_ = std::max<uint32_t>(4u << 20, maxGroupWords / 4);
+    if (anyCartesian_ && (rc = pruneScratch.ensure(4 * (groups_.size() * kPasses + 1)))) return rc;
+    if (anyCartesian_ && (rc = pruneLists.ensure(2 * 8 * (size_t)pruneCap_))) return rc;
     listCap_ = 0;
     keysCap_ = 0;
     if (anyMaterials_) {
@@ -345,12 +353,25 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
         else
             VXB_CUDA(cudaMemcpyAsync(fin.p, fillP, 4 * (size_t)totalWords_, cudaMemcpyDeviceToDevice, s));
         VXB_CUDA(cudaMemsetAsync(st + kFlags, 0, 4 * (size_t)nRegions_ * kPasses, s));
+        // Per subspace index and pass: the count of its change list; the
+        // last word is the list overflow flag.
+        uint32_t* counts = pruneScratch.as<uint32_t>();
+        uint32_t* overflow = counts + groups_.size() * kPasses;
+        VXB_CUDA(cudaMemsetAsync(counts, 0, 4 * (groups_.size() * kPasses + 1), s));
         const PruneRegion* regions = reinterpret_cast<const PruneRegion*>(tables.as<uint8_t>() + oRegions_);
-        for (const Group& gr : groups_)
-            for (uint32_t pass = 0; pass < kPasses; ++pass)
-                launch_prune(b, regions + gr.first, gr.count, gr.words, fin.as<uint32_t>(), fillP,
-                             anyMaterials_ ? surf.as<uint32_t>() : nullptr, st + kFlags, gr.flagBase, kPasses, pass,
-                             s, &launches);
+        unsigned long long* lists[2] = {pruneLists.as<unsigned long long>(),
+                                        pruneLists.as<unsigned long long>() + pruneCap_};
+        const uint32_t* surfP = anyMaterials_ ? surf.as<uint32_t>() : nullptr;
+        for (size_t gi = 0; gi < groups_.size(); ++gi) {
+            const Group& gr = groups_[gi];
+            uint32_t* c = counts + gi * kPasses;
+            launch_prune(b, regions + gr.first, gr.count, gr.words, fin.as<uint32_t>(), fillP, surfP, st + kFlags,
+                         gr.flagBase, kPasses, lists[0], c, pruneCap_, overflow, s, &launches);
+            for (uint32_t pass = 1; pass < kPasses; ++pass)
+                launch_prune_list(b, regions + gr.first, fin.as<uint32_t>(), fillP, surfP, st + kFlags, gr.flagBase,
+                                  kPasses, pass, lists[(pass - 1) & 1], c + pass - 1, lists[pass & 1], c + pass,
+                                  pruneCap_, overflow, s, &launches);
+        }
         mark(2, true);
     }
     // Material keys by surface rank.
@@ -380,20 +401,23 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
     return 0;
 }
 
-// More passes over one subspace index until no region changes, one pass at
-// a time with a host check in between.
+// More passes over one subspace index until no region changes, one full
+// pass at a time with a host check in between.
 int Pipeline::pruneGroupUntilStable(const Group& gr, cudaStream_t s) {
     const Batch b = batch();
     uint32_t* st = status.as<uint32_t>();
     uint32_t* fillP = aliasFill_ ? static_cast<uint32_t*>(jobs_[0].out) : fill.as<uint32_t>();
     const PruneRegion* regions = reinterpret_cast<const PruneRegion*>(tables.as<uint8_t>() + oRegions_);
+    uint32_t* counts = pruneScratch.as<uint32_t>();
+    uint32_t* overflow = counts + groups_.size() * kPasses;
     std::vector<uint32_t> h((size_t)gr.count * kPasses);
     for (uint64_t round = 0;; ++round) {
         if (round > (1u << 24)) return failf(VXB_ETIMEDOUT, "pruning did not converge");
         VXB_CUDA(cudaMemsetAsync(st + kFlags + (size_t)gr.flagBase * kPasses, 0, 4 * h.size(), s));
+        VXB_CUDA(cudaMemsetAsync(counts, 0, 4, s));
         launch_prune(b, regions + gr.first, gr.count, gr.words, fin.as<uint32_t>(), fillP,
-                     anyMaterials_ ? surf.as<uint32_t>() : nullptr, st + kFlags, gr.flagBase, kPasses, 0, s,
-                     &launches);
+                     anyMaterials_ ? surf.as<uint32_t>() : nullptr, st + kFlags, gr.flagBase, kPasses,
+                     pruneLists.as<unsigned long long>(), counts, pruneCap_, overflow, s, &launches);
         VXB_CUDA(cudaMemcpyAsync(h.data(), st + kFlags + (size_t)gr.flagBase * kPasses, 4 * h.size(),
                                  cudaMemcpyDeviceToHost, s));
         VXB_CUDA(cudaStreamSynchronize(s));
@@ -441,7 +465,10 @@ int Pipeline::finish(cudaStream_t s) {
         // The first subspace index with a region that changed in its last
         // queued pass has not converged; it and every later index (pruned
         // against a superset of its final state) get passes until stable.
-        size_t first = groups_.size();
+        uint32_t overflow = 0;
+        VXB_CUDA(cudaMemcpy(&overflow, pruneScratch.as<uint32_t>() + groups_.size() * kPasses, 4,
+                            cudaMemcpyDeviceToHost));
+        size_t first = overflow ? 0 : groups_.size();
         for (size_t gi = 0; gi < groups_.size() && first == groups_.size(); ++gi)
             for (uint32_t r = 0; r < groups_[gi].count; ++r)
                 if (h[kFlags + ((size_t)groups_[gi].flagBase + r) * kPasses + kPasses - 1]) {

@@ -59,7 +59,7 @@ public:
     // Kernels launched by the last enqueue + finish.
     uint32_t launches = 0;
 
-    static constexpr uint32_t kPasses = 4;   // pruning passes queued per subspace
+    static constexpr uint32_t kPasses = 8;   // pruning passes queued per subspace
 
 private:
     struct Group {            // pruning regions of one subspace index
@@ -75,14 +75,14 @@ private:
     uint64_t totalWords_ = 0, totalRows_ = 0, totalGroups_ = 0;
     int nodeKind_ = 0, nodes_ = 1;
     bool anyMaterials_ = false, anyCartesian_ = false, wide_ = false, aliasFill_ = false;
-    uint32_t listCap_ = 0, keysCap_ = 0;
+    uint32_t listCap_ = 0, keysCap_ = 0, pruneCap_ = 0;
     // table offsets (bytes) in `tables`
     size_t oUnits_ = 0, oWork_ = 0, oRow_ = 0, oWord_ = 0, oSplits_ = 0, oSlices_ = 0, oLater_ = 0, oRegions_ = 0,
            oFcc_ = 0, oGroupBase_ = 0;
     std::vector<uint8_t> blob_;   // host copy of the tables (alive while the upload runs)
 
     DevBuf tables, status, counts, offsets, tileSums;
-    DevBuf fill, surf, fin, ranks, rankTiles;
+    DevBuf fill, surf, fin, ranks, rankTiles, pruneScratch, pruneLists;
     DevBuf codes, unitCounts, perm, buckets, recs, ovl, hitList, keys;
 };
 

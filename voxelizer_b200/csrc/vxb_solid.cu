@@ -257,26 +257,25 @@ __global__ void __launch_bounds__(kBlock, 3) solidToggleKernel(Batch b, uint32_t
     }
 }
 
-// Toggle bits -> solid runs, one warp per row: bit x = XOR of toggles <= x.
+// Toggle bits -> solid runs: bit x = XOR of the toggles at or before x.
+// One thread per row walks its row's words with a running parity; a row is
+// at most 32 words per x pass and the words stay in L1 between the load and
+// the store.
 __global__ void rowFillKernel(Batch b, uint64_t nRows, uint32_t* __restrict__ fill) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t warpsPerBlock = blockDim.x >> 5;
-    for (uint64_t row = (uint64_t)blockIdx.x * warpsPerBlock + (threadIdx.x >> 5); row < nRows;
-         row += (uint64_t)gridDim.x * warpsPerBlock) {
-        const uint32_t u = unitOf(b.rowBase, b.nUnits, row);
+    for (uint64_t row = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; row < nRows;
+         row += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t u = b.nUnits > 1 ? unitOf(b.rowBase, b.nUnits, row) : 0u;
         const Unit& U = b.units[u];
         const uint32_t ipx = U.g.ipx;
         uint32_t* r = fill + U.wordBase + (row - __ldg(b.rowBase + u)) * ipx;
-        uint32_t carry = 0;
-        for (uint32_t base = 0; base < ipx; base += 32) {
-            const uint32_t k = base + lane;
-            const uint32_t w = k < ipx ? r[k] : 0u;
+        uint32_t carry = 0u;
+        for (uint32_t k = 0; k < ipx; ++k) {
+            const uint32_t w = r[k];
+            if (!(w | carry)) continue;
             uint32_t p = w;
             p ^= p >> 1; p ^= p >> 2; p ^= p >> 4; p ^= p >> 8; p ^= p >> 16;
-            const uint32_t bal = __ballot_sync(0xffffffffu, __popc(w) & 1u);
-            const uint32_t before = (__popc(bal & laneMaskLt()) & 1u) ^ carry;
-            if (k < ipx) r[k] = before ? ~p : p;
-            carry ^= __popc(bal) & 1u;
+            r[k] = carry ? ~p : p;
+            carry ^= __popc(w) & 1u;
         }
     }
 }
@@ -295,7 +294,7 @@ void launch_solid_toggle(const Batch& b, uint32_t nWork, const uint32_t* offsets
 }
 
 void launch_row_fill(const Batch& b, uint64_t nRows, uint32_t* fill, cudaStream_t s, uint32_t* launches) {
-    rowFillKernel<<<gridFor(nRows * 32, 256), 256, 0, s>>>(b, nRows, fill);
+    rowFillKernel<<<gridFor(nRows, 256), 256, 0, s>>>(b, nRows, fill);
     *launches += 1;
 }
 
