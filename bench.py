@@ -349,6 +349,127 @@ def run_batched(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+SERVE_METRIC = "served voxelization (Poisson arrivals, 256-mesh mix shapes): sustained meshes/s and p50/p99 latency"
+
+
+def _poisson(rate, n, rng):
+    return np.cumsum(rng.exponential(1.0 / rate, size=n))
+
+
+def _drive(submit, wait, pool, arrivals):
+    """Submits pool[k % len(pool)] at arrivals[k] (seconds from start) from
+    one thread and waits for the results in order from another; returns the
+    latencies (s) and the span from the first arrival to the last result."""
+    results = [None] * len(arrivals)
+    lat = [0.0] * len(arrivals)
+    done = [0.0]
+    t0 = time.perf_counter() + 0.05
+
+    def waiter():
+        for k in range(len(arrivals)):
+            while results[k] is None:
+                time.sleep(0.0002)
+            lat[k] = wait(results[k]) - (t0 + arrivals[k])
+        done[0] = time.perf_counter()
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    for k, ta in enumerate(arrivals):
+        dt = t0 + ta - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        results[k] = submit(pool[k % len(pool)])
+    th.join()
+    return lat, done[0] - t0
+
+
+def run_served(args, world, rank, local):
+    """Poisson request streams at several rates through the continuous-
+    batching server, beside the plain path (one voxelization call per
+    request, first come first served) under the same arrivals."""
+    import queue
+
+    import torch
+
+    from voxelizer_b200 import scenes
+    from voxelizer_b200.api import LONG, Voxelizer
+    from voxelizer_b200.serve import VoxelServer
+
+    torch.cuda.set_device(local)
+    pool = scenes.batch_mix(args.batch_meshes, seed=1)
+    rng = np.random.default_rng(7)
+    rates = [50, 200, 1000, 2000]
+    rows = []
+    for rate in rates:
+        n = int(min(args.serve_max_requests, max(50, rate * args.serve_seconds)))
+        arrivals = _poisson(rate, n, rng)
+        # Served.
+        with VoxelServer(budget_bytes=160 << 30, lanes=2, device=local) as srv:
+            def submit(item):
+                m, md = item
+                return srv.submit(m.vertices, m.indices, m.materials, m.n_materials, size=md, node_type=LONG)
+
+            def wait(req):
+                req.wait()
+                t = req.t_done
+                srv.release(req)
+                return t
+
+            _drive(submit, wait, pool[:8], _poisson(1000, 16, rng))   # warm-up
+            lat_s, span_s = _drive(submit, wait, pool, arrivals)
+            batches = srv.batches
+        # Plain path: one worker, one call per request, in arrival order.
+        q = queue.Queue()
+        stream = torch.cuda.Stream()
+
+        def worker():
+            while True:
+                item = q.get()
+                if item is None:
+                    return
+                (m, md), box = item
+                with Voxelizer(m.vertices, m.indices, m.materials, m.n_materials, node_type=LONG,
+                               device=local) as v:
+                    info = v.plan(1, md)
+                    with torch.cuda.stream(stream):
+                        out = torch.empty(int(info.bytes), dtype=torch.uint8, device="cuda")
+                    v.voxelize_device(1, md, out, stream=stream.cuda_stream)
+                box.append(time.perf_counter())
+
+        th = threading.Thread(target=worker)
+        th.start()
+
+        def submit_plain(item):
+            box = []
+            q.put((item, box))
+            return box
+
+        def wait_plain(box):
+            while not box:
+                time.sleep(0.0002)
+            return box[0]
+
+        _drive(submit_plain, wait_plain, pool[:8], _poisson(1000, 16, rng))
+        lat_p, span_p = _drive(submit_plain, wait_plain, pool, arrivals)
+        q.put(None)
+        th.join()
+        pct = lambda a, p: round(float(np.percentile(np.asarray(a) * 1e3, p)), 3)  # noqa: E731
+        rows.append({"rate_req_s": rate, "requests": n,
+                     "served": {"meshes_per_s": round(n / span_s, 1), "p50_ms": pct(lat_s, 50),
+                                "p99_ms": pct(lat_s, 99), "batches": batches},
+                     "plain": {"meshes_per_s": round(n / span_p, 1), "p50_ms": pct(lat_p, 50),
+                               "p99_ms": pct(lat_p, 99)}})
+    top = rows[-1]
+    line = {"metric": SERVE_METRIC, "value": top["served"]["meshes_per_s"], "unit": "meshes/s", "n_gpus": world,
+            "steps": len(rates), "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64+f32+u32", "data": "synthetic (seeded 256-mesh mix shapes, Poisson arrivals)",
+            "config": {"workload": "LongNode with materials; admission by a 160 GB device-memory budget; 2 lanes",
+                       "rates_req_s": rates, "seconds_per_rate": args.serve_seconds},
+            "p50_ms": top["served"]["p50_ms"], "p99_ms": top["served"]["p99_ms"], "rates": rows}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -357,9 +478,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--workload", default="room", choices=["room", "batched"],
-                    help="room: the single-mesh headline; batched: the 256-mesh mix as one batch vs a per-mesh loop")
+    ap.add_argument("--workload", default="room", choices=["room", "batched", "served"],
+                    help="room: the single-mesh headline; batched: the 256-mesh mix as one batch vs a per-mesh "
+                         "loop; served: Poisson request streams through the continuous-batching server")
     ap.add_argument("--batch-meshes", type=int, default=256)
+    ap.add_argument("--serve-seconds", type=float, default=1.5)
+    ap.add_argument("--serve-max-requests", type=int, default=3000)
     ap.add_argument("--profile-run", type=int, default=0, metavar="MAXDIM",
                     help="no timing: voxelize the room scene at this maxDimension --steps times (a target for ncu)")
     args = ap.parse_args()
@@ -373,6 +497,9 @@ def main():
         return
     if args.workload == "batched":
         run_batched(args, world, rank, local)
+        return
+    if args.workload == "served":
+        run_served(args, world, rank, local)
         return
 
     import torch

@@ -82,10 +82,11 @@ const char* vxb_version(void);
  * them after the call.  `device` selects the CUDA device (reference: 0). */
 vxb_status vxb_create(vxb_voxelizer** out, int node_type, const float* vertices, const uint32_t* indices,
                       uint32_t n_vertices, uint32_t n_triangles, int device);
-/* ~Voxelizer(): frees the instance after waiting for the device to finish
- * its work.  Its device buffers go to a process-wide cache of idle blocks
- * (at most 16 GiB) that later instances draw from, so that creating one
- * voxelizer per mesh does not pay cudaMalloc / cudaFree every time. */
+/* ~Voxelizer(): frees the instance.  Its device buffers go to a
+ * process-wide cache of idle blocks (at most 16 GiB) that later instances
+ * draw from, so that creating one voxelizer per mesh does not pay cudaMalloc
+ * / cudaFree every time.  (Calls return with their work complete; after a
+ * failed call this waits for the device first.) */
 vxb_status vxb_destroy(vxb_voxelizer* v);
 /* No reference counterpart: returns every idle cached block to the driver. */
 vxb_status vxb_trim_cache(void);

@@ -42,10 +42,16 @@ struct vxb_voxelizer {
     std::vector<uint8_t> materials;
     double mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
     bool meshOnDevice = false, matsOnDevice = false;
+    bool hasMaterials = false;   // setMaterials was called (materials live on the host or the device)
     vxb::DevBuf dV, dI, dM, outStage;
     vxb::Pipeline pipe;
     vxb::StageTimer timer;
     uint32_t launches = 0;
+    // Set while work of a call may still be queued on the device (a call
+    // that failed half-way); vxb_destroy then waits for the device before
+    // its buffers return to the block cache.  Calls that succeed end with
+    // their work complete.
+    bool busy = false;
 
     int plan(int nodes, const vxb_request* r, vxb::Plan& p, vxb_grid_info* info) const;
     // Combinations the reference refuses (src/host_side.cpp:568-573,
@@ -56,11 +62,15 @@ struct vxb_voxelizer {
         if (nodes && isFcc(nodeType) && !r->by_cube_length)
             return failf(VXB_EUNSUPPORTED,
                          "FCC Nodes can currently only be defined through the side length of their cubic cells");
-        if (nodes && materialsOn && materials.empty())
+        if (nodes && materialsOn && !hasMaterials)
             return failf(VXB_ENOMATERIALS, "material output requested but no materials were set");
         return 0;
     }
     int upload(cudaStream_t s);
+    // Copies caller arrays to the device; false (nothing kept) when there is
+    // no usable device.
+    bool uploadFrom(const float* vertices, const uint32_t* indices);
+    bool uploadMaterials(const uint8_t* mats);
     void job(int nodes, const vxb_request* r, void* dout, uint64_t bytes, vxb::MeshJob* j) const;
     int run(int nodes, const vxb_request* r, void* dout, uint64_t bytes, cudaStream_t s, vxb_grid_info* info);
 };
@@ -92,6 +102,55 @@ int vxb_voxelizer::upload(cudaStream_t s) {
         matsOnDevice = true;
     }
     return 0;
+}
+
+namespace {
+
+// Runs `f` with `device` current, restoring the caller's device; false when
+// there is no such device.
+template <class F> bool onDevice(int device, F f) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return false;
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != device && cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const bool ok = f();
+    if (cur != device) cudaSetDevice(cur);
+    return ok;
+}
+
+}  // namespace
+
+bool vxb_voxelizer::uploadFrom(const float* vertices, const uint32_t* indices) {
+    return onDevice(device, [&]() {
+        if (dV.ensure(sizeof(float) * 3 * (size_t)nV) || dI.ensure(sizeof(uint32_t) * 3 * (size_t)nT)) return false;
+        if (cudaMemcpy(dV.p, vertices, sizeof(float) * 3 * (size_t)nV, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(dI.p, indices, sizeof(uint32_t) * 3 * (size_t)nT, cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        meshOnDevice = true;
+        return true;
+    });
+}
+
+bool vxb_voxelizer::uploadMaterials(const uint8_t* mats) {
+    if (!meshOnDevice) return false;
+    return onDevice(device, [&]() {
+        if (dM.ensure(nT)) return false;
+        if (cudaMemcpy(dM.p, mats, nT, cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        matsOnDevice = true;
+        return true;
+    });
 }
 
 void vxb_voxelizer::job(int nodes, const vxb_request* r, void* dout, uint64_t bytes, vxb::MeshJob* j) const {
@@ -126,6 +185,7 @@ int vxb_voxelizer::run(int nodes, const vxb_request* r, void* dout, uint64_t byt
     VXB_CUDA(cudaSetDevice(device));
     launches = 0;
     timer.reset();
+    busy = true;
     if ((rc = upload(s))) return rc;
     vxb::MeshJob j;
     job(nodes, r, dout, bytes, &j);
@@ -133,6 +193,7 @@ int vxb_voxelizer::run(int nodes, const vxb_request* r, void* dout, uint64_t byt
     if ((rc = pipe.enqueue(s, &timer))) return rc;
     rc = pipe.finish(s);
     launches = pipe.launches;
+    if (rc == 0) busy = false;
     return rc;
 }
 
@@ -155,6 +216,7 @@ struct vxb_batch {
     cudaStream_t graphStream = nullptr;
     uint32_t graphKernels = 0;
     uint32_t launches = 0;
+    bool busy = false;           // as vxb_voxelizer::busy
     void dropGraph() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
@@ -194,22 +256,27 @@ vxb_status vxb_create(vxb_voxelizer** out, int node_type, const float* vertices,
     v->device = device;
     v->nV = n_vertices;
     v->nT = n_triangles;
-    v->vertices.assign(vertices, vertices + 3 * (size_t)n_vertices);
-    v->indices.assign(indices, indices + 3 * (size_t)n_triangles);
     if (n_vertices) vxb::boundingBox(vertices, n_vertices, v->mn, v->mx);
+    // The copy the reference keeps on the host goes straight to the device
+    // when there is one; without a device (planning only) it stays on the
+    // host until the first voxelization.
+    if (!v->uploadFrom(vertices, indices)) {
+        v->vertices.assign(vertices, vertices + 3 * (size_t)n_vertices);
+        v->indices.assign(indices, indices + 3 * (size_t)n_triangles);
+    }
     *out = v;
     return VXB_OK;
 }
 
 vxb_status vxb_destroy(vxb_voxelizer* v) {
     if (!v) return VXB_OK;
-    // The instance's buffers go back to the block cache: wait for queued
-    // work that may still use them.
+    // The instance's buffers go back to the block cache: after a failed
+    // call, wait for queued work that may still use them.
     const int dev = v->device;
     int cur = 0;
     cudaGetDevice(&cur);
     if (cur != dev) cudaSetDevice(dev);
-    cudaDeviceSynchronize();
+    if (v->busy) cudaDeviceSynchronize();
     delete v;
     if (cur != dev) cudaSetDevice(cur);
     return VXB_OK;
@@ -222,8 +289,10 @@ vxb_status vxb_set_materials(vxb_voxelizer* v, const uint8_t* materials, uint32_
         return failf(VXB_EINVAL,
                      "The number of unique materials exceeds the capabilities of the node type @ setMaterials.");
     v->nUniqueMaterials = n_unique_materials;
-    v->materials.assign(materials, materials + v->nT);
     v->matsOnDevice = false;
+    v->materials.clear();
+    if (!v->uploadMaterials(materials)) v->materials.assign(materials, materials + v->nT);
+    v->hasMaterials = true;
     v->materialsOn = true;
     return VXB_OK;
 }
@@ -337,7 +406,7 @@ vxb_status vxb_batch_destroy(vxb_batch* b) {
     int cur = 0;
     cudaGetDevice(&cur);
     if (cur != dev) cudaSetDevice(dev);
-    cudaDeviceSynchronize();
+    if (b->busy) cudaDeviceSynchronize();
     delete b;
     if (cur != dev) cudaSetDevice(cur);
     return VXB_OK;
@@ -388,6 +457,8 @@ vxb_status vxb_batch_run(vxb_batch* b, void* stream, int flags) {
         s = b->own;
     }
     int rc;
+    b->busy = true;
+    for (const vxb_batch::Entry& e : b->entries) e.v->busy = true;
     if (!b->prepared) {
         std::vector<vxb::MeshJob> jobs(b->entries.size());
         for (size_t i = 0; i < jobs.size(); ++i) {
@@ -424,11 +495,15 @@ vxb_status vxb_batch_run(vxb_batch* b, void* stream, int flags) {
         b->pipe.launches = 0;
         rc = b->pipe.finish(s);
         b->launches = b->graphKernels + b->pipe.launches;
-        return rc;
+    } else {
+        if ((rc = b->pipe.enqueue(s, nullptr))) return rc;
+        rc = b->pipe.finish(s);
+        b->launches = b->pipe.launches;
     }
-    if ((rc = b->pipe.enqueue(s, nullptr))) return rc;
-    rc = b->pipe.finish(s);
-    b->launches = b->pipe.launches;
+    if (rc == 0) {
+        b->busy = false;
+        for (const vxb_batch::Entry& e : b->entries) e.v->busy = false;
+    }
     return rc;
 }
 

@@ -79,18 +79,14 @@ void cacheGive(int device, void* p, size_t bytes) {
 
 int DevBuf::ensure(size_t bytes) {
     if (bytes <= cap) return 0;
-    if (p) {
-        const cudaError_t e = cudaDeviceSynchronize();
-        if (e != cudaSuccess) return failf(VXB_ECUDA, "%s", cudaGetErrorString(e));
-        release();
-    }
+    release();
     cudaGetDevice(&dev);
     size_t got = 0;
     if ((p = cacheTake(dev, bytes, &got))) {
         cap = got;
         return 0;
     }
-    const size_t want = bytes + bytes / 8 + 256;
+    const size_t want = bytes + bytes / 2 + 256;
     const cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
         cudaGetLastError();

@@ -45,8 +45,10 @@ struct DevBuf {
         p = nullptr;
         cap = 0;
     }
-    // Grows to at least `bytes`; a buffer in use is given back only after
-    // the device has finished all queued work.
+    // Grows to at least `bytes` (with headroom).  Callers grow a buffer only
+    // while no queued work uses it: every entry point of this library
+    // returns with its own work complete, and a call grows its buffers
+    // before it queues any.
     int ensure(size_t bytes);
     template <class T> T* as() const { return reinterpret_cast<T*>(p); }
 };
