@@ -260,12 +260,28 @@ def cpu_baseline(mesh):
 
 
 def profile_run(args):
-    """The workload's launches and nothing else, for a profiler to capture."""
+    """The workload's launches and nothing else, for a profiler to capture:
+    the room scene at maxDimension --profile-run, or with --workload batched
+    the 256-mesh mix as one batch (without graph capture)."""
     import torch
 
     from voxelizer_b200 import scenes
-    from voxelizer_b200.api import LONG, Voxelizer
+    from voxelizer_b200.api import LONG, Voxelizer, VoxelizerBatch
 
+    if args.workload == "batched":
+        mix = scenes.batch_mix(args.batch_meshes, seed=0)
+        keep = []
+        with VoxelizerBatch() as b:
+            for mesh, md in mix:
+                v = Voxelizer(mesh.vertices, mesh.indices, mesh.materials, mesh.n_materials, node_type=LONG)
+                o = torch.empty(int(v.plan(1, md).bytes), dtype=torch.uint8, device="cuda")
+                keep.append((v, o))
+                b.add(v, 1, md, o)
+            for _ in range(args.steps):
+                b.run()
+            torch.cuda.synchronize()
+            print(f"profile run: {args.steps} x batch of {len(mix)}, {b.last_launch_count()} launches each", flush=True)
+        return
     mesh = scenes.room_scene()
     with Voxelizer(mesh.vertices, mesh.indices, mesh.materials, mesh.n_materials, node_type=LONG) as vx:
         info = vx.plan(1, args.profile_run)
