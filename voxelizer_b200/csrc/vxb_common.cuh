@@ -39,6 +39,23 @@ __device__ __forceinline__ uint32_t unitOf(const T* __restrict__ base, uint32_t 
     return lo;
 }
 
+// Largest t < n with off[t] <= item (off[n] > item), by a 32-way search of
+// the whole warp: ceil(log32 n) dependent loads.
+__device__ __forceinline__ uint32_t warpFindOwner(const uint32_t* __restrict__ off, uint32_t n, uint32_t item,
+                                                  uint32_t lane) {
+    uint32_t lo = 0, hi = n;  // off[lo] <= item < off[hi]
+    while (hi - lo > 1) {
+        const uint32_t step = (hi - lo + 31u) / 32u;
+        const uint32_t p = lo + lane * step;
+        const bool ok = p < hi && __ldg(off + p) <= item;
+        const uint32_t m = __ballot_sync(0xffffffffu, ok);
+        const uint32_t nlo = lo + (31u - (uint32_t)__clz(m)) * step;
+        hi = min(nlo + step, hi);
+        lo = nlo;
+    }
+    return lo;
+}
+
 // Blocks for `work` items at `threads` per block, capped (grid-stride loops).
 inline uint32_t gridFor(uint64_t work, uint32_t threads, uint32_t cap = 148u * 32u) {
     uint64_t b = (work + threads - 1) / threads;

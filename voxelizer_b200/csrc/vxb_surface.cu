@@ -518,23 +518,6 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
     }
 }
 
-// Largest t < n with off[t] <= item (off[n] > item), by a 32-way search of
-// the whole warp: ceil(log32 n) dependent loads.
-__device__ __forceinline__ uint32_t warpFindOwner(const uint32_t* __restrict__ off, uint32_t n, uint32_t item,
-                                                  uint32_t lane) {
-    uint32_t lo = 0, hi = n;  // off[lo] <= item < off[hi]
-    while (hi - lo > 1) {
-        const uint32_t step = (hi - lo + 31u) / 32u;
-        const uint32_t p = lo + lane * step;
-        const bool ok = p < hi && __ldg(off + p) <= item;
-        const uint32_t m = __ballot_sync(kFull, ok);
-        const uint32_t nlo = lo + (31u - (uint32_t)__clz(m)) * step;
-        hi = min(nlo + step, hi);
-        lo = nlo;
-    }
-    return lo;
-}
-
 // Pass 4: the work list.  Warps take batches of kBatch consecutive 32-item
 // chunks; within a batch the owner of each chunk's first item follows from
 // the previous chunk.  Every partitioned triangle has at least one unit, so
@@ -706,15 +689,33 @@ __global__ void zeroKeysKernel(void* keys, const uint32_t* __restrict__ countPtr
 __global__ void mergeKeysKernel(const unsigned long long* __restrict__ list, const uint32_t* __restrict__ countPtr,
                                 uint32_t cap, const uint32_t* __restrict__ bits, const uint32_t* __restrict__ ranks,
                                 uint32_t* keys, uint32_t keysCap) {
+    // Four independent entries per thread and iteration: the scattered
+    // loads of one entry overlap those of the others.
+    constexpr int U = 4;
     const uint32_t n = min(*countPtr, cap);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const unsigned long long e = list[i];
-        const uint64_t pos = e >> 24;
-        const uint64_t w = pos >> 5;
-        const uint32_t b = (uint32_t)(pos & 31u);
-        const uint32_t word = __ldg(bits + w);
-        const uint32_t r = __ldg(ranks + w) + (b ? __popc(word >> (32 - b)) : 0u);
-        if (r < keysCap) atomicMax(keys + r, (uint32_t)(e & 0xFFFFFFull));
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += U * stride) {
+        unsigned long long e[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t i = i0 + u * stride;
+            e[u] = i < n ? list[i] : ~0ull;
+        }
+        uint32_t word[U], rk[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (e[u] == ~0ull) continue;
+            const uint64_t w = (e[u] >> 24) >> 5;
+            word[u] = __ldg(bits + w);
+            rk[u] = __ldg(ranks + w);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (e[u] == ~0ull) continue;
+            const uint32_t b = (uint32_t)((e[u] >> 24) & 31u);
+            const uint32_t r = rk[u] + (b ? __popc(word[u] >> (32 - b)) : 0u);
+            if (r < keysCap) atomicMax(keys + r, (uint32_t)(e[u] & 0xFFFFFFull));
+        }
     }
 }
 
