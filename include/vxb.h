@@ -131,10 +131,25 @@ vxb_status vxb_voxelize_to_device(vxb_voxelizer* v, int nodes, const vxb_request
 /* Number of kernels the last voxelize call launched on the device. */
 vxb_status vxb_last_launch_count(vxb_voxelizer* v, uint32_t* launches);
 
+/* Work counters of the last voxelize call (no reference counterpart; the
+ * reference's verbose mode prints similar sizes). */
+typedef struct {
+    uint32_t units;                 /* meshes x lattices */
+    uint32_t work_triangles;        /* triangles x lattices */
+    uint32_t solid_candidates;      /* (triangle, subspace, 4x4 tile) candidates of the solid pass */
+    uint32_t surface_columns;       /* work items of the surface pass */
+    uint32_t surface_hits;          /* surface voxel hits (with repeats) */
+    uint32_t surface_voxels;        /* distinct surface voxels */
+    uint32_t surface_triangles[3];  /* triangles with surface work by class: 1D, 2D, 3D boxes */
+    uint64_t grid_words;            /* 32-bit words of one bit grid */
+} vxb_stats;
+vxb_status vxb_last_stats(vxb_voxelizer* v, vxb_stats* stats);
+
 /* Stage timing with CUDA events on the call's stream (off by default; no
  * reference counterpart, the reference only prints clock() stamps in verbose
  * mode).  Stages: 0 solid voxelization, 1 surface voxelization, 2 pruning,
- * 3 node emission, 4 material merge.  vxb_stage_times waits for the last call and writes the
+ * 3 node emission, 4 material merge, 5 the surface work kernel alone (part
+ * of stage 1).  vxb_stage_times waits for the last call and writes the
  * milliseconds of up to n stages (-1 for a stage that did not run). */
 vxb_status vxb_set_profiling(vxb_voxelizer* v, int enable);
 vxb_status vxb_stage_times(vxb_voxelizer* v, float* ms, uint32_t n);

@@ -25,7 +25,7 @@ EXPORTS = ["vxb_last_error", "vxb_version", "vxb_create", "vxb_destroy", "vxb_se
            "vxb_set_material_output", "vxb_verbose_output", "vxb_plan", "vxb_get_array_dimensions",
            "vxb_voxelize_to_host", "vxb_voxelize_to_device", "vxb_last_launch_count", "vxb_set_profiling",
            "vxb_stage_times", "vxb_voxelize_bits_noalloc", "vxb_trim_cache", "vxb_batch_create",
-           "vxb_batch_destroy", "vxb_batch_add", "vxb_batch_clear", "vxb_batch_run", "vxb_batch_last_launch_count"]
+           "vxb_batch_destroy", "vxb_batch_add", "vxb_batch_clear", "vxb_batch_run", "vxb_batch_last_launch_count", "vxb_last_stats"]
 
 BATCH_GRAPH = 1
 
@@ -55,6 +55,17 @@ class GridInfo(ctypes.Structure):
         return (int(self.dim.x), int(self.dim.y), int(self.dim.z))
 
 
+class Stats(ctypes.Structure):
+    _fields_ = [("units", ctypes.c_uint32), ("work_triangles", ctypes.c_uint32),
+                ("solid_candidates", ctypes.c_uint32), ("surface_columns", ctypes.c_uint32),
+                ("surface_hits", ctypes.c_uint32), ("surface_voxels", ctypes.c_uint32),
+                ("surface_triangles", ctypes.c_uint32 * 3), ("grid_words", ctypes.c_uint64)]
+
+    def as_dict(self):
+        return {k: (list(getattr(self, k)) if k == "surface_triangles" else int(getattr(self, k)))
+                for k, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -80,6 +91,7 @@ def lib():
         "vxb_batch_clear": (ctypes.c_int, [vp]),
         "vxb_batch_run": (ctypes.c_int, [vp, vp, ctypes.c_int]),
         "vxb_batch_last_launch_count": (ctypes.c_int, [vp, P(ctypes.c_uint32)]),
+        "vxb_last_stats": (ctypes.c_int, [vp, P(Stats)]),
         "vxb_set_materials": (ctypes.c_int, [vp, vp, ctypes.c_uint32]),
         "vxb_set_material_output": (ctypes.c_int, [vp, ctypes.c_int]),
         "vxb_verbose_output": (ctypes.c_int, [vp, ctypes.c_int]),

@@ -125,7 +125,7 @@ class Voxelizer:
     def set_profiling(self, enable):
         check(lib().vxb_set_profiling(self._h, int(bool(enable))))
 
-    STAGES = ("solid", "surface", "prune", "emit", "merge")
+    STAGES = ("solid", "surface", "prune", "emit", "merge", "surface_work")
 
     def stage_times(self):
         """Milliseconds per stage of the last call (-1: stage did not run)."""
@@ -137,6 +137,12 @@ class Voxelizer:
         n = ctypes.c_uint32()
         check(lib().vxb_last_launch_count(self._h, ctypes.byref(n)))
         return int(n.value)
+
+    def last_stats(self):
+        """Work counters of the last call (vxb_last_stats)."""
+        st = _lib.Stats()
+        check(lib().vxb_last_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
 
 
 class VoxelizerBatch:

@@ -388,6 +388,12 @@ vxb_status vxb_last_launch_count(vxb_voxelizer* v, uint32_t* launches) {
     return VXB_OK;
 }
 
+vxb_status vxb_last_stats(vxb_voxelizer* v, vxb_stats* stats) {
+    if (!v || !stats) return failf(VXB_EINVAL, "NULL argument");
+    *stats = v->pipe.stats;
+    return VXB_OK;
+}
+
 // ---- batches ----
 
 vxb_status vxb_batch_create(vxb_batch** out, int device) {

@@ -338,9 +338,11 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
                                perm.as<uint32_t>(), counts.as<uint32_t>(), recs.p, ovl.p, s, &launches);
         launch_scan(counts.as<uint32_t>(), offsets.as<uint32_t>(), nWork_, tileSums.as<uint32_t>(), st + kSurfTotal,
                     st + kSurfOverflow, s, &launches);
+        mark(5, false);
         launch_surface_work(0, wide_ ? 1 : 0, b, recs.p, ovl.p, offsets.as<uint32_t>(), nWork_, st + kSurfTotal,
                             buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_,
                             hitList.as<unsigned long long>(), st + kHitCount, listCap_, s, &launches);
+        mark(5, true);
         launch_surface_rank(surf.as<uint32_t>(), totalWords_, ranks.as<uint32_t>(), rankTiles.as<uint32_t>(),
                             st + kSurfaceVoxels, s, &launches);
         mark(1, true);
@@ -437,7 +439,18 @@ int Pipeline::finish(cudaStream_t s) {
     }
     std::vector<uint32_t> h(kFlags + (size_t)nRegions_ * kPasses);
     VXB_CUDA(cudaMemcpyAsync(h.data(), status.p, 4 * h.size(), cudaMemcpyDeviceToHost, s));
+    uint32_t bk[kSurfaceBuckets] = {0};
+    if (anyMaterials_) VXB_CUDA(cudaMemcpyAsync(bk, buckets.p, sizeof(bk), cudaMemcpyDeviceToHost, s));
     VXB_CUDA(cudaStreamSynchronize(s));
+    memset(&stats, 0, sizeof(stats));
+    stats.units = (uint32_t)units_.size();
+    stats.work_triangles = nWork_;
+    stats.solid_candidates = h[kSolidTotal];
+    stats.surface_columns = anyMaterials_ ? h[kSurfTotal] : 0;
+    stats.surface_hits = anyMaterials_ ? h[kHitCount] : 0;
+    stats.surface_voxels = anyMaterials_ ? h[kSurfaceVoxels] : 0;
+    for (uint32_t k = 0; k < kSurfaceBuckets; ++k) stats.surface_triangles[k / 3] += bk[k];
+    stats.grid_words = totalWords_;
     if (h[kSolidOverflow] || (anyMaterials_ && h[kSurfOverflow]))
         return failf(VXB_EOVERFLOW, "work list exceeds 2^32 entries");
     bool reemit = false;

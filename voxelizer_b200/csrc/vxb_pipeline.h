@@ -33,7 +33,9 @@ PassGeom makeGeom(const Plan& p, int lattice);
 
 // Per-stage CUDA events on the launching stream (vxb_set_profiling).
 struct StageTimer {
-    static constexpr int kStages = 5;   // 0 solid, 1 surface, 2 prune, 3 emit, 4 material merge
+    // 0 solid, 1 surface, 2 prune, 3 emit, 4 material merge, 5 the surface
+    // work kernel alone (inside stage 1)
+    static constexpr int kStages = 6;
     bool enabled = false;
     cudaEvent_t ev[2 * kStages] = {};
     bool used[kStages] = {};
@@ -58,6 +60,8 @@ public:
     int finish(cudaStream_t s);
     // Kernels launched by the last enqueue + finish.
     uint32_t launches = 0;
+    // Counters of the last finish (vxb_last_stats).
+    vxb_stats stats{};
 
     static constexpr uint32_t kPasses = 8;   // pruning passes queued per subspace
 
