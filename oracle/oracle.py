@@ -55,6 +55,7 @@ def fma_sites(model=None):
     return arr
 
 NODE_BYTES = {0: 1, 1: 2, 2: 8, 3: 2, 4: 4}
+PARTIAL_NODE = 2
 
 
 class _Params(ctypes.Structure):
@@ -86,6 +87,8 @@ def lib():
         _lib.orc_voxelize.argtypes = [ctypes.POINTER(_Params), ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
                                       ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
                                       ctypes.c_uint64, ctypes.c_void_p, ctypes.POINTER(Info)]
+        _lib.orc_voxelize_winners.restype = ctypes.c_int
+        _lib.orc_voxelize_winners.argtypes = _lib.orc_voxelize.argtypes + [ctypes.c_void_p, ctypes.c_void_p]
     return _lib
 
 
@@ -138,3 +141,25 @@ def voxelize(mesh, node_type, nodes, materials, size, vox=(1024, 512, 512), mat=
     if rc:
         raise RuntimeError(f"orc_voxelize failed: {rc}")
     return out, info, conf
+
+
+def voxelize_winners(mesh, size, vox=(1024, 512, 512), mat=(512, 512, 512), fma_model=None, threads=0):
+    """PartialNode with materials: (output, Info, conflict mask, winning
+    triangle per node (0xFFFFFFFF off the surface), winning class per node)."""
+    p = _params(PARTIAL_NODE, 1, 1, size, vox, mat, fma_model, threads)
+    info = Info()
+    L = lib()
+    rc = L.orc_plan(ctypes.byref(p), mesh.vertices.ctypes.data, mesh.n_vertices, ctypes.byref(info))
+    if rc:
+        raise RuntimeError(f"orc_plan failed: {rc}")
+    out = np.empty(int(info.out_bytes) // 8, dtype=np.uint64)
+    conf = np.zeros(out.size, np.uint8)
+    tri = np.full(out.size, 0xFFFFFFFF, np.uint32)
+    cls = np.zeros(out.size, np.uint8)
+    mats = mesh.materials if mesh.materials is not None else np.zeros(mesh.n_triangles, np.uint8)
+    rc = L.orc_voxelize_winners(ctypes.byref(p), mesh.vertices.ctypes.data, mesh.n_vertices, mesh.indices.ctypes.data,
+                                mesh.n_triangles, mats.ctypes.data, mesh.n_materials, out.ctypes.data, out.nbytes,
+                                conf.ctypes.data, ctypes.byref(info), tri.ctypes.data, cls.ctypes.data)
+    if rc:
+        raise RuntimeError(f"orc_voxelize_winners failed: {rc}")
+    return out, info, conf, tri, cls

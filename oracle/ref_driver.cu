@@ -247,6 +247,13 @@ struct Runner {
         const bool materials = p.materials && p.node_output;
         // initDevices, host_side.cpp:164-202
         dev.dev = 0; dev.blocks = 64; dev.threads = 512;
+        // process3DTriangles<PartialNode> needs 209 registers per thread when
+        // built for sm_100a (ptxas -v), so a 512-thread block exceeds the
+        // 64K-register file and calcOptSurfaceVoxelization fails with "too
+        // many resources requested for launch".  Every launch of the path is
+        // a grid-stride loop, so the block size changes only the scheduling
+        // (the order of racing material stores), not the work done.
+        if (Node::hasRatio()) dev.threads = 256;
         // voxelizeEntry device partition (1 device): host_side.cpp:782-813
         dev.resolution = host.resolution;
         dev.minVertex = mn;

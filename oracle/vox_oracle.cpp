@@ -13,6 +13,7 @@
 #include <cfloat>
 #include <climits>
 #include <cmath>
+#include <limits>
 #include <cstring>
 #include <unordered_map>
 #include <vector>
@@ -776,12 +777,187 @@ static void surfaceTriangle(const SurfaceCtx& c, uint tri, uint code, Bounds<u3>
     }
 }
 
+// ---------------------------------------------------------------------------
+// PartialNode volume ratio: processVoxel<PartialNode> and
+// calculateVoxelPlaneIntersectionVolume with its helpers,
+// src/voxelizer.cu:2996-3033, 4220-4807 (a Salama-Kolb style plane-box cut).
+// The reference computes, in FP32, the volume of the part of a voxel behind
+// the triangle's plane and stores |1 - volume / d^3|.  Facts of the
+// reference that the result depends on, restated here:
+//  * the voxel is the one centred at minCorner + d * (node coordinates), the
+//    node coordinates including the one-voxel padding, i.e. one voxel further
+//    along x, y and z than the voxel that passed the overlap test;
+//  * the plane normal is the class kernel's unnormalised cross product
+//    (zero for 1D-class triangles, which makes the ratio NaN);
+//  * |n.x|, |n.y| or |n.z| exactly 1 takes the axis-parallel shortcut;
+//  * when the plane misses the voxel the reference reads an unset array
+//    element for the cut polygon's pyramid; that pyramid counts as empty.
+// Operation order follows the reference; the reference build contracts some
+// multiply-adds and its normalize() uses rsqrtf, so this restatement (plain
+// IEEE operations, 1 / sqrtf) agrees with it to a tolerance, not bit for bit.
+namespace ratio {
+
+static inline f3 add(f3 a, f3 b) { return f3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline f3 mul(float s, f3 a) { return f3{s * a.x, s * a.y, s * a.z}; }
+static inline float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline f3 rotX(f3 v, float s, float c) { return f3{v.x, v.y * c - v.z * s, v.y * s + v.z * c}; }
+static inline f3 rotY(f3 v, float s, float c) { return f3{v.x * c + v.z * s, v.y, v.z * c - v.x * s}; }
+
+struct Poly { f3 p[6]; int n = 0; void push(f3 v) { if (n < 6) p[n++] = v; } };
+
+// Pyramid over `base` (rotated into a plane z = const) with apex `top`:
+// surveyor's formula for the base area.
+static float pyramid(const Poly& b, f3 top) {
+    float area = 0.0f;
+    for (int i = 0; i < b.n; i++) {
+        f3 u = b.p[i], w = b.p[(i + 1) % b.n];
+        area += 0.5f * (u.x * w.y - w.x * u.y);
+    }
+    float base0z = b.n ? b.p[0].z : 0.0f;
+    return std::fabs((1.0f / 3.0f) * area * (top.z - base0z));
+}
+
+// Rotates `poly` (and the apex) so that `rn` becomes the z axis: about x
+// when rn.y != 0, then about y when the (rotated) rn.x != 0.
+static float rotatedPyramid(Poly poly, f3 rn, f3 apex) {
+    f3 top = apex;
+    if (rn.y != 0.0f) {
+        float pl = std::sqrt(rn.y * rn.y + rn.z * rn.z);
+        float sn = rn.y / pl, cs = rn.z / pl;
+        top = rotX(top, sn, cs);
+        for (int i = 0; i < poly.n; i++) poly.p[i] = rotX(poly.p[i], sn, cs);
+        rn = rotX(rn, sn, cs);
+    }
+    if (rn.x != 0.0f) {
+        float pl = std::sqrt(rn.z * rn.z + rn.x * rn.x);
+        float sn = -rn.x / pl, cs = rn.z / pl;
+        top = rotY(top, sn, cs);
+        for (int i = 0; i < poly.n; i++) poly.p[i] = rotY(poly.p[i], sn, cs);
+    }
+    return pyramid(poly, top);
+}
+
+// `unstable` is set when an edge is (nearly) parallel to the plane (its
+// parameter is then 0 / 0, an infinity or a huge quotient) or when the plane
+// passes (nearly) through a voxel corner (a parameter near 0 or 1): which
+// side of [0, 1] the parameter falls on then depends on the last bits of the
+// products, so arithmetic with and without multiply-add contraction can take
+// different branches.
+static float cutVolume(const f3* t, f3 n, int x, int y, int z, f3 m, float d, bool& unstable) {
+    f3 vc = add(m, mul(d, f3{float(x), float(y), float(z)}));
+    if (std::fabs(n.x) == 1.0f) return (d * d) * ((d / 2.0f) + t[0].x - vc.x);
+    if (std::fabs(n.y) == 1.0f) return (d * d) * ((d / 2.0f) + t[0].y - vc.y);
+    if (std::fabs(n.z) == 1.0f) return (d * d) * ((d / 2.0f) + t[0].z - vc.z);
+    const bool sx = n.x > 0.0f, sy = n.y > 0.0f, sz = n.z > 0.0f;
+    // Steps along x, y, z away from the corner nearest the plane (the corner
+    // on the normal's side); the y and z steps trade places when an odd
+    // number of normal components are positive, keeping the frame
+    // right-handed.
+    const float ex = sx ? -d : d, ey = sy ? -d : d, ez = sz ? -d : d;
+    const bool even = ((int)sx + (int)sy + (int)sz) % 2 == 0;
+    const f3 dx{ex, 0.0f, 0.0f};
+    const f3 dy = even ? f3{0.0f, ey, 0.0f} : f3{0.0f, 0.0f, ez};
+    const f3 dz = even ? f3{0.0f, 0.0f, ez} : f3{0.0f, ey, 0.0f};
+    const float h = d / 2.0f;
+    f3 c[8];
+    c[0] = add(vc, f3{sx ? h : -h, sy ? h : -h, sz ? h : -h});
+    c[1] = add(c[0], dx);
+    c[2] = add(c[0], dy);
+    c[3] = add(c[0], dz);
+    c[4] = add(c[1], dz);
+    c[5] = add(c[2], dx);
+    c[6] = add(c[3], dy);
+    c[7] = add(c[4], dy);
+    // Walk three corner paths 0 -> A -> B -> 7 with a side edge A -> S; path
+    // k builds face k and closes the previous face where it turns at B.
+    static const int A[3] = {1, 2, 3}, B[3] = {4, 5, 6}, S[3] = {5, 6, 4};
+    const float nscale = (std::fabs(n.x) + std::fabs(n.y) + std::fabs(n.z)) * d;
+    auto along = [&](f3 p, f3 q) {
+        const float den = dot(n, f3{q.x - p.x, q.y - p.y, q.z - p.z});
+        if (!(std::fabs(den) > 1e-5f * nscale)) unstable = true;
+        const float tt = dot(n, f3{t[0].x - p.x, t[0].y - p.y, t[0].z - p.z}) / den;
+        if (std::fabs(tt) < 1e-4f || std::fabs(tt - 1.0f) < 1e-4f) unstable = true;
+        return tt;
+    };
+    auto point = [&](f3 p, f3 q, float tt) { return add(p, mul(tt, f3{q.x - p.x, q.y - p.y, q.z - p.z})); };
+    // A NaN tt (edge in the plane) is neither: the first two edges of a path
+    // are tested for "outside", the others for "inside", as in the reference.
+    auto inside = [](float tt) { return tt >= 0.0f && tt <= 1.0f; };
+    auto outside = [](float tt) { return tt < 0.0f || tt > 1.0f; };
+    Poly cut, face[3];
+    for (int k = 0; k < 3; k++) {
+        Poly& own = face[k];
+        Poly& prev = face[(k + 2) % 3];
+        const f3 a = c[A[k]], b = c[B[k]];
+        float tt = along(c[0], a);
+        if (outside(tt)) {
+            own.push(a);
+            tt = along(a, b);
+            if (outside(tt)) {
+                tt = along(b, c[7]);
+                if (inside(tt)) {
+                    f3 ip = point(b, c[7], tt);
+                    own.push(b); own.push(ip);
+                    prev.push(ip); prev.push(b);
+                    cut.push(ip);
+                } else {
+                    own.push(b);
+                    prev.push(b);
+                }
+            } else {
+                f3 ip = point(a, b, tt);
+                own.push(ip);
+                cut.push(ip);
+            }
+        } else {
+            cut.push(point(c[0], a, tt));
+        }
+        tt = along(a, c[S[k]]);
+        if (inside(tt)) {
+            f3 ip = point(a, c[S[k]], tt);
+            own.push(ip);
+            cut.push(ip);
+        }
+    }
+    float vol = rotatedPyramid(cut, n, c[0]);
+    for (int k = 0; k < 3; k++) {
+        const Poly& f = face[k];
+        if (f.n <= 2) continue;
+        f3 e0{f.p[0].x - f.p[2].x, f.p[0].y - f.p[2].y, f.p[0].z - f.p[2].z};
+        f3 e1{f.p[1].x - f.p[0].x, f.p[1].y - f.p[0].y, f.p[1].z - f.p[0].z};
+        f3 fn{e0.y * e1.z - e0.z * e1.y, e0.z * e1.x - e0.x * e1.z, e0.x * e1.y - e0.y * e1.x};
+        fn = mul(1.0f / std::sqrt(dot(fn, fn)), fn);
+        vol += rotatedPyramid(f, fn, c[0]);
+    }
+    return vol;
+}
+
+// The stored ratio for surface node (x, y, z) written by triangle `tri` of
+// class `cls` (1, 2, 3).
+static float nodeRatio(const SurfaceCtx& cx, uint tri, uint cls, int x, int y, int z, bool& unstable) {
+    f3 t[3];
+    fetchF(cx.V, cx.I, tri, t);
+    f3 n{0.0f, 0.0f, 0.0f};
+    if (cls >= 2)
+        n = crossF(sub3(t[0], t[2]), sub3(t[1], t[0]), (*cx.F)[cls == 2 ? ORC_S_CRF_2D : ORC_S_CRF_3D]);
+    else
+        return std::numeric_limits<float>::quiet_NaN();   // zero normal: every edge parameter is 0 / 0
+    float vol = cutVolume(t, n, x, y, z, cx.m, cx.d, unstable);
+    return std::fabs(1.0f - vol / (cx.d * cx.d * cx.d));
+}
+
+}  // namespace ratio
+
 // Deterministic material resolution.  The reference stores Node(1, mat)
 // with plain racing stores (src/voxelizer.cu:2988) from the 1D, 2D and 3D
 // kernels in that order, so a node ends with the material of *some*
 // triangle of the highest class that touched it.  This restatement (and the
 // CUDA path) picks the largest (class, material) key among those triangles.
-struct SurfaceRec { uint key; uint minMatTop; };
+// For PartialNode the stored ratio comes from one racing triangle as well;
+// here it is the largest (class, material, triangle index), and `topHits`
+// counts the triangles of the winning class (more than one: the reference's
+// ratio is not determined).
+struct SurfaceRec { uint key; uint minMatTop; uint tri; uint topHits; };
 
 static void surfacePass(const SurfaceCtx& c, uint nT, const std::vector<Bounds<u3> >& splits,
                         std::unordered_map<uint, SurfaceRec>& rec) {
@@ -804,7 +980,7 @@ static void surfacePass(const SurfaceCtx& c, uint nT, const std::vector<Bounds<u
     int nth = 1;
 #endif
     for (const Bounds<u3>& sub : splits) {
-        std::vector<std::vector<std::pair<uint, uint> > > local(nth);
+        std::vector<std::vector<SurfHit> > local(nth);
 #pragma omp parallel
         {
 #ifdef _OPENMP
@@ -818,20 +994,21 @@ static void surfacePass(const SurfaceCtx& c, uint nT, const std::vector<Bounds<u
                 uint code = codes[tri];
                 uint cls = code >> 30;
                 uint key = (cls << 8) | c.M[tri];
-                surfaceTriangle(c, tri, code, sub, [&](uint idx) { local[tid].push_back({idx, key}); });
+                surfaceTriangle(c, tri, code, sub, [&](uint idx) { local[tid].push_back(SurfHit{idx, key, tri}); });
             }
         }
         for (auto& l : local)
             for (auto& h : l) {
-                auto it = rec.find(h.first);
-                if (it == rec.end()) rec[h.first] = SurfaceRec{h.second, h.second & 255u};
+                auto it = rec.find(h.idx);
+                if (it == rec.end()) rec[h.idx] = SurfaceRec{h.key, h.key & 255u, h.tri, 1u};
                 else {
                     SurfaceRec& r = it->second;
-                    uint cls = h.second >> 8, rc = r.key >> 8;
-                    if (cls > rc) { r.key = h.second; r.minMatTop = h.second & 255u; }
+                    uint cls = h.key >> 8, rc = r.key >> 8;
+                    if (cls > rc) r = SurfaceRec{h.key, h.key & 255u, h.tri, 1u};
                     else if (cls == rc) {
-                        if (h.second > r.key) r.key = h.second;
-                        r.minMatTop = std::min(r.minMatTop, h.second & 255u);
+                        if (h.key > r.key || (h.key == r.key && h.tri > r.tri)) { r.key = h.key; r.tri = h.tri; }
+                        r.minMatTop = std::min(r.minMatTop, h.key & 255u);
+                        r.topHits++;
                     }
                 }
             }
@@ -841,7 +1018,8 @@ static void surfacePass(const SurfaceCtx& c, uint nT, const std::vector<Bounds<u
 // ---------------------------------------------------------------------------
 template <class N>
 static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, const uint* I, uint nT,
-               const uchar* M, void* out, uint8_t* conflict, orc_info* info) {
+               const uchar* M, void* out, uint8_t* conflict, orc_info* info, uint32_t* winTri = nullptr,
+               uint8_t* winCls = nullptr) {
     typedef Tr<N> T;
     const Fma F(p->fma_sites);
     const bool fcc = T::fcc;
@@ -861,6 +1039,7 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
         return 0;
     }
     const size_t nNodes = fcc ? (size_t)(2 * alloc.x) * alloc.y * (2 * alloc.z) : (size_t)alloc.x * alloc.y * alloc.z;
+    if (conflict) memset(conflict, 0, nNodes);
     N* nodes = (N*)out;
     N zero = T::make(0, 0);
 #pragma omp parallel for schedule(static)
@@ -921,17 +1100,30 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
             }
         }
     }
-    // processVoxel's Node(1, mat) for every surface node (max rule).
+    // processVoxel's Node(1, mat) for every surface node (max rule); the
+    // PartialNode ratio of the winning triangle.  Conflict bits: 1 = the
+    // winning class saw more than one material, 2 = more than one triangle.
     uint64_t nConf = 0;
-    for (auto& kv : rec) {
-        uint matv = kv.second.key & 255u;
+    const SurfaceCtx rc{V, I, M, f3{float(pl.mn.x), float(pl.mn.y), float(pl.mn.z)}, float(pl.d), alloc, false, 1, &F};
+    std::vector<std::pair<uint, SurfaceRec> > recs(rec.begin(), rec.end());
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : nConf)
+    for (long long i = 0; i < (long long)recs.size(); ++i) {
+        const uint idx = recs[i].first;
+        const SurfaceRec& r = recs[i].second;
+        uint matv = r.key & 255u;
         N nd = T::make(1, matv);
-        if (T::ratio) T::setR(nd, 0.0f);
-        nodes[kv.first] = nd;
-        if (kv.second.minMatTop != matv) {
-            nConf++;
-            if (conflict) conflict[kv.first] = 1;
+        if (T::ratio) {
+            const int x = (int)(idx % alloc.x), y = (int)(idx / alloc.x % alloc.y), z = (int)(idx / alloc.x / alloc.y);
+            bool unstable = false;
+            T::setR(nd, ratio::nodeRatio(rc, r.tri, r.key >> 8, x, y, z, unstable));
+            if (unstable && conflict) conflict[idx] |= 4;
         }
+        nodes[idx] = nd;
+        if (winTri) winTri[idx] = r.tri;
+        if (winCls) winCls[idx] = (uint8_t)(r.key >> 8);
+        uint8_t cf = (r.minMatTop != matv ? 1u : 0u) | (r.topHits > 1 ? 2u : 0u);
+        if (r.minMatTop != matv) nConf++;
+        if (conflict && cf) conflict[idx] |= cf;
     }
     info->n_conflicts = nConf;
     info->n_surface = rec.size();
@@ -1070,4 +1262,29 @@ extern "C" int orc_voxelize(const orc_params* p, const float* verts, uint32_t nV
     case ORC_LONG_FCC: return run<LFccN>(p, pl, verts, nV, idx, nT, mats, out, conflict, info);
     }
     return -13;
+}
+
+// Cartesian node outputs with, per node, the triangle and class that won its
+// surface record (0xFFFFFFFF / 0 where the node is not a surface node): the
+// inputs of the PartialNode ratio, for tests that evaluate it separately.
+extern "C" int orc_voxelize_winners(const orc_params* p, const float* verts, uint32_t nV, const uint32_t* idx,
+                                    uint32_t nT, const uint8_t* mats, uint32_t nMat, void* out, uint64_t out_bytes,
+                                    uint8_t* conflict, orc_info* info, uint32_t* win_tri, uint8_t* win_cls) {
+    if (!p->node_output || p->node_type != ORC_PARTIAL || !p->materials) return -13;
+    int rc = orc_plan(p, verts, nV, info);
+    if (rc) return rc;
+    if (out_bytes < info->out_bytes) return -14;
+    Plan pl = makePlan(p, verts, nV);
+    return run<PartialN>(p, pl, verts, nV, idx, nT, mats, out, conflict, info, win_tri, win_cls);
+}
+
+// The PartialNode ratio one triangle would give one node (the restatement
+// above), for tests that attribute a ratio to its triangle.
+extern "C" float orc_node_ratio(const orc_params* p, const float* verts, const uint32_t* idx, uint32_t tri,
+                                uint32_t cls, int x, int y, int z, const float* min_corner, float d) {
+    const Fma F(p->fma_sites);
+    const SurfaceCtx c{verts, idx, nullptr, f3{min_corner[0], min_corner[1], min_corner[2]}, d, u3{0, 0, 0},
+                       false, 1, &F};
+    bool unstable = false;
+    return ratio::nodeRatio(c, tri, cls, x, y, z, unstable);
 }

@@ -77,11 +77,28 @@ typedef struct {
 int orc_plan(const orc_params* p, const float* verts, uint32_t n_verts, orc_info* info);
 
 /* Full voxelization into `out` (host memory, `out_bytes` >= info.out_bytes).
- * `conflict_out` (optional, one byte per node) receives 1 where the surface
- * material of a node was contested inside its winning triangle class. */
+ * `conflict_out` (optional, one byte per node) receives bit 1 where the
+ * surface material of a node was contested inside its winning triangle class
+ * and bit 2 where more than one triangle of that class hit the node (the
+ * reference's PartialNode ratio then depends on which store landed last);
+ * bit 4 marks a PartialNode ratio computed with an edge (nearly) parallel to
+ * the plane, where contracted and plain FP32 arithmetic can branch apart. */
 int orc_voxelize(const orc_params* p, const float* verts, uint32_t n_verts, const uint32_t* indices,
                  uint32_t n_tris, const uint8_t* materials, uint32_t n_materials, void* out,
                  uint64_t out_bytes, uint8_t* conflict_out, orc_info* info);
+
+/* PartialNode with materials only: orc_voxelize plus, per node, the winning
+ * surface triangle (`win_tri`, 0xFFFFFFFF elsewhere; caller fills) and its
+ * class 1..3 (`win_cls`). */
+int orc_voxelize_winners(const orc_params* p, const float* verts, uint32_t n_verts, const uint32_t* indices,
+                         uint32_t n_tris, const uint8_t* materials, uint32_t n_materials, void* out,
+                         uint64_t out_bytes, uint8_t* conflict_out, orc_info* info, uint32_t* win_tri,
+                         uint8_t* win_cls);
+
+/* The PartialNode ratio triangle `tri` of class `cls` would store at node
+ * (x, y, z) of a grid with minimum corner `min_corner` and voxel length d. */
+float orc_node_ratio(const orc_params* p, const float* verts, const uint32_t* indices, uint32_t tri, uint32_t cls,
+                     int x, int y, int z, const float* min_corner, float d);
 
 #ifdef __cplusplus
 }

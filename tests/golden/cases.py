@@ -132,6 +132,8 @@ CASES = [
     # which racing triangle wrote last).
     case("ico4_partial_nomat", "ico4", PARTIAL, 1, 0, 1.0 / 64.0),
     case("ico4_partial_mat", "ico4", PARTIAL, 1, 1, 1.0 / 64.0, strict_mats=False),
+    case("torus_partial_mat", "torus", PARTIAL, 1, 1, 96, strict_mats=False),
+    case("stress_partial_mat", "stress", PARTIAL, 1, 1, 1.0 / 96.0, mat=(48, 48, 48), strict_mats=False),
 ]
 
 BY_NAME = {c["name"]: c for c in CASES}

@@ -19,7 +19,9 @@ import pytest
 
 import cases as C
 import oracle as O
-from helpers import bid_of, describe_diff, mat_of, masked
+from helpers import (CONFLICT_MAT, CONFLICT_RATIO, PARTIAL, RATIO_REF_TOL, RATIO_TOL, RATIO_UNSTABLE, bid_of,
+                     describe_diff,
+                     mat_of, masked, ratio_bad, ratio_of)
 from voxelizer_b200.api import Voxelizer
 
 pytestmark = pytest.mark.gpu
@@ -31,7 +33,8 @@ INDEX = json.load(open(os.path.join(GOLD, "index.json")))
 # Cases whose oracle output is not yet pinned to the reference at exact FP32
 # ties of the surface tests (vertices snapped to voxel corners).  The CUDA
 # path must still equal the oracle exactly on them.
-UNPINNED = {"stress_short_mat", "stress_long_splits", "stress_sfcc_mat", "stress_lfcc_mat", "stress_full_sfcc"}
+UNPINNED = {"stress_short_mat", "stress_long_splits", "stress_sfcc_mat", "stress_lfcc_mat", "stress_full_sfcc",
+            "stress_partial_mat"}
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -70,20 +73,40 @@ def test_small_cases(name):
     want, _, conf = O.voxelize(m, c["node_type"], c["nodes"], c["materials"], c["size"], c["vox"], c["mat"],
                                want_conflicts=True)
     want = masked(c["node_type"], c["nodes"], want)
-    assert np.array_equal(got, want), "CUDA vs oracle: " + describe_diff(got, want, info.dims)
+    nt = c["node_type"]
+    ratios = nt == PARTIAL and c["materials"]
+    if ratios:
+        # Same winning triangle per node; the ratio field within the oracle's
+        # tolerance, everything else exact.
+        low = np.uint64(0xFFFFFFFF)
+        assert np.array_equal(got & low, want & low), "CUDA vs oracle: " + describe_diff(got & low, want & low)
+        stable = np.nonzero((conf & RATIO_UNSTABLE) == 0)[0]
+        bad = stable[ratio_bad(got[stable], want[stable], RATIO_TOL)]
+        assert bad.size == 0, f"CUDA vs oracle: {bad.size} ratios differ: {ratio_of(got[bad[:5]])} vs " \
+                              f"{ratio_of(want[bad[:5]])}"
+    else:
+        assert np.array_equal(got, want), "CUDA vs oracle: " + describe_diff(got, want, info.dims)
     gold = np.load(os.path.join(GOLD, name + ".npz"))["out"]
     if name in UNPINNED:
         return
     if not c["nodes"]:
         assert np.array_equal(got, gold), "CUDA vs reference: " + describe_diff(got, gold, info.dims)
         return
-    nt = c["node_type"]
     assert np.array_equal(bid_of(nt, got), bid_of(nt, gold)), "ids vs reference: " + describe_diff(
         bid_of(nt, got), bid_of(nt, gold), info.dims)
-    keep = conf == 0
+    keep = (conf & CONFLICT_MAT) == 0
     gm, wm = mat_of(nt, got), mat_of(nt, gold)
     assert np.array_equal(gm[keep], wm[keep]), "materials vs reference: " + describe_diff(gm[keep], wm[keep])
-    if INDEX[name]["deterministic"]:
+    if ratios:
+        # Against the reference's own ratio wherever a single triangle of the
+        # winning class wrote the node (non-surface nodes hold exactly 0 or 1)
+        # and no edge parameter sits at a branch point.
+        sole = np.nonzero((conf & (CONFLICT_RATIO | RATIO_UNSTABLE)) == 0)[0]
+        bad = sole[ratio_bad(got[sole], gold[sole], RATIO_REF_TOL)]
+        exact = int(np.count_nonzero((got >> np.uint64(32))[sole] == (gold >> np.uint64(32))[sole]))
+        assert bad.size == 0, f"ratios vs reference: {bad.size} of {sole.size} beyond {RATIO_REF_TOL} " \
+                              f"({exact} bit-identical): {ratio_of(got[bad[:5]])} vs {ratio_of(gold[bad[:5]])}"
+    elif INDEX[name]["deterministic"]:
         assert np.array_equal(got, gold)
 
 

@@ -137,13 +137,14 @@ def test_cli_argument_errors(tmp_path, capsys, sphere):
     assert "No resolution or distance" in capsys.readouterr().out
     assert cli.main([str(tmp_path / "missing.obj"), "-r", "32"]) == 1
     a = cli.parser().parse_args([path, "-r", "64", "-L", "-F", "-m", "-V", "64", "32", "32"])
+    assert a.resolution == 64 and a.long and a.fcc and a.materials
     assert cli._node_type(a) == cli.api.LONG_FCC and a.voxRes == [64, 32, 32]
 
 
 # --- GPU: a mesh from a file voxelizes exactly like the same mesh from memory ---
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("fmt,flags", [("obj", []), ("stl", ["-L", "-m"]), ("ply", ["-F", "-m"]),
+@pytest.mark.parametrize("fmt,flags", [("obj", []), ("stl", ["-L", "-m"]), ("ply", ["-F", "-m", "-d", "0.025"]),
                                        ("vtk", ["-x"]), ("obj", ["-L", "-F", "-d", "0.03"])])
 def test_cli_file_matches_memory(tmp_path, fmt, flags):
     import oracle as O
@@ -154,7 +155,7 @@ def test_cli_file_matches_memory(tmp_path, fmt, flags):
         fmt, lambda p, v, f: _write_vtk(p, v, f.tolist()))(path, mesh.vertices, mesh.indices)
     out = str(tmp_path / "out.npy")
     args = [path, *flags, "-o", out]
-    if "-d" not in flags:
+    if "-d" not in flags:   # FCC lattices are sized by cube length only (as in the reference)
         args += ["-r", "96"]
     assert cli.main(args) == 0
     got = np.load(out).reshape(-1)

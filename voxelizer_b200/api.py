@@ -18,7 +18,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import LONG, LONG_FCC, NODE_BYTES, PARTIAL, SHORT, SHORT_FCC, check, lib, make_request  # noqa: F401
+from ._lib import LONG, LONG_FCC, NODE_BYTES, PARTIAL, SHORT, SHORT_FCC, VxbError, check, lib, make_request  # noqa: F401
 
 NODE_DTYPE = {SHORT: np.uint8, LONG: np.uint16, PARTIAL: np.uint64, SHORT_FCC: np.uint16, LONG_FCC: np.uint32}
 DEFAULT_VOX = (1024, 512, 512)

@@ -101,19 +101,23 @@ def main(argv=None):
     size = a.resolution if a.resolution is not None else float(a.distance)
     vox_res = tuple(a.voxRes) if a.voxRes else api.DEFAULT_VOX
     mat_res = tuple(a.matRes) if a.matRes else api.DEFAULT_MAT
-    with api.Voxelizer(mesh.vertices, mesh.indices, node_type=node_type, device=a.device) as vz:
-        if a.verbose:
-            vz.verboseOutput(True)
-        if a.materials:
-            mats = (1 + np.arange(mesh.n_triangles) % 7).astype(np.uint8)
-            vz.setMaterials(mats, 8)
-            vz.setMaterialOutput(True)
-        t0 = time.perf_counter()
-        if a.voxels:
-            result, info = vz.voxelizeToRAM(size, vox_res)
-        else:
-            result, info = vz.voxelizeToNodesToRAM(size, vox_res, mat_res)
-        dt = time.perf_counter() - t0
+    try:
+        with api.Voxelizer(mesh.vertices, mesh.indices, node_type=node_type, device=a.device) as vz:
+            if a.verbose:
+                vz.verboseOutput(True)
+            if a.materials:
+                mats = (1 + np.arange(mesh.n_triangles) % 7).astype(np.uint8)
+                vz.setMaterials(mats, 8)
+                vz.setMaterialOutput(True)
+            t0 = time.perf_counter()
+            if a.voxels:
+                result, info = vz.voxelizeToRAM(size, vox_res)
+            else:
+                result, info = vz.voxelizeToNodesToRAM(size, vox_res, mat_res)
+            dt = time.perf_counter() - t0
+    except api.VxbError as e:
+        print(e)
+        return 1
     print(f"{mesh.n_vertices} vertices, {mesh.n_triangles} triangles; voxelized in {dt * 1e3:.2f} ms")
     for line in summarize(result, info, not a.voxels, node_type):
         print(line)

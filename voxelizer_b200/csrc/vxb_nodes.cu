@@ -15,6 +15,7 @@
 #include "vxb_common.cuh"
 #include "vxb_device.cuh"
 #include "vxb_kernels.cuh"
+#include "vxb_ratio.cuh"
 
 namespace vxb {
 
@@ -398,6 +399,8 @@ __global__ void __launch_bounds__(256) emitPartialKernel(EmitArgs a, uint64_t to
             continue;
         }
         uint32_t matRank = n.s0 ? __ldg(a.ranks + U.wordBase + w) : 0u;
+        // Node coordinates of the word's first node (ratio of surface nodes).
+        const int x0 = (int)(w % U.g.ipx) * 32, y0 = (int)(w / U.g.ipx % U.g.AY), z0 = (int)(w / U.g.ipx / U.g.AY);
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
             uint32_t v32[4];
@@ -406,13 +409,18 @@ __global__ void __launch_bounds__(256) emitPartialKernel(EmitArgs a, uint64_t to
                 const uint32_t bt = 2 * i + j, q = 31u - bt;
                 uint32_t bid = 0, mat = 0;
                 if ((n.c >> q) & 1u) bid = lut[permOf(n, q)];
+                // constructNodeList2 writes float(solid); processVoxel<PartialNode>
+                // overwrites surface nodes with the winning triangle's ratio.
+                float r = ((n.f0 >> q) & 1u) ? 1.0f : 0.0f;
                 if ((n.s0 >> q) & 1u) {
-                    mat = matRank < a.keysCap
-                              ? NT::keyMat(reinterpret_cast<const unsigned long long*>(a.keys)[matRank])
-                              : 0u;
+                    if (matRank < a.keysCap) {
+                        const uint64_t key = reinterpret_cast<const unsigned long long*>(a.keys)[matRank];
+                        mat = NT::keyMat(key);
+                        r = ratio::nodeRatio(U.V, U.I, (uint32_t)key, (uint32_t)(key >> 40), x0 + (int)bt, y0, z0,
+                                             detail::F3{U.g.mnf[0], U.g.mnf[1], U.g.mnf[2]}, U.g.df);
+                    }
                     ++matRank;
                 }
-                const float r = ((n.f0 >> q) & 1u) && !((n.s0 >> q) & 1u) ? 1.0f : 0.0f;
                 const uint64_t nv = NT::pack(bid, mat, r);
                 v32[2 * j] = (uint32_t)nv;
                 v32[2 * j + 1] = (uint32_t)(nv >> 32);
