@@ -10,9 +10,13 @@
 //    delete[]s them (NodePointer::ptr or ::vptr).
 //  * voxelize / voxelizeToNodes return device pointers allocated with
 //    cudaMalloc on device 0; the caller cudaFree()s them.
-// Only one device is used: devConfig must be (1, 1).  The slice API and
-// simulateMultidevice are declared for source compatibility and throw
-// vox::Exception.
+// One GPU: devConfig (dy, dz) partitions the grid as the reference's
+// devices do (each partition voxelized with its overlap rows, faces zeroed in
+// node output) but runs every partition on this voxelizer's device; the
+// NodePointers carry each partition's dim and loc.  Inside
+// simulateMultidevice the results are host arrays (new[]), as the
+// reference's collectData uploads them.  Slices along y and z are provided
+// (devConfig 1); slicing along x (the reference rotates the mesh) throws.
 #ifndef VOX_VOXELIZER_B200_H
 #define VOX_VOXELIZER_B200_H
 
@@ -202,7 +206,8 @@ public:
     NodePointer<Node> voxelizeToNodesToRAM(double cubeLength, uint3 voxSplitRes = make_uint3(1024, 512, 512),
                                            uint3 matSplitRes = make_uint3(512, 512, 512));
 
-    // Slice API: declared for source compatibility, not provided.
+    // Slices (src/host_side.cpp:1927-2262): direction 1 (y) or 2 (z); a
+    // three-layer node array whose middle layer is slice `slice`.
     std::vector<NodePointer<Node> > voxelizeSlice(uint maxDimension, int direction, uint slice, uint devConfig = 1,
                                                   uint2 voxSplitRes = make_uint2(1024, 512),
                                                   uint2 matSplitRes = make_uint2(512, 512));
@@ -236,6 +241,9 @@ private:
     Voxelizer& operator=(const Voxelizer&);
 
     NodePointer<Node> run(bool toHost, uint3 voxSplitRes, uint3 matSplitRes);
+    std::vector<NodePointer<Node> > runParts(uint2 devConfig, uint3 voxSplitRes, uint3 matSplitRes);
+    NodePointer<Node> runSlice(bool toHost, int direction, uint slice, uint2 voxSplitRes, uint2 matSplitRes);
+    vxb_request request(uint3 voxSplitRes, uint3 matSplitRes) const;
 
     vxb_voxelizer* handle;
     std::vector<float> vertices;
@@ -245,6 +253,7 @@ private:
     // Options struct (include/host_support.h:39-56).
     bool nodeOutput;
     bool voxelDistanceGiven;
+    bool simulate = false;   // inside simulateMultidevice
     uint maxDimensionSetting;
     double voxelLength;
     double3 minVertex, maxVertex;

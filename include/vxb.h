@@ -68,6 +68,11 @@ typedef struct {
     double max_vertex[3];
     vxb_uint3 resolution;      /* voxel resolution incl. x padding/rounding, before y/z padding */
     uint32_t x_splits;
+    /* Device spaces (partitions, slices): NodePointer::loc, the partition's
+     * index (0, y, z) among the partitions, and its voxel range [y0, y1) x
+     * [z0, z1) of the full grid; (0, 0, 0) and the whole grid otherwise. */
+    vxb_uint3 location;
+    uint32_t partition[4];
 } vxb_grid_info;
 
 typedef struct vxb_voxelizer vxb_voxelizer;
@@ -107,8 +112,9 @@ vxb_status vxb_verbose_output(vxb_voxelizer* v, int enable);
 vxb_status vxb_plan(vxb_voxelizer* v, int nodes, const vxb_request* req, vxb_grid_info* info);
 
 /* getArrayDimensions(longestSizeInVoxels | cubeLength, maxInternalXSize,
- * sliceAlongX), src/host_side.cpp:3329-3475.  sliceAlongX is not supported
- * (the slice API is outside this library) and returns VXB_EUNSUPPORTED. */
+ * sliceAlongX), src/host_side.cpp:3329-3475.  sliceAlongX (the dimensions of
+ * the rotated model the reference slices along x) returns
+ * VXB_EUNSUPPORTED, as slicing along x does. */
 vxb_status vxb_get_array_dimensions(vxb_voxelizer* v, int by_cube_length, uint32_t max_dimension,
                                     double cube_length, uint32_t max_internal_x, int slice_along_x,
                                     vxb_uint3* dims);
@@ -127,6 +133,45 @@ vxb_status vxb_voxelize_to_host(vxb_voxelizer* v, int nodes, const vxb_request* 
  * once, after all launches. */
 vxb_status vxb_voxelize_to_device(vxb_voxelizer* v, int nodes, const vxb_request* req, void* dev_out,
                                   uint64_t dev_bytes, void* stream, vxb_grid_info* info);
+
+/* Partitioned voxelization: voxelize / voxelizeToNodes with devConfig
+ * (dev_y, dev_z), include/voxelizer.h:718-770 and src/host_side.cpp:782-1011
+ * (voxelizeEntry / voxelizeWorker).  The yz voxel range is split into
+ * dev_y x dev_z partitions (splitResolutionByNrOfParts; remainders to the
+ * first part) and each is voxelized as the reference voxelizes it on its own
+ * device: its box grows by one voxel towards each neighbouring partition,
+ * the allocation is the partition plus one row on each side, and in node
+ * output the allocation's faces are zeroed (zeroPadding).  The reference
+ * hands one NodePointer per device; here every partition is its own output
+ * buffer and all of them run as one batch on this voxelizer's GPU.  Arrays
+ * hold dev_y * dev_z entries, y fastest; info.location is the partition's
+ * (0, y, z).  FCC lattices return VXB_EUNSUPPORTED. */
+vxb_status vxb_plan_parts(vxb_voxelizer* v, int nodes, const vxb_request* req, uint32_t dev_y, uint32_t dev_z,
+                          vxb_grid_info* infos);
+vxb_status vxb_voxelize_parts_to_device(vxb_voxelizer* v, int nodes, const vxb_request* req, uint32_t dev_y,
+                                        uint32_t dev_z, void* const* dev_outs, const uint64_t* dev_bytes,
+                                        void* stream, vxb_grid_info* infos);
+vxb_status vxb_voxelize_parts_to_host(vxb_voxelizer* v, int nodes, const vxb_request* req, uint32_t dev_y,
+                                      uint32_t dev_z, void* const* host_outs, const uint64_t* host_bytes,
+                                      vxb_grid_info* infos);
+
+/* Slices: voxelizeSlice / voxelizeSliceToRAM with devConfig 1,
+ * include/voxelizer.h:765-795, src/host_side.cpp:1927-2262.  `direction`
+ * 1 (y) or 2 (z) is the slice normal; `slice` counts grid rows including
+ * the padding row, so 1 .. resolution are the voxel rows.  The result is
+ * the node array of a partition one voxel thick: three layers along
+ * `direction`, the middle one the slice, the outer ones (and all faces)
+ * zero; boundary ids see the voxelized neighbour rows.  Slice 0 or past the
+ * grid gives the zero array (sliceOOB).  Node output only; the request's
+ * split sizes are used as given (the reference's uint2 (a, b) means
+ * (a, b, b)).  Direction 0 (the reference rotates the mesh) and FCC lattices
+ * return VXB_EUNSUPPORTED. */
+vxb_status vxb_plan_slice(vxb_voxelizer* v, const vxb_request* req, int direction, uint32_t slice,
+                          vxb_grid_info* info);
+vxb_status vxb_voxelize_slice_to_device(vxb_voxelizer* v, const vxb_request* req, int direction, uint32_t slice,
+                                        void* dev_out, uint64_t dev_bytes, void* stream, vxb_grid_info* info);
+vxb_status vxb_voxelize_slice_to_host(vxb_voxelizer* v, const vxb_request* req, int direction, uint32_t slice,
+                                      void* host_out, uint64_t host_bytes, vxb_grid_info* info);
 
 /* Number of kernels the last voxelize call launched on the device. */
 vxb_status vxb_last_launch_count(vxb_voxelizer* v, uint32_t* launches);

@@ -62,7 +62,8 @@ class _Params(ctypes.Structure):
     _fields_ = [("node_type", ctypes.c_int), ("node_output", ctypes.c_int), ("materials", ctypes.c_int),
                 ("by_cube_length", ctypes.c_int), ("max_dim", ctypes.c_uint32), ("cube_length", ctypes.c_double),
                 ("vox_split", ctypes.c_uint32 * 3), ("mat_split", ctypes.c_uint32 * 3),
-                ("fma_sites", ctypes.c_uint8 * 48), ("threads", ctypes.c_int)]
+                ("fma_sites", ctypes.c_uint8 * 48), ("threads", ctypes.c_int), ("space", ctypes.c_int),
+                ("part", ctypes.c_uint32 * 4)]
 
 
 class Info(ctypes.Structure):
@@ -92,7 +93,7 @@ def lib():
     return _lib
 
 
-def _params(node_type, nodes, materials, size, vox, mat, fma_model, threads):
+def _params(node_type, nodes, materials, size, vox, mat, fma_model, threads, part=None):
     p = _Params()
     p.node_type = int(node_type)
     p.node_output = int(bool(nodes))
@@ -104,6 +105,9 @@ def _params(node_type, nodes, materials, size, vox, mat, fma_model, threads):
     p.mat_split[:] = list(mat)
     p.fma_sites[:] = fma_sites(fma_model)
     p.threads = int(threads)
+    if part is not None:   # device space: yz partition (y0, y1, z0, z1) of the grid
+        p.space = 1
+        p.part[:] = [int(v) for v in part]
     return p
 
 
@@ -113,8 +117,8 @@ def out_dtype(node_type, nodes):
     return {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}[NODE_BYTES[node_type]]
 
 
-def plan(mesh, node_type, nodes, size, vox=(1024, 512, 512)):
-    p = _params(node_type, nodes, 0, size, vox, (512, 512, 512), None, 0)
+def plan(mesh, node_type, nodes, size, vox=(1024, 512, 512), part=None):
+    p = _params(node_type, nodes, 0, size, vox, (512, 512, 512), None, 0, part)
     info = Info()
     rc = lib().orc_plan(ctypes.byref(p), mesh.vertices.ctypes.data, mesh.n_vertices, ctypes.byref(info))
     if rc:
@@ -123,9 +127,10 @@ def plan(mesh, node_type, nodes, size, vox=(1024, 512, 512)):
 
 
 def voxelize(mesh, node_type, nodes, materials, size, vox=(1024, 512, 512), mat=(512, 512, 512),
-             fma_model=None, threads=0, want_conflicts=False):
-    """Returns (output array (flat), Info, conflict mask or None)."""
-    p = _params(node_type, nodes, materials, size, vox, mat, fma_model, threads)
+             fma_model=None, threads=0, want_conflicts=False, part=None):
+    """Returns (output array (flat), Info, conflict mask or None).  `part`
+    (y0, y1, z0, z1) voxelizes that partition as a device space."""
+    p = _params(node_type, nodes, materials, size, vox, mat, fma_model, threads, part)
     info = Info()
     L = lib()
     rc = L.orc_plan(ctypes.byref(p), mesh.vertices.ctypes.data, mesh.n_vertices, ctypes.byref(info))

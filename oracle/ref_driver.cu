@@ -80,6 +80,19 @@ static Split3 split3(uint3 maxDim, Bounds<uint3> r) {
     return s;
 }
 
+// zeroPadding (src/voxelizer.cu:4811-4844), Cartesian nodes: every node on a
+// face of the device array becomes Node().  The reference reaches it through
+// makePaddingZero, whose only instantiations the compiler inlines into
+// dummyFunction (src/voxelizer.cu:4862-4886), so no out-of-line copy exists
+// for this driver to call; the kernel is restated here.
+template <class Node> __global__ void refZeroFaces(Node* nodes, uint3 dim) {
+    const uint n = dim.x * dim.y * dim.z;
+    for (uint i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint x = i % dim.x, y = (i % (dim.x * dim.y)) / dim.x, z = i / (dim.x * dim.y);
+        if (x == 0 || x == dim.x - 1 || y == 0 || y == dim.y - 1 || z == 0 || z == dim.z - 1) nodes[i] = Node();
+    }
+}
+
 struct RefError { int code; };
 #define RCHK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) throw RefError{(int)e_}; } while (0)
 
@@ -92,6 +105,11 @@ struct Params {
     double cube_length;
     uint3 vox_split;
     uint3 mat_split;
+    // Device space: voxelize the yz partition [part[0], part[1]) x
+    // [part[2], part[3]) as voxelizeEntry assigns it to one device
+    // (host_side.cpp:782-813) and voxelizeWorker runs it (911-1236).
+    int space;
+    uint part[4];
 };
 
 // host_side.cpp:2462-2488
@@ -254,14 +272,34 @@ struct Runner {
         // a grid-stride loop, so the block size changes only the scheduling
         // (the order of racing material stores), not the work done.
         if (Node::hasRatio()) dev.threads = 256;
-        // voxelizeEntry device partition (1 device): host_side.cpp:782-813
+        // voxelizeEntry device partition: host_side.cpp:782-813 (the whole
+        // grid, or the requested partition of it)
         dev.resolution = host.resolution;
-        dev.minVertex = mn;
-        dev.left = dev.right = dev.up = dev.down = false;
+        if (p.space) {
+            if (fcc || !(p.part[0] < p.part[1] && p.part[1] <= res.y && p.part[2] < p.part[3] && p.part[3] <= res.z))
+                return -3;
+            dev.resolution.min = make_uint3(0, p.part[0], p.part[2]);
+            dev.resolution.max = make_uint3(res.x, p.part[1], p.part[3]);
+        }
+        dev.minVertex = make_double3(mn.x + double(dev.resolution.min.x) * d, mn.y + double(dev.resolution.min.y) * d,
+                                     mn.z + double(dev.resolution.min.z) * d);
+        // voxelizeWorker neighbour flags, host_side.cpp:920-949
+        {
+            const Bounds<uint3> pt = dev.resolution, hr = host.resolution;
+            dev.left = dev.right = dev.up = dev.down = false;
+            if (pt.min.y == hr.min.y && pt.max.y != hr.max.y) dev.right = true;
+            else if (pt.max.y == hr.max.y && pt.min.y != hr.min.y) dev.left = true;
+            else if (pt.min.y != hr.min.y && pt.max.y != hr.max.y) dev.left = dev.right = true;
+            if (pt.min.z == hr.min.z && pt.max.z != hr.max.z) dev.up = true;
+            else if (pt.max.z == hr.max.z && pt.min.z != hr.min.z) dev.down = true;
+            else if (pt.min.z != hr.min.z && pt.max.z != hr.max.z) dev.down = dev.up = true;
+        }
         dev.allocResolution = dev.resolution;
         dev.allocResolution.max.y += 2;
         dev.allocResolution.max.z += 2;
-        uint3 ar = make_uint3(dev.allocResolution.max.x, dev.allocResolution.max.y, dev.allocResolution.max.z);
+        uint3 ar = make_uint3(dev.allocResolution.max.x - dev.allocResolution.min.x,
+                              dev.allocResolution.max.y - dev.allocResolution.min.y,
+                              dev.allocResolution.max.z - dev.allocResolution.min.z);
         uint nNodes = fcc ? 2 * ar.x * ar.y * 2 * ar.z : ar.x * ar.y * ar.z;
         uint nInts = (ar.x * ar.y * ar.z) >> VOX_DIV;
         uint3 outDim = fcc ? make_uint3(2 * ar.x, ar.y, 2 * ar.z) : ar;
@@ -296,9 +334,14 @@ struct Runner {
         offsetBuffer.assign(nT, 0);
         dev.maxWorkQueueSize = 0;
         {
-            // host_side.cpp:986-1041 / 1357-1400 (no neighbouring devices)
+            // host_side.cpp:986-1041 / 1357-1400: the partition extended by
+            // one voxel towards each neighbouring partition
             Bounds<uint3> part = dev.resolution;
             Bounds<uint3> ext = part;
+            ext.min.y -= dev.left ? 1 : 0;
+            ext.min.z -= dev.down ? 1 : 0;
+            ext.max.y += dev.right ? 1 : 0;
+            ext.max.z += dev.up ? 1 : 0;
             dev.extMinVertex = make_double3(mn.x + double(ext.min.x) * d, mn.y + double(ext.min.y) * d,
                                             mn.z + double(ext.min.z) * d);
             Split2 extYz = splitYZ(make_uint2(p.vox_split.y, p.vox_split.z), ext);
@@ -328,6 +371,11 @@ struct Runner {
                             procNodeList<Node>(dev, (Node*)g.nodes, nullptr, g.error, allocYz.splits[i], false, 0, false);
                             RCHK(cudaMemcpy(&e, g.error, sizeof(bool), cudaMemcpyDeviceToHost));
                         } while (e);
+                    }
+                    // host_side.cpp:1211-1222
+                    if (dev.left || dev.right || dev.up || dev.down) {
+                        refZeroFaces<Node><<<dev.blocks, dev.threads>>>((Node*)g.nodes, ar);
+                        RCHK(cudaGetLastError());
                     }
                 }
             } else {
@@ -396,16 +444,21 @@ static char g_refError[512] = {0};
 
 extern "C" const char* ref_last_error() { return g_refError; }
 
-extern "C" int ref_voxelize(int node_type, int node_output, int materials, int by_cube_length,
-                            uint32_t max_dim, double cube_length, const uint32_t* vox_split,
-                            const uint32_t* mat_split, const float* verts, uint32_t nV,
-                            const uint32_t* idx, uint32_t nT, const uint8_t* mats, uint32_t nMat,
-                            void* out, uint64_t out_bytes, uint32_t* dims_out, double* ms) {
+// ref_voxelize over one device space: `part` (y0, y1, z0, z1), or NULL for
+// the whole grid.
+extern "C" int ref_voxelize_space(int node_type, int node_output, int materials, int by_cube_length,
+                                  uint32_t max_dim, double cube_length, const uint32_t* vox_split,
+                                  const uint32_t* mat_split, const float* verts, uint32_t nV,
+                                  const uint32_t* idx, uint32_t nT, const uint8_t* mats, uint32_t nMat,
+                                  const uint32_t* part, void* out, uint64_t out_bytes, uint32_t* dims_out,
+                                  double* ms) {
     Params p;
     p.node_type = node_type; p.node_output = node_output; p.materials = materials;
     p.by_cube_length = by_cube_length; p.max_dim = max_dim; p.cube_length = cube_length;
     p.vox_split = make_uint3(vox_split[0], vox_split[1], vox_split[2]);
     p.mat_split = make_uint3(mat_split[0], mat_split[1], mat_split[2]);
+    p.space = part ? 1 : 0;
+    for (int k = 0; k < 4; ++k) p.part[k] = part ? part[k] : 0u;
     try {
         switch (node_type) {
         case 0: { Runner<ShortNode> r(p); return r.run(verts, nV, idx, nT, mats, nMat, out, out_bytes, dims_out, ms); }
@@ -421,4 +474,13 @@ extern "C" int ref_voxelize(int node_type, int node_output, int materials, int b
         return -4;
     }
     return -5;
+}
+
+extern "C" int ref_voxelize(int node_type, int node_output, int materials, int by_cube_length,
+                            uint32_t max_dim, double cube_length, const uint32_t* vox_split,
+                            const uint32_t* mat_split, const float* verts, uint32_t nV,
+                            const uint32_t* idx, uint32_t nT, const uint8_t* mats, uint32_t nMat,
+                            void* out, uint64_t out_bytes, uint32_t* dims_out, double* ms) {
+    return ref_voxelize_space(node_type, node_output, materials, by_cube_length, max_dim, cube_length, vox_split,
+                              mat_split, verts, nV, idx, nT, mats, nMat, nullptr, out, out_bytes, dims_out, ms);
 }

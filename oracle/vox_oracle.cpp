@@ -217,8 +217,16 @@ struct Plan {
     double d;
     u3 res;       // resolution.max (x includes padding and rounding)
     uint xSplits, xRes;
-    u3 alloc;     // res + (0,2,2)
+    u3 alloc;     // res + (0,2,2); a device space: partition + (0,2,2)
     int err;
+    // Device space, voxelizeWorker (src/host_side.cpp:911-1011): the
+    // voxelized (extended) box `ext` (local extents), its minimum corner
+    // (extMinVertex), the allocation row of local row 0 (padding: 1, overlap
+    // with a neighbour: 0) and whether zeroPadding clears the faces.
+    d3 mnExt;
+    u3 ext;
+    uint padY, padZ;
+    bool border;
 };
 
 static Plan makePlan(const orc_params* p, const float* v, uint nV) {
@@ -276,10 +284,39 @@ static Plan makePlan(const orc_params* p, const float* v, uint nV) {
     pl.res = res;
     pl.xRes = res.x / pl.xSplits;
     pl.alloc = u3{res.x, res.y + 2, res.z + 2};
+    pl.mnExt = pl.mn;
+    pl.ext = res;
+    pl.padY = pl.padZ = 1;
+    pl.border = false;
     // The solid voxelizer's per-split word mask holds at most 32 words
     // (src/voxelizer.cu:1579-1616): larger x passes are undefined there.
     if (pl.xRes > 1024) pl.err = -12;
     return pl;
+}
+
+// The device space of partition p->part (voxelizeWorker,
+// src/host_side.cpp:911-1011): neighbour flags from the partition's
+// position, the box extended by one voxel towards each neighbour, its
+// minimum corner hostMin + extMin * d, the allocation partition + 2.
+static void applySpace(const orc_params* p, Plan& pl) {
+    if (!p->space || pl.err) return;
+    const uint y0 = p->part[0], y1 = p->part[1], z0 = p->part[2], z1 = p->part[3];
+    if (!(y0 < y1 && y1 <= pl.res.y && z0 < z1 && z1 <= pl.res.z)) { pl.err = -15; return; }
+    bool left = false, right = false, down = false, up = false;
+    if (y0 == 0 && y1 != pl.res.y) right = true;
+    else if (y1 == pl.res.y && y0 != 0) left = true;
+    else if (y0 != 0 && y1 != pl.res.y) left = right = true;
+    if (z0 == 0 && z1 != pl.res.z) up = true;
+    else if (z1 == pl.res.z && z0 != 0) down = true;
+    else if (z0 != 0 && z1 != pl.res.z) down = up = true;
+    const uint ey0 = y0 - (left ? 1 : 0), ey1 = y1 + (right ? 1 : 0);
+    const uint ez0 = z0 - (down ? 1 : 0), ez1 = z1 + (up ? 1 : 0);
+    pl.mnExt = d3{pl.mn.x + double(0u) * pl.d, pl.mn.y + double(ey0) * pl.d, pl.mn.z + double(ez0) * pl.d};
+    pl.ext = u3{pl.res.x, ey1 - ey0, ez1 - ez0};
+    pl.alloc = u3{pl.res.x, (y1 - y0) + 2, (z1 - z0) + 2};
+    pl.padY = left ? 0 : 1;
+    pl.padZ = down ? 0 : 1;
+    pl.border = left || right || down || up;
 }
 
 // ---------------------------------------------------------------------------
@@ -372,7 +409,8 @@ static void traverseTiles(const TriSetupD& s, d3 mn, double d, const Fma& F, Emi
 // Solid voxelization of one yz subspace, src/host_side.cpp:274-397 with the
 // kernels src/voxelizer.cu:840-1617.
 static void performVoxelization(const float* V, const uint* I, uint nT, d3 mn, double d, Bounds<u3> extRes,
-                                Bounds<u2> yz, uint xRes, uint nX, uint32_t* voxels, u3 alloc, const Fma& F) {
+                                Bounds<u2> yz, uint xRes, uint nX, uint32_t* voxels, u3 alloc, const Fma& F,
+                                uint padY, uint padZ) {
     Bounds<u2> space{u2{yz.min.x - extRes.min.y, yz.min.y - extRes.min.z},
                      u2{yz.max.x - extRes.min.y, yz.max.y - extRes.min.z}};
     u3 resExt{extRes.max.x - extRes.min.x, extRes.max.y - extRes.min.y, extRes.max.z - extRes.min.z};
@@ -431,7 +469,9 @@ static void performVoxelization(const float* V, const uint* I, uint nT, d3 mn, d
     }
     tileStart.push_back(W);
     const uint ipx = alloc.x >> 5;
-    const uint resY2 = resExt.y + 2;  // no neighbouring subspaces: +1 on both sides
+    // Row stride: the allocation (src/voxelizer.cu:1486-1501 grows the
+    // extended box by the padding rows that no neighbour overlaps).
+    const uint resY2 = alloc.y;
     // generateVoxelization, src/voxelizer.cu:1273-1617, once per x subspace.
     for (uint xs = 0; xs < nX; ++xs) {
         Bounds<u3> sub{u3{xs * xRes, yz.min.x, yz.min.y}, u3{(xs + 1) * xRes, yz.max.x, yz.max.y}};
@@ -453,7 +493,7 @@ static void performVoxelization(const float* V, const uint* I, uint nT, d3 mn, d
                 if (!(voxelY >= sp.min.x && voxelY < sp.max.x && voxelZ >= sp.min.y && voxelZ < sp.max.y)) continue;
                 uint32_t bitmask = 0;
                 bool any = false;
-                uint rowBase = resY2 * ipx * (voxelZ + 1) + ipx * (voxelY + 1);
+                uint rowBase = resY2 * ipx * (voxelZ + padZ) + ipx * (voxelY + padY);
                 double px = pcoord(voxelY, d, mn.y, F[ORC_S_P_GEN]), py = pcoord(voxelZ, d, mn.z, F[ORC_S_P_GEN]);
                 for (uint w = tileStart[tl]; w < tileStart[tl + 1]; ++w) {
                     uint tri = wqTri[order[w]];
@@ -619,9 +659,10 @@ static inline float vbComp(int c, float m, float d, int mode) {
 struct SurfaceCtx {
     const float* V; const uint* I; const uchar* M;
     f3 m; float d;
-    u3 res;          // (X, Y+2, Z+2): extResolution size plus the padding
+    u3 res;          // the allocation: extResolution plus the padding rows
     bool fcc; int gridType;
     const Fma* F;
+    int padY, padZ;  // adjustment (1, left ? 0 : 1, down ? 0 : 1), src/voxelizer.cu:3362-3368
 };
 
 static inline uint nodeIndex(const SurfaceCtx& c, int x, int y, int z) {
@@ -688,7 +729,7 @@ static void surfaceTriangle(const SurfaceCtx& c, uint tri, uint code, Bounds<u3>
     Bounds<i3> vb = voxBoundsHalf(bmin, bmax, c.m, c.d);
     if (!adjustRange(vb, sub)) return;
     uint axis = (code >> 28) & 3u;
-    const int ax = 1, ay = 1, az = 1;  // padding adjustment without neighbouring subspaces
+    const int ax = 1, ay = c.padY, az = c.padZ;  // padding adjustment
     if (bb == 1) {
         vb.min = i3{vb.min.x + ax, vb.min.y + ay, vb.min.z + az};
         vb.max = i3{vb.max.x + ax, vb.max.y + ay, vb.max.z + az};
@@ -1026,7 +1067,7 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
     const u3 alloc = pl.alloc;
     const uint nInts = (alloc.x * alloc.y * alloc.z) >> 5;
     std::vector<uint32_t> voxels(nInts, 0u);
-    Bounds<u3> ext{u3{0, 0, 0}, pl.res};
+    Bounds<u3> ext{u3{0, 0, 0}, pl.ext};
     Bounds<u3> allocPart{u3{0, 0, 0}, alloc};
     const u2 vs{p->vox_split[1], p->vox_split[2]};
     std::vector<Bounds<u2> > extYz = splitYZ(vs, ext);
@@ -1034,7 +1075,8 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
     const bool mats = p->materials && p->node_output;
     if (!p->node_output) {
         for (auto& s : extYz)
-            performVoxelization(V, I, nT, pl.mn, pl.d, ext, s, pl.xRes, pl.xSplits, voxels.data(), alloc, F);
+            performVoxelization(V, I, nT, pl.mnExt, pl.d, ext, s, pl.xRes, pl.xSplits, voxels.data(), alloc, F, pl.padY,
+                                pl.padZ);
         memcpy(out, voxels.data(), sizeof(uint32_t) * (size_t)nInts);
         return 0;
     }
@@ -1048,7 +1090,8 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
     std::unordered_map<uint, SurfaceRec> rec;
     if (!fcc) {
         for (auto& s : extYz)
-            performVoxelization(V, I, nT, pl.mn, pl.d, ext, s, pl.xRes, pl.xSplits, voxels.data(), alloc, F);
+            performVoxelization(V, I, nT, pl.mnExt, pl.d, ext, s, pl.xRes, pl.xSplits, voxels.data(), alloc, F, pl.padY,
+                                pl.padZ);
         // constructNodeList2, src/voxelizer.cu:1626-1681 (all alloc splits together)
 #pragma omp parallel for schedule(static)
         for (long long w = 0; w < (long long)nInts; ++w) {
@@ -1061,7 +1104,8 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
             }
         }
         if (mats) {
-            SurfaceCtx c{V, I, M, f3{float(pl.mn.x), float(pl.mn.y), float(pl.mn.z)}, float(pl.d), alloc, false, 1, &F};
+            SurfaceCtx c{V, I, M, f3{float(pl.mnExt.x), float(pl.mnExt.y), float(pl.mnExt.z)}, float(pl.d), alloc,
+                         false, 1, &F, (int)pl.padY, (int)pl.padZ};
             surfacePass(c, nT, matSplits, rec);
         }
     } else {
@@ -1071,7 +1115,7 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
             d3 m{pl.mn.x + sh.x, pl.mn.y + sh.y, pl.mn.z + sh.z};
             std::fill(voxels.begin(), voxels.end(), 0u);
             for (auto& s : extYz)
-                performVoxelization(V, I, nT, m, pl.d, ext, s, pl.xRes, pl.xSplits, voxels.data(), alloc, F);
+                performVoxelization(V, I, nT, m, pl.d, ext, s, pl.xRes, pl.xSplits, voxels.data(), alloc, F, 1, 1);
             // convertToFCCGrid, src/voxelizer.cu:1710-1776
             const uint rx = alloc.x, ry = alloc.y;
 #pragma omp parallel for schedule(static)
@@ -1095,7 +1139,7 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
             for (int g = 1; g <= 4; ++g) {
                 d3 sh = g == 1 ? d3{0, 0, 0} : g == 2 ? d3{h, h, 0} : g == 3 ? d3{0, h, h} : d3{h, 0, h};
                 f3 m{float(pl.mn.x + sh.x), float(pl.mn.y + sh.y), float(pl.mn.z + sh.z)};
-                SurfaceCtx c{V, I, M, m, float(pl.d), alloc, true, g, &F};
+                SurfaceCtx c{V, I, M, m, float(pl.d), alloc, true, g, &F, 1, 1};
                 surfacePass(c, nT, matSplits, rec);
             }
         }
@@ -1104,7 +1148,8 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
     // PartialNode ratio of the winning triangle.  Conflict bits: 1 = the
     // winning class saw more than one material, 2 = more than one triangle.
     uint64_t nConf = 0;
-    const SurfaceCtx rc{V, I, M, f3{float(pl.mn.x), float(pl.mn.y), float(pl.mn.z)}, float(pl.d), alloc, false, 1, &F};
+    const SurfaceCtx rc{V, I, M, f3{float(pl.mnExt.x), float(pl.mnExt.y), float(pl.mnExt.z)}, float(pl.d), alloc,
+                        false, 1, &F, (int)pl.padY, (int)pl.padZ};
     std::vector<std::pair<uint, SurfaceRec> > recs(rec.begin(), rec.end());
 #pragma omp parallel for schedule(dynamic, 256) reduction(+ : nConf)
     for (long long i = 0; i < (long long)recs.size(); ++i) {
@@ -1180,6 +1225,16 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
                     }
         }
         info->prune_passes = passes;
+        // zeroPadding (src/voxelizer.cu:4811-4844) in a device space with
+        // neighbours: every node on a face of the allocation.
+        if (pl.border) {
+#pragma omp parallel for schedule(static)
+            for (long long z = 0; z < (long long)alloc.z; ++z)
+                for (uint y = 0; y < alloc.y; ++y)
+                    for (uint x = 0; x < alloc.x; ++x)
+                        if (x == 0 || x + 1 == alloc.x || y == 0 || y + 1 == alloc.y || z == 0 || z + 1 == alloc.z)
+                            nodes[(size_t)z * npy + (size_t)y * npx + x] = zero;
+        }
     } else {
         // calculateFCCBoundaries, src/voxelizer.cu:1929-2048.  The 12
         // neighbour offsets are symmetric, so the in-place kernel equals a
@@ -1221,11 +1276,13 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
 
 extern "C" int orc_plan(const orc_params* p, const float* verts, uint32_t nV, orc_info* info) {
     Plan pl = makePlan(p, verts, nV);
+    applySpace(p, pl);
     memset(info, 0, sizeof(*info));
     if (pl.err) return pl.err;
     bool fcc = p->node_type == ORC_SHORT_FCC || p->node_type == ORC_LONG_FCC;
     static const uint nb[5] = {1, 2, 8, 2, 4};
     if (p->node_type < 0 || p->node_type > 4) return -13;
+    if (p->space && fcc && p->node_output) return -13;   // device spaces of FCC lattices: not restated
     if (p->node_output) {
         info->dims[0] = fcc ? 2 * pl.alloc.x : pl.alloc.x;
         info->dims[1] = pl.alloc.y;
@@ -1250,6 +1307,7 @@ extern "C" int orc_voxelize(const orc_params* p, const float* verts, uint32_t nV
     if (rc) return rc;
     if (out_bytes < info->out_bytes) return -14;
     Plan pl = makePlan(p, verts, nV);
+    applySpace(p, pl);
 #ifdef _OPENMP
     if (p->threads > 0) omp_set_num_threads(p->threads);
 #endif
@@ -1275,6 +1333,7 @@ extern "C" int orc_voxelize_winners(const orc_params* p, const float* verts, uin
     if (rc) return rc;
     if (out_bytes < info->out_bytes) return -14;
     Plan pl = makePlan(p, verts, nV);
+    applySpace(p, pl);
     return run<PartialN>(p, pl, verts, nV, idx, nT, mats, out, conflict, info, win_tri, win_cls);
 }
 
@@ -1284,7 +1343,7 @@ extern "C" float orc_node_ratio(const orc_params* p, const float* verts, const u
                                 uint32_t cls, int x, int y, int z, const float* min_corner, float d) {
     const Fma F(p->fma_sites);
     const SurfaceCtx c{verts, idx, nullptr, f3{min_corner[0], min_corner[1], min_corner[2]}, d, u3{0, 0, 0},
-                       false, 1, &F};
+                       false, 1, &F, 1, 1};
     bool unstable = false;
     return ratio::nodeRatio(c, tri, cls, x, y, z, unstable);
 }

@@ -59,6 +59,11 @@ typedef struct {
     uint32_t mat_split[3];
     uint8_t fma_sites[48];   /* one mode per ORC_S_* site */
     int threads;          /* OpenMP threads (0 = library default) */
+    /* Device space (src/host_side.cpp:782-1011): space = 1 voxelizes the
+     * yz partition [part[0], part[1]) x [part[2], part[3]) of the grid as
+     * the reference's devices do; 0 = the whole grid. */
+    int space;
+    uint32_t part[4];
 } orc_params;
 
 typedef struct {

@@ -3,8 +3,9 @@
 // against include/vox/voxelizer.h and libvxb.so.  Reads a mesh from a raw
 // file (uint32 nV, nT; float vertices[3nV]; uint32 indices[3nT];
 // uint8 materials[nT]), runs voxelizeToNodesToRAM / voxelizeToRAM / the
-// device-pointer voxelizeToNodes, and writes the results for the Python test
-// to compare with the C ABI.
+// device-pointer voxelizeToNodes, a slice, devConfig partitions and
+// simulateMultidevice, and writes the results for the Python test to compare
+// with the C ABI.
 #include <vox/voxelizer.h>
 
 #include <cstdio>
@@ -48,6 +49,39 @@ int main(int argc, char** argv) {
         cudaFree(dres[0].ptr);
         o = std::fopen((pre + "_nodes_dev.bin").c_str(), "wb");
         std::fwrite(back.data(), sizeof(vox::LongNode), n, o);
+        std::fclose(o);
+
+        // A slice along y (voxelizeSliceToRAM) and devConfig partitions, as
+        // device pointers and, inside simulateMultidevice, host arrays.
+        vox::NodePointer<vox::LongNode> sl = voxelizer.voxelizeSliceToRAM(80u, 1, 20);
+        size_t ns = (size_t)sl.dim.x * sl.dim.y * sl.dim.z;
+        o = std::fopen((pre + "_slice.bin").c_str(), "wb");
+        std::fwrite(&sl.dim, sizeof(sl.dim), 1, o);
+        std::fwrite(sl.ptr, sizeof(vox::LongNode), ns, o);
+        std::fclose(o);
+        delete[] sl.ptr;
+        std::vector<vox::NodePointer<vox::LongNode> > parts = voxelizer.voxelizeToNodes(80u, make_uint2(2, 2));
+        o = std::fopen((pre + "_parts.bin").c_str(), "wb");
+        for (auto& pp : parts) {
+            size_t np = (size_t)pp.dim.x * pp.dim.y * pp.dim.z;
+            std::vector<vox::LongNode> hb(np);
+            cudaMemcpy(hb.data(), pp.ptr, np * sizeof(vox::LongNode), cudaMemcpyDeviceToHost);
+            cudaFree(pp.ptr);
+            std::fwrite(&pp.dim, sizeof(pp.dim), 1, o);
+            std::fwrite(&pp.loc, sizeof(pp.loc), 1, o);
+            std::fwrite(hb.data(), sizeof(vox::LongNode), np, o);
+        }
+        std::fclose(o);
+        std::vector<vox::NodePointer<vox::LongNode> > sim = voxelizer.simulateMultidevice(
+            [&]() { return voxelizer.voxelizeToNodes(80u, make_uint2(2, 1)); });
+        o = std::fopen((pre + "_sim.bin").c_str(), "wb");
+        for (auto& pp : sim) {
+            size_t np = (size_t)pp.dim.x * pp.dim.y * pp.dim.z;
+            std::fwrite(&pp.dim, sizeof(pp.dim), 1, o);
+            std::fwrite(&pp.loc, sizeof(pp.loc), 1, o);
+            std::fwrite(pp.ptr, sizeof(vox::LongNode), np, o);   // host arrays inside simulateMultidevice
+            delete[] pp.ptr;
+        }
         std::fclose(o);
 
         // Plain bit array through a fresh instance (node output off).

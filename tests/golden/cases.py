@@ -83,15 +83,55 @@ def mesh(name):
 
 
 def case(name, mesh, node_type, nodes, materials, size, vox=DEFAULT_VOX, mat=DEFAULT_MAT, store="full",
-         strict_mats=True):
+         strict_mats=True, space=None):
     """``size`` is an int (maxDimension) or a float (cubeLength).
     ``store`` is "full" (array kept) or "digest" (SHA-256 and counts only).
     ``strict_mats`` is False where triangles of different materials touch the
     same voxel, so that the reference's plain-store race (src/voxelizer.cu:2988)
-    makes its material bytes nondeterministic there."""
+    makes its material bytes nondeterministic there.
+    ``space`` voxelizes one device space instead of the whole grid:
+    ("slice", direction, s) the slice s (1-based, padding row 0) along y (1)
+    or z (2); ("part", dev_y, dev_z, k) partition k (y fastest) of devConfig
+    (dev_y, dev_z)."""
     return dict(name=name, mesh=mesh, node_type=node_type, nodes=int(nodes), materials=int(materials),
                 by_cube=isinstance(size, float), size=size, vox=tuple(vox), mat=tuple(mat), store=store,
-                strict_mats=strict_mats)
+                strict_mats=strict_mats, space=tuple(space) if space else None)
+
+
+def split_parts(length, parts):
+    """splitResolutionByNrOfParts along one axis: floor division, the
+    remainder to the first part (src/host_side.cpp:3025-3105)."""
+    out, prev = [None] * parts, length
+    for i in range(parts, 0, -1):
+        lo = prev - prev // i
+        out[i - 1] = (lo, prev)
+        prev = lo
+    return out
+
+
+def partition(c, res_y, res_z):
+    """(y0, y1, z0, z1) of a case's device space for a grid of res_y x res_z
+    voxel rows; None for the whole grid."""
+    sp = c.get("space")
+    if not sp:
+        return None
+    if sp[0] == "slice":
+        _, direction, s = sp
+        n = res_y if direction == 1 else res_z
+        s0 = 0 if (s == 0 or s > n) else s - 1   # sliceOOB voxelizes row 0 (and zeroes the result)
+        return (s0, s0 + 1, 0, res_z) if direction == 1 else (0, res_y, s0, s0 + 1)
+    _, dy, dz, k = sp
+    ys, zs = split_parts(res_y, dy), split_parts(res_z, dz)
+    y, z = k % dy, k // dy
+    return (ys[y][0], ys[y][1], zs[z][0], zs[z][1])
+
+
+def slice_oob(c, res_y, res_z):
+    sp = c.get("space")
+    if not sp or sp[0] != "slice":
+        return False
+    n = res_y if sp[1] == 1 else res_z
+    return sp[2] == 0 or sp[2] > n
 
 
 CASES = [
@@ -134,6 +174,20 @@ CASES = [
     case("ico4_partial_mat", "ico4", PARTIAL, 1, 1, 1.0 / 64.0, strict_mats=False),
     case("torus_partial_mat", "torus", PARTIAL, 1, 1, 96, strict_mats=False),
     case("stress_partial_mat", "stress", PARTIAL, 1, 1, 1.0 / 96.0, mat=(48, 48, 48), strict_mats=False),
+    # Device spaces: slices (voxelizeSlice) and devConfig partitions.
+    case("torus_long_slice_y_mid", "torus", LONG, 1, 1, 120, space=("slice", 1, 50)),
+    case("torus_long_slice_y_first", "torus", LONG, 1, 1, 120, space=("slice", 1, 1)),
+    case("torus_long_slice_y_last", "torus", LONG, 1, 1, 120, space=("slice", 1, 120)),
+    case("torus_short_slice_z_mid", "torus", SHORT, 1, 1, 120, space=("slice", 2, 20)),
+    case("ico3_long_slice_z_splits", "ico3_mixed", LONG, 1, 1, 90, vox=(64, 16, 16), mat=(16, 16, 16),
+         strict_mats=False, space=("slice", 2, 40)),
+    case("torus_long_slice_oob", "torus", LONG, 1, 1, 120, space=("slice", 1, 0)),
+    case("room_lite_long_part22_0", "room_lite", LONG, 1, 1, 160, space=("part", 2, 2, 0)),
+    case("room_lite_long_part22_1", "room_lite", LONG, 1, 1, 160, space=("part", 2, 2, 1)),
+    case("room_lite_long_part22_2", "room_lite", LONG, 1, 1, 160, space=("part", 2, 2, 2)),
+    case("room_lite_long_part22_3", "room_lite", LONG, 1, 1, 160, space=("part", 2, 2, 3)),
+    case("ico4_partial_part31_1", "ico4", PARTIAL, 1, 1, 1.0 / 64.0, strict_mats=False, space=("part", 3, 1, 1)),
+    case("room_lite_bits_part13_1", "room_lite", LONG, 0, 0, 160, space=("part", 1, 3, 1)),
 ]
 
 BY_NAME = {c["name"]: c for c in CASES}

@@ -36,13 +36,15 @@ import cases as C  # noqa: E402
 
 
 def load_ref():
+    """ref_voxelize_space of oracle/_ref/libvoxref.so: the reference's kernels
+    over the whole grid (part NULL) or one device space."""
     lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libvoxref.so"))
-    f = lib.ref_voxelize
+    f = lib.ref_voxelize_space
     f.restype = ctypes.c_int
     f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_double,
                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
-                  ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint64,
-                  ctypes.c_void_p, ctypes.c_void_p]
+                  ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                  ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]
     lib.ref_last_error.restype = ctypes.c_char_p
     f.last_error = lambda: lib.ref_last_error().decode()
     return f
@@ -102,9 +104,18 @@ def run_case(f, c):
     args = [c["node_type"], c["nodes"], c["materials"], int(c["by_cube"]), md, cl, vs, ms,
             m.vertices.ctypes.data, m.n_vertices, m.indices.ctypes.data, m.n_triangles,
             mats.ctypes.data, m.n_materials]
-    rc = f(*args, None, 0, dims, None)
+    rc = f(*args, None, None, 0, dims, None)
     if rc != 0:
         raise RuntimeError(f"{c['name']}: plan failed rc={rc}")
+    part, oob = None, False
+    if c.get("space"):
+        res_y, res_z = int(dims[1]) - 2, int(dims[2]) - 2
+        part = (ctypes.c_uint32 * 4)(*C.partition(c, res_y, res_z))
+        oob = C.slice_oob(c, res_y, res_z)
+        rc = f(*args, part, None, 0, dims, None)
+        if rc != 0:
+            raise RuntimeError(f"{c['name']}: plan failed rc={rc}")
+    args.append(part)
     dt = C.out_dtype(c)
     n = int(dims[0]) * int(dims[1]) * int(dims[2])
     count = n // 32 if not c["nodes"] else n
@@ -117,6 +128,8 @@ def run_case(f, c):
         pm = padding_mask(c)
         if pm is not None:
             out &= pm
+        if oob:   # sliceOOB: the reference zeroes the slice array (src/host_side.cpp:1225-1236)
+            out[:] = 0
         outs.append(out)
         times.append(elapsed.value)
     return m, (int(dims[0]), int(dims[1]), int(dims[2])), outs, times

@@ -40,6 +40,26 @@ def test_cpp_front_end(tmp_path):
     assert dims == info.dims
     assert np.array_equal(nodes, want)
     assert np.array_equal(np.fromfile(tmp_path / "r_nodes_dev.bin", np.uint16), want)
+    with Voxelizer(v, f, mats, 8, node_type=LONG) as vx:
+        wslice, sinfo = vx.voxelizeSliceToRAM(80, 1, 20)
+        wparts = vx.voxelizePartsToRAM(1, 80, (2, 2))
+        wsim = vx.voxelizePartsToRAM(1, 80, (2, 1))
+    raw = open(tmp_path / "r_slice.bin", "rb").read()
+    assert tuple(np.frombuffer(raw[:12], np.uint32)) == sinfo.dims
+    assert np.array_equal(np.frombuffer(raw[12:], np.uint16), wslice)
+    for fname, want_parts in (("r_parts.bin", wparts), ("r_sim.bin", wsim)):
+        raw = open(tmp_path / fname, "rb").read()
+        pos = 0
+        for want_arr, want_info in want_parts:
+            dims = tuple(np.frombuffer(raw[pos:pos + 12], np.uint32))
+            loc = tuple(np.frombuffer(raw[pos + 12:pos + 24], np.uint32))
+            pos += 24
+            assert dims == want_info.dims
+            assert loc == (want_info.location.x, want_info.location.y, want_info.location.z)
+            n = dims[0] * dims[1] * dims[2]
+            assert np.array_equal(np.frombuffer(raw[pos:pos + 2 * n], np.uint16), want_arr)
+            pos += 2 * n
+        assert pos == len(raw)
     raw = open(tmp_path / "r_bits.bin", "rb").read()
     with Voxelizer(v, f, node_type=SHORT) as vx:
         wbits, binfo = vx.voxelizeToRAM(80)

@@ -41,10 +41,21 @@ RAN = sorted(n for n, e in INDEX.items() if "ref_error" not in e)
 def test_plan_matches_golden_dims(name):
     c = C.BY_NAME[name]
     m = C.mesh(c["mesh"])
+    sp = c.get("space")
     with Voxelizer(m.vertices, m.indices, node_type=c["node_type"]) as v:
-        info = v.plan(c["nodes"], c["size"], c["vox"], c["mat"])
+        full = v.plan(c["nodes"], c["size"], c["vox"], c["mat"])
+        if sp and sp[0] == "slice":
+            info = v.planSlice(c["size"], sp[1], sp[2], c["vox"], c["mat"])
+        elif sp:
+            info = v.planParts(c["nodes"], c["size"], (sp[1], sp[2]), c["vox"], c["mat"])[sp[3]]
+            assert (info.location.y, info.location.z) == (sp[3] % sp[1], sp[3] // sp[1])
+        else:
+            info = full
     assert info.dims == tuple(INDEX[name]["dims"])
-    oi = O.plan(m, c["node_type"], c["nodes"], c["size"], c["vox"])
+    part = C.partition(c, int(full.resolution.y), int(full.resolution.z))
+    if part:
+        assert tuple(info.partition) == part
+    oi = O.plan(m, c["node_type"], c["nodes"], c["size"], c["vox"], part=part)
     assert info.dims == tuple(oi.dims)
     assert info.voxel_length == oi.voxel_length
     assert info.x_splits == oi.x_splits

@@ -25,7 +25,9 @@ EXPORTS = ["vxb_last_error", "vxb_version", "vxb_create", "vxb_destroy", "vxb_se
            "vxb_set_material_output", "vxb_verbose_output", "vxb_plan", "vxb_get_array_dimensions",
            "vxb_voxelize_to_host", "vxb_voxelize_to_device", "vxb_last_launch_count", "vxb_set_profiling",
            "vxb_stage_times", "vxb_voxelize_bits_noalloc", "vxb_trim_cache", "vxb_batch_create",
-           "vxb_batch_destroy", "vxb_batch_add", "vxb_batch_clear", "vxb_batch_run", "vxb_batch_last_launch_count", "vxb_last_stats"]
+           "vxb_batch_destroy", "vxb_batch_add", "vxb_batch_clear", "vxb_batch_run", "vxb_batch_last_launch_count",
+           "vxb_last_stats", "vxb_plan_parts", "vxb_voxelize_parts_to_device", "vxb_voxelize_parts_to_host",
+           "vxb_plan_slice", "vxb_voxelize_slice_to_device", "vxb_voxelize_slice_to_host"]
 
 BATCH_GRAPH = 1
 
@@ -48,7 +50,8 @@ class Request(ctypes.Structure):
 class GridInfo(ctypes.Structure):
     _fields_ = [("dim", Uint3), ("bytes", ctypes.c_uint64), ("count", ctypes.c_uint64),
                 ("voxel_length", ctypes.c_double), ("min_vertex", ctypes.c_double * 3),
-                ("max_vertex", ctypes.c_double * 3), ("resolution", Uint3), ("x_splits", ctypes.c_uint32)]
+                ("max_vertex", ctypes.c_double * 3), ("resolution", Uint3), ("x_splits", ctypes.c_uint32),
+                ("location", Uint3), ("partition", ctypes.c_uint32 * 4)]
 
     @property
     def dims(self):
@@ -104,6 +107,18 @@ def lib():
         "vxb_last_launch_count": (ctypes.c_int, [vp, P(ctypes.c_uint32)]),
         "vxb_set_profiling": (ctypes.c_int, [vp, ctypes.c_int]),
         "vxb_stage_times": (ctypes.c_int, [vp, P(ctypes.c_float), ctypes.c_uint32]),
+        "vxb_plan_parts": (ctypes.c_int, [vp, ctypes.c_int, P(Request), ctypes.c_uint32, ctypes.c_uint32,
+                                          P(GridInfo)]),
+        "vxb_voxelize_parts_to_device": (ctypes.c_int, [vp, ctypes.c_int, P(Request), ctypes.c_uint32,
+                                                        ctypes.c_uint32, P(vp), P(ctypes.c_uint64), vp,
+                                                        P(GridInfo)]),
+        "vxb_voxelize_parts_to_host": (ctypes.c_int, [vp, ctypes.c_int, P(Request), ctypes.c_uint32,
+                                                      ctypes.c_uint32, P(vp), P(ctypes.c_uint64), P(GridInfo)]),
+        "vxb_plan_slice": (ctypes.c_int, [vp, P(Request), ctypes.c_int, ctypes.c_uint32, P(GridInfo)]),
+        "vxb_voxelize_slice_to_device": (ctypes.c_int, [vp, P(Request), ctypes.c_int, ctypes.c_uint32, vp,
+                                                        ctypes.c_uint64, vp, P(GridInfo)]),
+        "vxb_voxelize_slice_to_host": (ctypes.c_int, [vp, P(Request), ctypes.c_int, ctypes.c_uint32, vp,
+                                                      ctypes.c_uint64, P(GridInfo)]),
         "vxb_voxelize_bits_noalloc": (ctypes.c_int, [vp, vp, ctypes.c_uint32, ctypes.c_uint32, P(ctypes.c_double),
                                                      P(ctypes.c_double), P(Request), vp, ctypes.c_uint64, vp,
                                                      P(GridInfo)]),

@@ -122,6 +122,69 @@ class Voxelizer:
                                            nbytes, ctypes.c_void_p(stream or 0), ctypes.byref(info)))
         return info
 
+    # -- slices (voxelizeSlice / voxelizeSliceToRAM, include/voxelizer.h:765-795) --
+    @staticmethod
+    def _slice_request(size, voxSplitRes, matSplitRes):
+        # The reference's slice members take uint2 split sizes (a, b) and use
+        # (a, b, b) (src/host_side.cpp:1966-1972).
+        vs = tuple(voxSplitRes) if len(voxSplitRes) == 3 else (voxSplitRes[0], voxSplitRes[1], voxSplitRes[1])
+        ms = tuple(matSplitRes) if len(matSplitRes) == 3 else (matSplitRes[0], matSplitRes[1], matSplitRes[1])
+        return make_request(size, vs, ms)
+
+    def planSlice(self, size, direction, slice, voxSplitRes=(1024, 512), matSplitRes=(512, 512)):
+        info = _lib.GridInfo()
+        r = self._slice_request(size, voxSplitRes, matSplitRes)
+        check(lib().vxb_plan_slice(self._h, ctypes.byref(r), int(direction), int(slice), ctypes.byref(info)))
+        return info
+
+    def voxelizeSliceToRAM(self, size, direction, slice, voxSplitRes=(1024, 512), matSplitRes=(512, 512), out=None):
+        """Node array of slice ``slice`` (1 .. resolution, counting the
+        padding row as 0) along ``direction`` (1: y, 2: z): three layers along
+        that axis, the middle one the slice.  Returns (array, GridInfo)."""
+        info = self.planSlice(size, direction, slice, voxSplitRes, matSplitRes)
+        if out is None:
+            out = np.empty(int(info.count), dtype=NODE_DTYPE[self.node_type])
+        elif out.nbytes < info.bytes:
+            raise ValueError("output buffer too small")
+        r = self._slice_request(size, voxSplitRes, matSplitRes)
+        check(lib().vxb_voxelize_slice_to_host(self._h, ctypes.byref(r), int(direction), int(slice),
+                                               out.ctypes.data, out.nbytes, ctypes.byref(info)))
+        return out, info
+
+    def voxelize_slice_device(self, size, direction, slice, out, voxSplitRes=(1024, 512), matSplitRes=(512, 512),
+                              stream=None):
+        info = _lib.GridInfo()
+        r = self._slice_request(size, voxSplitRes, matSplitRes)
+        nbytes = out.numel() * out.element_size() if hasattr(out, "element_size") else int(out.nbytes)
+        check(lib().vxb_voxelize_slice_to_device(self._h, ctypes.byref(r), int(direction), int(slice),
+                                                 ctypes.c_void_p(out.data_ptr()), nbytes,
+                                                 ctypes.c_void_p(stream or 0), ctypes.byref(info)))
+        return info
+
+    # -- devConfig partitions (voxelize(..., devConfig, ...), include/voxelizer.h:718-770) --
+    def planParts(self, nodes, size, devConfig, voxSplitRes=DEFAULT_VOX, matSplitRes=DEFAULT_MAT):
+        dy, dz = (int(v) for v in devConfig)
+        infos = (_lib.GridInfo * (dy * dz))()
+        r = make_request(size, voxSplitRes, matSplitRes)
+        check(lib().vxb_plan_parts(self._h, int(bool(nodes)), ctypes.byref(r), dy, dz, infos))
+        return list(infos)
+
+    def voxelizePartsToRAM(self, nodes, size, devConfig, voxSplitRes=DEFAULT_VOX, matSplitRes=DEFAULT_MAT):
+        """One result per partition of the yz voxel range (devConfig (dev_y,
+        dev_z), y fastest), each voxelized as the reference's devices do.
+        Returns a list of (array, GridInfo); GridInfo.location is the
+        partition's (0, y, z)."""
+        dy, dz = (int(v) for v in devConfig)
+        infos = self.planParts(nodes, size, devConfig, voxSplitRes, matSplitRes)
+        dt = NODE_DTYPE[self.node_type] if nodes else np.uint32
+        outs = [np.empty(int(i.count), dtype=dt) for i in infos]
+        ptrs = (ctypes.c_void_p * len(outs))(*[o.ctypes.data for o in outs])
+        sizes = (ctypes.c_uint64 * len(outs))(*[o.nbytes for o in outs])
+        arr = (_lib.GridInfo * len(outs))()
+        r = make_request(size, voxSplitRes, matSplitRes)
+        check(lib().vxb_voxelize_parts_to_host(self._h, int(bool(nodes)), ctypes.byref(r), dy, dz, ptrs, sizes, arr))
+        return list(zip(outs, list(arr)))
+
     def set_profiling(self, enable):
         check(lib().vxb_set_profiling(self._h, int(bool(enable))))
 

@@ -130,9 +130,9 @@ std::vector<NodePointer<Node> > Voxelizer<Node>::voxelize(uint maxDimension, uin
         std::cout << "Please use a standard Node-type when producing a plain voxelization.\n";
         return result;
     }
-    if (devConfig.x * devConfig.y != 1) throw Exception("Only one device is supported (devConfig must be (1, 1)).");
     nodeOutput = false;
     maxDimensionSetting = maxDimension;
+    if (devConfig.x * devConfig.y != 1 || simulate) return runParts(devConfig, voxSplitRes, make_uint3(512, 512, 512));
     result.push_back(run(false, voxSplitRes, make_uint3(512, 512, 512)));
     return result;
 }
@@ -144,10 +144,10 @@ std::vector<NodePointer<Node> > Voxelizer<Node>::voxelize(double cubeLength, uin
         std::cout << "Please use a standard Node-type when producing a plain voxelization.\n";
         return result;
     }
-    if (devConfig.x * devConfig.y != 1) throw Exception("Only one device is supported (devConfig must be (1, 1)).");
     nodeOutput = false;
     voxelDistanceGiven = true;
     voxelLength = cubeLength;
+    if (devConfig.x * devConfig.y != 1 || simulate) return runParts(devConfig, voxSplitRes, make_uint3(512, 512, 512));
     result.push_back(run(false, voxSplitRes, make_uint3(512, 512, 512)));
     return result;
 }
@@ -182,8 +182,8 @@ std::vector<NodePointer<Node> > Voxelizer<Node>::voxelizeToNodes(uint maxDimensi
         std::cout << "FCC Nodes can currently only be defined through the side length of their cubic cells";
         return result;
     }
-    if (devConfig.x * devConfig.y != 1) throw Exception("Only one device is supported (devConfig must be (1, 1)).");
     maxDimensionSetting = maxDimension;
+    if (devConfig.x * devConfig.y != 1 || simulate) return runParts(devConfig, voxSplitRes, matSplitRes);
     result.push_back(run(false, voxSplitRes, matSplitRes));
     return result;
 }
@@ -192,10 +192,10 @@ template <class Node>
 std::vector<NodePointer<Node> > Voxelizer<Node>::voxelizeToNodes(double cubeLength, uint2 devConfig,
                                                                  uint3 voxSplitRes, uint3 matSplitRes) {
     std::vector<NodePointer<Node> > result;
-    if (devConfig.x * devConfig.y != 1) throw Exception("Only one device is supported (devConfig must be (1, 1)).");
     nodeOutput = true;
     voxelDistanceGiven = true;
     voxelLength = cubeLength;
+    if (devConfig.x * devConfig.y != 1 || simulate) return runParts(devConfig, voxSplitRes, matSplitRes);
     result.push_back(run(false, voxSplitRes, matSplitRes));
     return result;
 }
@@ -219,21 +219,164 @@ NodePointer<Node> Voxelizer<Node>::voxelizeToNodesToRAM(double cubeLength, uint3
     return run(true, voxSplitRes, matSplitRes);
 }
 
+// The reference's slice members take uint2 split sizes (a, b) and use
+// (a, b, b) (src/host_side.cpp:1966-1972).
 template <class Node>
-std::vector<NodePointer<Node> > Voxelizer<Node>::voxelizeSlice(uint, int, uint, uint, uint2, uint2) {
-    throw Exception("voxelizeSlice is not provided by this library");
+vxb_request Voxelizer<Node>::request(uint3 voxSplitRes, uint3 matSplitRes) const {
+    vxb_request r;
+    r.by_cube_length = voxelDistanceGiven ? 1 : 0;
+    r.max_dimension = maxDimensionSetting;
+    r.cube_length = voxelLength;
+    r.vox_split_res = u3(voxSplitRes);
+    r.mat_split_res = u3(matSplitRes);
+    return r;
 }
+
+// Partitions of devConfig, each voxelized as the reference voxelizes it on
+// its own device (vxb_voxelize_parts_*).  All run on this voxelizer's GPU;
+// the results are device pointers there, or host arrays (new[]) inside
+// simulateMultidevice, whose collectData uploads to the host
+// (src/host_side.cpp:3535-3543).
 template <class Node>
-std::vector<NodePointer<Node> > Voxelizer<Node>::voxelizeSlice(double, int, uint, uint, uint2, uint2) {
-    throw Exception("voxelizeSlice is not provided by this library");
+std::vector<NodePointer<Node> > Voxelizer<Node>::runParts(uint2 devConfig, uint3 voxSplitRes, uint3 matSplitRes) {
+    const vxb_request r = request(voxSplitRes, matSplitRes);
+    const int nodes = nodeOutput ? 1 : 0;
+    const uint n = devConfig.x * devConfig.y;
+    if (n == 0) throw Exception("devConfig needs at least one device along each axis");
+    std::vector<vxb_grid_info> gi(n);
+    check(vxb_plan_parts(handle, nodes, &r, devConfig.x, devConfig.y, gi.data()));
+    std::vector<void*> bufs(n, nullptr);
+    std::vector<uint64_t> bytes(n);
+    const bool host = simulate;
+    int device = 0;
+    cudaGetDevice(&device);
+    auto release = [&]() {
+        for (uint i = 0; i < n; ++i) {
+            if (!bufs[i]) continue;
+            if (!host) cudaFree(bufs[i]);
+            else if (nodes) delete[] static_cast<Node*>(bufs[i]);
+            else delete[] static_cast<VoxInt*>(bufs[i]);
+        }
+    };
+    for (uint i = 0; i < n; ++i) {
+        bytes[i] = gi[i].bytes;
+        if (host) {
+            bufs[i] = nodes ? static_cast<void*>(new Node[gi[i].count]) : static_cast<void*>(new VoxInt[gi[i].count]);
+        } else if (cudaMalloc(&bufs[i], gi[i].bytes) != cudaSuccess) {
+            cudaGetLastError();
+            bufs[i] = nullptr;
+            release();
+            throw Exception("cudaMalloc of a partition result failed");
+        }
+    }
+    vxb_status rc = host ? vxb_voxelize_parts_to_host(handle, nodes, &r, devConfig.x, devConfig.y, bufs.data(),
+                                                      bytes.data(), gi.data())
+                         : vxb_voxelize_parts_to_device(handle, nodes, &r, devConfig.x, devConfig.y, bufs.data(),
+                                                        bytes.data(), nullptr, gi.data());
+    if (rc != VXB_OK) {
+        release();
+        check(rc);
+    }
+    std::vector<NodePointer<Node> > result(n);
+    for (uint i = 0; i < n; ++i) {
+        NodePointer<Node>& np = result[i];
+        if (nodes) np.ptr = static_cast<Node*>(bufs[i]);
+        else np.vptr = static_cast<VoxInt*>(bufs[i]);
+        np.dev = device;
+        np.dim = make_uint3(gi[i].dim.x, gi[i].dim.y, gi[i].dim.z);
+        np.loc = make_uint3(gi[i].location.x, gi[i].location.y, gi[i].location.z);
+    }
+    voxelLength = gi[0].voxel_length;
+    resolution = make_uint3(gi[0].resolution.x, gi[0].resolution.y, gi[0].resolution.z);
+    return result;
 }
+
+// One slice (vxb_voxelize_slice_*): node output, a device pointer or, with
+// toHost (or inside simulateMultidevice), a host array.
 template <class Node>
-NodePointer<Node> Voxelizer<Node>::voxelizeSliceToRAM(uint, int, uint, uint2, uint2) {
-    throw Exception("voxelizeSliceToRAM is not provided by this library");
+NodePointer<Node> Voxelizer<Node>::runSlice(bool toHost, int direction, uint slice, uint2 voxSplitRes,
+                                            uint2 matSplitRes) {
+    nodeOutput = true;   // the slice members set nodeOutput (src/host_side.cpp:1946)
+    const vxb_request r = request(make_uint3(voxSplitRes.x, voxSplitRes.y, voxSplitRes.y),
+                                  make_uint3(matSplitRes.x, matSplitRes.y, matSplitRes.y));
+    vxb_grid_info gi;
+    check(vxb_plan_slice(handle, &r, direction, slice, &gi));
+    NodePointer<Node> res = NodePointer<Node>();
+    int device = 0;
+    cudaGetDevice(&device);
+    res.dev = device;
+    res.loc = make_uint3(0, 0, 0);
+    res.dim = make_uint3(gi.dim.x, gi.dim.y, gi.dim.z);
+    if (toHost || simulate) {
+        Node* host = new Node[gi.count];
+        vxb_status rc = vxb_voxelize_slice_to_host(handle, &r, direction, slice, host, gi.bytes, &gi);
+        if (rc != VXB_OK) {
+            delete[] host;
+            check(rc);
+        }
+        res.ptr = host;
+    } else {
+        void* dev = nullptr;
+        if (cudaMalloc(&dev, gi.bytes) != cudaSuccess) {
+            cudaGetLastError();
+            throw Exception("cudaMalloc of the result failed");
+        }
+        vxb_status rc = vxb_voxelize_slice_to_device(handle, &r, direction, slice, dev, gi.bytes, nullptr, &gi);
+        if (rc != VXB_OK) {
+            cudaFree(dev);
+            check(rc);
+        }
+        res.ptr = static_cast<Node*>(dev);
+    }
+    voxelLength = gi.voxel_length;
+    resolution = make_uint3(gi.resolution.x, gi.resolution.y, gi.resolution.z);
+    return res;
 }
+
 template <class Node>
-NodePointer<Node> Voxelizer<Node>::voxelizeSliceToRAM(double, int, uint, uint2, uint2) {
-    throw Exception("voxelizeSliceToRAM is not provided by this library");
+std::vector<NodePointer<Node> > Voxelizer<Node>::voxelizeSlice(uint maxDimension, int direction, uint slice,
+                                                               uint devConfig, uint2 voxSplitRes,
+                                                               uint2 matSplitRes) {
+    std::vector<NodePointer<Node> > result;
+    if (Node::isFCCNode()) {
+        std::cout << "FCC Nodes can currently only be defined through the length of their cubic cells";
+        return result;
+    }
+    if (devConfig != 1) throw Exception("slices are voxelized on one device (devConfig 1)");
+    maxDimensionSetting = maxDimension;
+    result.push_back(runSlice(false, direction, slice, voxSplitRes, matSplitRes));
+    return result;
+}
+
+template <class Node>
+std::vector<NodePointer<Node> > Voxelizer<Node>::voxelizeSlice(double cubeLength, int direction, uint slice,
+                                                               uint devConfig, uint2 voxSplitRes,
+                                                               uint2 matSplitRes) {
+    std::vector<NodePointer<Node> > result;
+    if (devConfig != 1) throw Exception("slices are voxelized on one device (devConfig 1)");
+    voxelDistanceGiven = true;
+    voxelLength = cubeLength;
+    result.push_back(runSlice(false, direction, slice, voxSplitRes, matSplitRes));
+    return result;
+}
+
+template <class Node>
+NodePointer<Node> Voxelizer<Node>::voxelizeSliceToRAM(uint maxDimension, int direction, uint slice, uint2 voxSplitRes,
+                                                      uint2 matSplitRes) {
+    if (Node::isFCCNode()) {
+        std::cout << "FCC Nodes can currently only be defined through the length of their cubic cells";
+        return NodePointer<Node>();
+    }
+    maxDimensionSetting = maxDimension;
+    return runSlice(true, direction, slice, voxSplitRes, matSplitRes);
+}
+
+template <class Node>
+NodePointer<Node> Voxelizer<Node>::voxelizeSliceToRAM(double cubeLength, int direction, uint slice,
+                                                      uint2 voxSplitRes, uint2 matSplitRes) {
+    voxelDistanceGiven = true;
+    voxelLength = cubeLength;
+    return runSlice(true, direction, slice, voxSplitRes, matSplitRes);
 }
 
 template <class Node>
@@ -251,10 +394,20 @@ uint3 Voxelizer<Node>::getArrayDimensions(double cubeLength, uint maxInternalXSi
     return make_uint3(d.x, d.y, d.z);
 }
 
+// simulateMultidevice (src/host_side.cpp): runs `func` with every partition
+// on one device and host results.
 template <class Node>
 std::vector<NodePointer<Node> > Voxelizer<Node>::simulateMultidevice(
-    std::function<std::vector<NodePointer<Node> >()>) {
-    throw Exception("simulateMultidevice is not provided by this library (single device only)");
+    std::function<std::vector<NodePointer<Node> >()> func) {
+    simulate = true;
+    try {
+        std::vector<NodePointer<Node> > result = func();
+        simulate = false;
+        return result;
+    } catch (...) {
+        simulate = false;
+        throw;
+    }
 }
 
 template class Voxelizer<ShortNode>;

@@ -54,6 +54,8 @@ struct vxb_voxelizer {
     bool busy = false;
 
     int plan(int nodes, const vxb_request* r, vxb::Plan& p, vxb_grid_info* info) const;
+    // The request's plan of the whole grid, without the output size checks.
+    int fullPlan(const vxb_request* r, vxb::Plan& p) const;
     // Combinations the reference refuses (src/host_side.cpp:568-573,
     // 1744-1749, 1836-1841, 2280-2285) and missing materials.
     int validate(int nodes, const vxb_request* r) const {
@@ -73,9 +75,25 @@ struct vxb_voxelizer {
     bool uploadMaterials(const uint8_t* mats);
     void job(int nodes, const vxb_request* r, void* dout, uint64_t bytes, vxb::MeshJob* j) const;
     int run(int nodes, const vxb_request* r, void* dout, uint64_t bytes, cudaStream_t s, vxb_grid_info* info);
+    // Device spaces (partitions of the yz voxel range, voxelized as the
+    // reference's devices do) of one request: plans and runs them all as one
+    // batch.
+    struct Space {
+        uint32_t part[4];
+        vxb_uint3 loc;
+    };
+    int planSpaces(int nodes, const vxb_request* r, const std::vector<Space>& sp, vxb_grid_info* infos) const;
+    int runSpaces(int nodes, const vxb_request* r, const std::vector<Space>& sp, void* const* outs,
+                  const uint64_t* bytes, cudaStream_t s, vxb_grid_info* infos);
+    // The partitions of devConfig (dev_y, dev_z) (splitResolutionByNrOfParts,
+    // src/host_side.cpp:782-813), y fastest.
+    int partitions(const vxb_request* r, uint32_t devY, uint32_t devZ, std::vector<Space>* sp) const;
+    // The device space of a slice (src/host_side.cpp:748-779): *oob for a
+    // slice 0 or past the grid, whose result is all zeros.
+    int sliceSpace(const vxb_request* r, int direction, uint32_t slice, Space* sp, bool* oob) const;
 };
 
-int vxb_voxelizer::plan(int nodes, const vxb_request* r, vxb::Plan& p, vxb_grid_info* info) const {
+int vxb_voxelizer::fullPlan(const vxb_request* r, vxb::Plan& p) const {
     if (!r) return failf(VXB_EINVAL, "request is NULL");
     if (nV == 0 || nT == 0) return failf(VXB_EINVAL, "empty mesh");
     const uint32_t vs[3] = {r->vox_split_res.x, r->vox_split_res.y, r->vox_split_res.z};
@@ -83,6 +101,12 @@ int vxb_voxelizer::plan(int nodes, const vxb_request* r, vxb::Plan& p, vxb_grid_
     if (vxb::makePlan(mn, mx, r->by_cube_length, r->max_dimension, r->cube_length, vs, ms, p))
         return failf(VXB_EINVAL, "invalid request (maxDimension >= 2 or cubeLength > 0, split sizes > 0 and an x "
                                  "pass of at most 1024 voxels are required)");
+    return 0;
+}
+
+int vxb_voxelizer::plan(int nodes, const vxb_request* r, vxb::Plan& p, vxb_grid_info* info) const {
+    int rc = fullPlan(r, p);
+    if (rc) return rc;
     return vxb::gridInfo(p, nodeType, nodes, info);
 }
 
@@ -195,6 +219,97 @@ int vxb_voxelizer::run(int nodes, const vxb_request* r, void* dout, uint64_t byt
     launches = pipe.launches;
     if (rc == 0) busy = false;
     return rc;
+}
+
+int vxb_voxelizer::planSpaces(int nodes, const vxb_request* r, const std::vector<Space>& sp,
+                              vxb_grid_info* infos) const {
+    vxb::Plan full;
+    int rc = fullPlan(r, full);
+    if (rc) return rc;
+    if (isFcc(nodeType)) return failf(VXB_EUNSUPPORTED, "device spaces of FCC lattices are not supported");
+    const uint32_t vs[3] = {r->vox_split_res.x, r->vox_split_res.y, r->vox_split_res.z};
+    const uint32_t ms[3] = {r->mat_split_res.x, r->mat_split_res.y, r->mat_split_res.z};
+    for (size_t i = 0; i < sp.size(); ++i) {
+        vxb::Plan q;
+        if (vxb::devicePlan(full, sp[i].part[0], sp[i].part[1], sp[i].part[2], sp[i].part[3], vs, ms, q))
+            return failf(VXB_EINVAL, "partition %zu is empty or outside the grid", i);
+        if ((rc = vxb::gridInfo(q, nodeType, nodes, infos + i))) return rc;
+        infos[i].location = sp[i].loc;
+    }
+    return 0;
+}
+
+int vxb_voxelizer::runSpaces(int nodes, const vxb_request* r, const std::vector<Space>& sp, void* const* outs,
+                             const uint64_t* bytes, cudaStream_t s, vxb_grid_info* infos) {
+    std::vector<vxb_grid_info> gi(sp.size());
+    int rc = planSpaces(nodes, r, sp, gi.data());
+    if (rc) return rc;
+    for (size_t i = 0; i < sp.size(); ++i) {
+        if (infos) infos[i] = gi[i];
+        if (!outs || !outs[i]) return failf(VXB_EINVAL, "output buffer %zu is NULL", i);
+        if (!bytes || bytes[i] < gi[i].bytes)
+            return failf(VXB_EINVAL, "output buffer %zu holds too few bytes (%llu needed)", i,
+                         (unsigned long long)gi[i].bytes);
+    }
+    if ((rc = validate(nodes, r))) return rc;
+    VXB_CUDA(cudaSetDevice(device));
+    launches = 0;
+    timer.reset();
+    busy = true;
+    if ((rc = upload(s))) return rc;
+    std::vector<vxb::MeshJob> jobs(sp.size());
+    for (size_t i = 0; i < sp.size(); ++i) {
+        job(nodes, r, outs[i], bytes[i], &jobs[i]);
+        jobs[i].space = 1;
+        for (int k = 0; k < 4; ++k) jobs[i].part[k] = sp[i].part[k];
+    }
+    if ((rc = pipe.prepare(jobs, s))) return rc;
+    if ((rc = pipe.enqueue(s, &timer))) return rc;
+    rc = pipe.finish(s);
+    launches = pipe.launches;
+    if (rc == 0) busy = false;
+    return rc;
+}
+
+int vxb_voxelizer::partitions(const vxb_request* r, uint32_t devY, uint32_t devZ, std::vector<Space>* sp) const {
+    if (devY == 0 || devZ == 0) return failf(VXB_EINVAL, "devConfig needs at least one partition per axis");
+    vxb::Plan full;
+    int rc = fullPlan(r, full);
+    if (rc) return rc;
+    const std::vector<vxb::Range> ys = vxb::splitParts(full.res[1], devY), zs = vxb::splitParts(full.res[2], devZ);
+    sp->clear();
+    for (uint32_t z = 0; z < devZ; ++z)
+        for (uint32_t y = 0; y < devY; ++y) {
+            Space q;
+            q.part[0] = ys[y].lo;
+            q.part[1] = ys[y].hi;
+            q.part[2] = zs[z].lo;
+            q.part[3] = zs[z].hi;
+            q.loc = vxb_uint3{0, y, z};
+            if (q.part[0] == q.part[1] || q.part[2] == q.part[3])
+                return failf(VXB_EINVAL, "devConfig (%u, %u) leaves an empty partition", devY, devZ);
+            sp->push_back(q);
+        }
+    return 0;
+}
+
+int vxb_voxelizer::sliceSpace(const vxb_request* r, int direction, uint32_t slice, Space* sp, bool* oob) const {
+    if (direction == 0)
+        return failf(VXB_EUNSUPPORTED, "slicing along x is not supported; rotate the model and slice along y or z");
+    if (direction != 1 && direction != 2) return failf(VXB_EINVAL, "slice direction must be 0, 1 or 2");
+    vxb::Plan full;
+    int rc = fullPlan(r, full);
+    if (rc) return rc;
+    const uint32_t len = direction == 1 ? full.res[1] : full.res[2];
+    *oob = slice == 0 || slice > len;
+    const uint32_t s0 = *oob ? 0u : slice - 1;   // slices count the padding row
+    sp->loc = vxb_uint3{0, 0, 0};
+    if (direction == 1) {
+        sp->part[0] = s0; sp->part[1] = s0 + 1; sp->part[2] = 0; sp->part[3] = full.res[2];
+    } else {
+        sp->part[0] = 0; sp->part[1] = full.res[1]; sp->part[2] = s0; sp->part[3] = s0 + 1;
+    }
+    return 0;
 }
 
 // A batch of voxelizations run together.
@@ -340,6 +455,111 @@ vxb_status vxb_voxelize_to_device(vxb_voxelizer* v, int nodes, const vxb_request
                                   uint64_t dev_bytes, void* stream, vxb_grid_info* info) {
     if (!v) return failf(VXB_EINVAL, "voxelizer is NULL");
     return v->run(nodes, req, dev_out, dev_bytes, reinterpret_cast<cudaStream_t>(stream), info);
+}
+
+vxb_status vxb_plan_parts(vxb_voxelizer* v, int nodes, const vxb_request* req, uint32_t dev_y, uint32_t dev_z,
+                          vxb_grid_info* infos) {
+    if (!v || !infos) return failf(VXB_EINVAL, "NULL argument");
+    std::vector<vxb_voxelizer::Space> sp;
+    int rc = v->partitions(req, dev_y, dev_z, &sp);
+    if (rc) return rc;
+    return v->planSpaces(nodes, req, sp, infos);
+}
+
+vxb_status vxb_voxelize_parts_to_device(vxb_voxelizer* v, int nodes, const vxb_request* req, uint32_t dev_y,
+                                        uint32_t dev_z, void* const* dev_outs, const uint64_t* dev_bytes,
+                                        void* stream, vxb_grid_info* infos) {
+    if (!v) return failf(VXB_EINVAL, "voxelizer is NULL");
+    std::vector<vxb_voxelizer::Space> sp;
+    int rc = v->partitions(req, dev_y, dev_z, &sp);
+    if (rc) return rc;
+    return v->runSpaces(nodes, req, sp, dev_outs, dev_bytes, reinterpret_cast<cudaStream_t>(stream), infos);
+}
+
+vxb_status vxb_voxelize_parts_to_host(vxb_voxelizer* v, int nodes, const vxb_request* req, uint32_t dev_y,
+                                      uint32_t dev_z, void* const* host_outs, const uint64_t* host_bytes,
+                                      vxb_grid_info* infos) {
+    if (!v) return failf(VXB_EINVAL, "voxelizer is NULL");
+    std::vector<vxb_voxelizer::Space> sp;
+    int rc = v->partitions(req, dev_y, dev_z, &sp);
+    if (rc) return rc;
+    std::vector<vxb_grid_info> gi(sp.size());
+    if ((rc = v->planSpaces(nodes, req, sp, gi.data()))) return rc;
+    if (infos)
+        for (size_t i = 0; i < sp.size(); ++i) infos[i] = gi[i];
+    if (!host_outs || !host_bytes) return failf(VXB_EINVAL, "NULL output arrays");
+    uint64_t total = 0;
+    std::vector<uint64_t> off(sp.size());
+    for (size_t i = 0; i < sp.size(); ++i) {
+        if (!host_outs[i] || host_bytes[i] < gi[i].bytes)
+            return failf(VXB_EINVAL, "output buffer %zu is NULL or too small", i);
+        off[i] = total;
+        total += (gi[i].bytes + 255) & ~uint64_t(255);
+    }
+    VXB_CUDA(cudaSetDevice(v->device));
+    if ((rc = v->outStage.ensure(total))) return rc;
+    std::vector<void*> outs(sp.size());
+    for (size_t i = 0; i < sp.size(); ++i) outs[i] = v->outStage.as<uint8_t>() + off[i];
+    std::vector<uint64_t> bytes(sp.size());
+    for (size_t i = 0; i < sp.size(); ++i) bytes[i] = gi[i].bytes;
+    rc = v->runSpaces(nodes, req, sp, outs.data(), bytes.data(), 0, infos);
+    for (size_t i = 0; rc == 0 && i < sp.size(); ++i) {
+        cudaError_t e = cudaMemcpy(host_outs[i], outs[i], gi[i].bytes, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = failf(VXB_ECUDA, "%s", cudaGetErrorString(e));
+    }
+    return rc;
+}
+
+vxb_status vxb_plan_slice(vxb_voxelizer* v, const vxb_request* req, int direction, uint32_t slice,
+                          vxb_grid_info* info) {
+    if (!v || !info) return failf(VXB_EINVAL, "NULL argument");
+    vxb_voxelizer::Space sp;
+    bool oob = false;
+    int rc = v->sliceSpace(req, direction, slice, &sp, &oob);
+    if (rc) return rc;
+    return v->planSpaces(1, req, std::vector<vxb_voxelizer::Space>{sp}, info);
+}
+
+vxb_status vxb_voxelize_slice_to_device(vxb_voxelizer* v, const vxb_request* req, int direction, uint32_t slice,
+                                        void* dev_out, uint64_t dev_bytes, void* stream, vxb_grid_info* info) {
+    if (!v) return failf(VXB_EINVAL, "voxelizer is NULL");
+    vxb_voxelizer::Space sp;
+    bool oob = false;
+    int rc = v->sliceSpace(req, direction, slice, &sp, &oob);
+    if (rc) return rc;
+    const std::vector<vxb_voxelizer::Space> one{sp};
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (!oob) return v->runSpaces(1, req, one, &dev_out, &dev_bytes, s, info);
+    // sliceOOB (src/host_side.cpp:1225-1236): the reference voxelizes slice
+    // 0 and then zeroes the array; the result is the zero array.
+    vxb_grid_info gi;
+    if ((rc = v->planSpaces(1, req, one, &gi))) return rc;
+    if (info) *info = gi;
+    if ((rc = v->validate(1, req))) return rc;
+    if (!dev_out || dev_bytes < gi.bytes) return failf(VXB_EINVAL, "output buffer is NULL or too small");
+    VXB_CUDA(cudaSetDevice(v->device));
+    VXB_CUDA(cudaMemsetAsync(dev_out, 0, gi.bytes, s));
+    VXB_CUDA(cudaStreamSynchronize(s));
+    v->launches = 0;
+    return VXB_OK;
+}
+
+vxb_status vxb_voxelize_slice_to_host(vxb_voxelizer* v, const vxb_request* req, int direction, uint32_t slice,
+                                      void* host_out, uint64_t host_bytes, vxb_grid_info* info) {
+    if (!v) return failf(VXB_EINVAL, "voxelizer is NULL");
+    vxb_grid_info gi;
+    int rc = vxb_plan_slice(v, req, direction, slice, &gi);
+    if (rc) return rc;
+    if (info) *info = gi;
+    if (!host_out || host_bytes < gi.bytes) return failf(VXB_EINVAL, "output buffer is NULL or too small");
+    VXB_CUDA(cudaSetDevice(v->device));
+    if ((rc = v->outStage.ensure(gi.bytes))) return rc;
+    rc = vxb_voxelize_slice_to_device(v, req, direction, slice, v->outStage.p, gi.bytes, nullptr, info);
+    if (rc == 0) {
+        cudaError_t e = cudaMemcpy(host_out, v->outStage.p, gi.bytes, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = failf(VXB_ECUDA, "%s", cudaGetErrorString(e));
+    }
+    return rc;
 }
 
 vxb_status vxb_voxelize_to_host(vxb_voxelizer* v, int nodes, const vxb_request* req, void* host_out,

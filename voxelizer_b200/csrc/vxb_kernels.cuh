@@ -26,6 +26,9 @@ struct PassGeom {
     uint32_t resY, resZ; // voxels along y / z before the 1-voxel padding
     uint32_t AY, AZ;     // allocated rows: resY + 2, resZ + 2
     uint32_t ipx;        // 32-bit words per row: X / 32
+    uint32_t padY, padZ; // allocation row / plane of local voxel row / plane 0 (1, or 0 next to a neighbour)
+    uint32_t border;     // zero the allocation's faces in the node output (a device space with neighbours)
+    uint32_t pad0;
 };
 
 struct SplitYZ { uint32_t y0, y1, z0, z1; };

@@ -254,6 +254,9 @@ extern "C" vxb_status vxb_voxelize_bits_noalloc(const float* dev_vertices, const
     g.AY = bg.alloc[1];
     g.AZ = bg.alloc[2];
     g.ipx = bg.res[0] / 32;
+    g.padY = 1;
+    g.padZ = 1;
+    g.border = 0;
     tab.unit.V = dev_vertices;
     tab.unit.I = dev_indices;
     tab.unit.nT = n_triangles;

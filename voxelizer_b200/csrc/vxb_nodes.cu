@@ -210,8 +210,18 @@ struct UnitWords {
     const uint32_t* surf;     // NULL without materials
     const uint8_t* yLater;
     const uint8_t* zLater;
-    uint32_t ipx, AY, AZ;
+    uint32_t ipx, AY, AZ, border;
 };
+
+// Nodes of word w that zeroPadding (src/voxelizer.cu:4811-4844) clears in a
+// device space with neighbours: every node on a face of the allocation.
+__device__ __forceinline__ uint32_t borderMask(const UnitWords& u, uint32_t w) {
+    if (!u.border) return 0u;
+    const uint32_t row = w / u.ipx, k = w - row * u.ipx;
+    const uint32_t z = row / u.AY, y = row - z * u.AY;
+    if (y == 0 || y + 1 == u.AY || z == 0 || z + 1 == u.AZ) return 0xFFFFFFFFu;
+    return (k == 0 ? 0x80000000u : 0u) | (k + 1 == u.ipx ? 1u : 0u);
+}
 
 struct EmitArgs {
     Batch b;
@@ -233,6 +243,7 @@ __device__ __forceinline__ UnitWords unitWords(const EmitArgs& a, const Unit& U)
     uw.ipx = U.g.ipx;
     uw.AY = U.g.AY;
     uw.AZ = U.g.AZ;
+    uw.border = U.g.border;
     return uw;
 }
 
@@ -320,9 +331,13 @@ __global__ void __launch_bounds__(256, 6) emitNarrowKernel(EmitArgs a, uint64_t 
         if (wbase >= nWords) continue;            // padding after the unit's grid (whole warp)
         const uint32_t w = wbase + lane;
         WordNbrs n{};
-        if (w < nWords) n = loadNbrs<K>(uw, w);
-        const uint32_t interior = n.c & n.L & n.R & n.In & n.Out & n.Dn & n.Up & ~n.s0;
-        uint32_t rest = (n.c & ~interior) | n.s0;
+        uint32_t zero = 0u;
+        if (w < nWords) {
+            n = loadNbrs<K>(uw, w);
+            zero = borderMask(uw, w);
+        }
+        const uint32_t interior = n.c & n.L & n.R & n.In & n.Out & n.Dn & n.Up & ~n.s0 & ~zero;
+        uint32_t rest = ((n.c & ~interior) | n.s0) & ~zero;
         uint32_t v[CH * 4];
         if (interior == 0u) {
 #pragma unroll
@@ -392,8 +407,9 @@ __global__ void __launch_bounds__(256) emitPartialKernel(EmitArgs a, uint64_t to
         if (w >= U.g.ipx * U.g.AY * U.g.AZ) continue;
         const UnitWords uw = unitWords(a, U);
         const WordNbrs n = loadNbrs<kPartial>(uw, w);
+        const uint32_t zero = borderMask(uw, w);
         uint4* out = reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(U.out) + (size_t)w * 32 * 8);
-        if ((n.c | n.s0 | n.f0) == 0u) {
+        if (((n.c | n.s0 | n.f0) & ~zero) == 0u) {
 #pragma unroll
             for (int i = 0; i < 16; ++i) out[i] = make_uint4(0, 0, 0, 0);
             continue;
@@ -413,7 +429,7 @@ __global__ void __launch_bounds__(256) emitPartialKernel(EmitArgs a, uint64_t to
                 // overwrites surface nodes with the winning triangle's ratio.
                 float r = ((n.f0 >> q) & 1u) ? 1.0f : 0.0f;
                 if ((n.s0 >> q) & 1u) {
-                    if (matRank < a.keysCap) {
+                    if (matRank < a.keysCap && !((zero >> q) & 1u)) {
                         const uint64_t key = reinterpret_cast<const unsigned long long*>(a.keys)[matRank];
                         mat = NT::keyMat(key);
                         r = ratio::nodeRatio(U.V, U.I, (uint32_t)key, (uint32_t)(key >> 40), x0 + (int)bt, y0, z0,
@@ -421,7 +437,7 @@ __global__ void __launch_bounds__(256) emitPartialKernel(EmitArgs a, uint64_t to
                     }
                     ++matRank;
                 }
-                const uint64_t nv = NT::pack(bid, mat, r);
+                const uint64_t nv = (zero >> q) & 1u ? 0ull : NT::pack(bid, mat, r);
                 v32[2 * j] = (uint32_t)nv;
                 v32[2 * j + 1] = (uint32_t)(nv >> 32);
             }

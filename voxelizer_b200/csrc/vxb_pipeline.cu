@@ -61,9 +61,10 @@ int gridInfo(const Plan& p, int nodeType, int nodes, vxb_grid_info* info) {
     }
     gi.voxel_length = p.d;
     for (int a = 0; a < 3; ++a) {
-        gi.min_vertex[a] = p.mn[a];
+        gi.min_vertex[a] = p.mnHost[a];
         gi.max_vertex[a] = p.mx[a];
     }
+    for (int k = 0; k < 4; ++k) gi.partition[k] = p.part[k];
     gi.resolution.x = p.res[0];
     gi.resolution.y = p.res[1];
     gi.resolution.z = p.res[2];
@@ -89,6 +90,10 @@ PassGeom makeGeom(const Plan& p, int lattice) {
     g.AY = p.alloc[1];
     g.AZ = p.alloc[2];
     g.ipx = p.res[0] / 32;
+    g.padY = p.padY;
+    g.padZ = p.padZ;
+    g.border = p.border ? 1u : 0u;
+    g.pad0 = 0;
     return g;
 }
 
@@ -149,6 +154,12 @@ int Pipeline::prepare(const std::vector<MeshJob>& jobs, cudaStream_t s) {
         if (makePlan(j.mn, j.mx, j.req.by_cube_length, j.req.max_dimension, j.req.cube_length, vs, ms, p))
             return failf(VXB_EINVAL, "invalid request (maxDimension >= 2 or cubeLength > 0, split sizes > 0 and an x "
                                      "pass of at most 1024 voxels are required)");
+        if (j.space) {
+            if (fcc) return failf(VXB_EUNSUPPORTED, "device spaces of FCC lattices are not supported");
+            Plan full = p;
+            if (devicePlan(full, j.part[0], j.part[1], j.part[2], j.part[3], vs, ms, p))
+                return failf(VXB_EINVAL, "empty or out-of-range partition");
+        }
         vxb_grid_info gi;
         if (int rc = gridInfo(p, j.nodeType, j.nodes, &gi)) return rc;
         if (!j.out) return failf(VXB_EINVAL, "output buffer is NULL");

@@ -24,6 +24,11 @@ struct MeshJob {
     vxb_request req;
     void* out;
     uint64_t outBytes;
+    // Device space: voxelize partition [part[0], part[1]) x [part[2],
+    // part[3]) of the yz voxel range as the reference's devices do (space
+    // = 1); 0 = the whole grid.
+    int space = 0;
+    uint32_t part[4] = {0, 0, 0, 0};
 };
 
 // Shape of a job's result (vxb_plan).  Returns 0 or a vxb status.

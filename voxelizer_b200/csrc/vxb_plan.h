@@ -16,7 +16,8 @@ namespace vxb {
 struct Range { uint32_t lo, hi; };
 
 struct Plan {
-    double mn[3], mx[3];   // bounding box (float vertices widened to double)
+    double mn[3], mx[3];   // bounding box (float vertices widened to double); mn: the voxelized box's corner
+    double mnHost[3];      // the mesh's minimum corner (getMinVertex)
     double d;              // voxel length
     uint32_t res[3];       // resolution.max: x padded (+2) and rounded to 32 * xSplits
     uint32_t xSplits, xRes;
@@ -24,6 +25,16 @@ struct Plan {
     std::vector<Range> ySplitsExt, zSplitsExt;        // voxSplitRes over [0, res)
     std::vector<Range> ySplitsAlloc, zSplitsAlloc;    // voxSplitRes over [0, alloc)
     std::vector<Range> xMat, yMat, zMat;              // matSplitRes over [0, res)
+    // Device space (src/host_side.cpp:782-1011): a yz partition of the full
+    // grid whose voxelized box is extended by one voxel towards each
+    // neighbouring partition.  Row `padY` of the allocation holds local
+    // voxel row 0 (1 without a neighbour below in y, the zero padding row;
+    // 0 with one, the overlap row), likewise `padZ`; `border` zeroes the
+    // allocation's faces after the boundary ids (zeroPadding).  A full grid
+    // is the device space without neighbours.
+    uint32_t padY = 1, padZ = 1;
+    bool border = false;
+    uint32_t part[4] = {0, 0, 0, 0};   // partition y0, y1, z0, z1 (voxels of the full grid)
 };
 
 // Reference conversion semantics for uint(ceil(...)): NaN and negatives to 0.
@@ -61,7 +72,7 @@ inline void boundingBox(const float* v, uint32_t nV, double* mn, double* mx) {
 // Returns 0, or a negative vxb status for arguments the path cannot honour.
 inline int makePlan(const double* mn, const double* mx, int byCube, uint32_t maxDim, double cube,
                     const uint32_t* voxSplit, const uint32_t* matSplit, Plan& p) {
-    for (int a = 0; a < 3; ++a) { p.mn[a] = mn[a]; p.mx[a] = mx[a]; }
+    for (int a = 0; a < 3; ++a) { p.mn[a] = mn[a]; p.mx[a] = mx[a]; p.mnHost[a] = mn[a]; }
     const double dx = mx[0] - mn[0], dy = mx[1] - mn[1], dz = mx[2] - mn[2];
     uint32_t r[3];
     double d;
@@ -113,7 +124,69 @@ inline int makePlan(const double* mn, const double* mx, int byCube, uint32_t max
     p.xMat = splitLength(r[0], matSplit[0] ? matSplit[0] : r[0]);
     p.yMat = splitLength(r[1], matSplit[1] ? matSplit[1] : r[1]);
     p.zMat = splitLength(r[2], matSplit[2] ? matSplit[2] : r[2]);
+    p.padY = p.padZ = 1;
+    p.border = false;
+    p.part[0] = 0;
+    p.part[1] = r[1];
+    p.part[2] = 0;
+    p.part[3] = r[2];
     return 0;
+}
+
+// The device space of partition [y0, y1) x [z0, z1) of the full plan `p`
+// (voxelizeWorker, src/host_side.cpp:911-1011): neighbour flags from the
+// partition's position, the extended box, its minimum corner in double
+// (hostMin + extMin * d), the allocation (partition + 2 rows each way) and
+// the split lists over the extended box and the allocation.
+inline int devicePlan(const Plan& p, uint32_t y0, uint32_t y1, uint32_t z0, uint32_t z1, const uint32_t* voxSplit,
+                      const uint32_t* matSplit, Plan& q) {
+    if (!(y0 < y1 && y1 <= p.res[1] && z0 < z1 && z1 <= p.res[2])) return -1;
+    bool left = false, right = false, down = false, up = false;
+    if (y0 == 0 && y1 != p.res[1]) right = true;
+    else if (y1 == p.res[1] && y0 != 0) left = true;
+    else if (y0 != 0 && y1 != p.res[1]) left = right = true;
+    if (z0 == 0 && z1 != p.res[2]) up = true;
+    else if (z1 == p.res[2] && z0 != 0) down = true;
+    else if (z0 != 0 && z1 != p.res[2]) down = up = true;
+    const uint32_t ey0 = y0 - (left ? 1u : 0u), ey1 = y1 + (right ? 1u : 0u);
+    const uint32_t ez0 = z0 - (down ? 1u : 0u), ez1 = z1 + (up ? 1u : 0u);
+    q = p;
+    q.mn[0] = p.mn[0] + double(0u) * p.d;
+    q.mn[1] = p.mn[1] + double(ey0) * p.d;
+    q.mn[2] = p.mn[2] + double(ez0) * p.d;
+    q.res[1] = ey1 - ey0;
+    q.res[2] = ez1 - ez0;
+    q.alloc[1] = (y1 - y0) + 2;
+    q.alloc[2] = (z1 - z0) + 2;
+    q.ySplitsExt = splitLength(q.res[1], voxSplit[1]);
+    q.zSplitsExt = splitLength(q.res[2], voxSplit[2]);
+    q.ySplitsAlloc = splitLength(q.alloc[1], voxSplit[1]);
+    q.zSplitsAlloc = splitLength(q.alloc[2], voxSplit[2]);
+    q.yMat = splitLength(q.res[1], matSplit[1] ? matSplit[1] : q.res[1]);
+    q.zMat = splitLength(q.res[2], matSplit[2] ? matSplit[2] : q.res[2]);
+    q.padY = left ? 0u : 1u;
+    q.padZ = down ? 0u : 1u;
+    q.border = left || right || down || up;
+    q.part[0] = y0;
+    q.part[1] = y1;
+    q.part[2] = z0;
+    q.part[3] = z1;
+    return 0;
+}
+
+// splitResolutionByNrOfParts over one axis (src/host_side.cpp:3025-3105):
+// `parts` pieces of [0, len), floor division, the remainder to the first.
+inline std::vector<Range> splitParts(uint32_t len, uint32_t parts) {
+    std::vector<Range> out(parts);
+    uint32_t prev = len;
+    for (uint32_t i = parts; i > 0; --i) {
+        Range r;
+        r.hi = prev;
+        r.lo = r.hi - r.hi / i;
+        prev = r.lo;
+        out[i - 1] = r;
+    }
+    return out;
 }
 
 }  // namespace vxb

@@ -207,7 +207,7 @@ __device__ __forceinline__ void solidCandidate(const SolidStage& st, const Batch
         px = px < 0.0 ? 0.0 : px;
         const uint32_t vx = __double2uint_rz(ceil(__ddiv_rn(px, d))) + 1u;
         if (vx >= g.X) continue;
-        const uint32_t row = (vz + 1) * g.AY + (vy + 1);
+        const uint32_t row = (vz + g.padZ) * g.AY + (vy + g.padY);
         atomicXor(toggles + (size_t)row * g.ipx + (vx >> 5), 0x80000000u >> (vx & 31u));
     }
 }

@@ -364,10 +364,10 @@ struct WarpStage {
 // Where a unit's surface bits live.
 struct UnitGrid {
     uint64_t wordBase;   // first word of the unit in the surface arena
-    uint32_t AY, ipx;
+    uint32_t AY, ipx, padY, padZ;
 };
 
-// processVoxel of the surface pass, coordinates with the 1-voxel padding.
+// processVoxel of the surface pass.
 // mode 0: set the bit and append (bit position << 24 | key) to the hit list;
 // mode 1: merge the key at the voxel's rank (surface bits are complete).
 struct Sink {
@@ -380,9 +380,11 @@ struct Sink {
     uint32_t listCap;
     int mode;
     int wide;                  // 64-bit keys (PartialNode)
+    // (xi, yi, zi): voxel of the unit's voxelized box; the allocation holds
+    // it one column further along x and padY / padZ rows further along y / z.
     __device__ __forceinline__ void operator()(int xi, int yi, int zi, uint64_t key, const UnitGrid& ug,
                                                const WarpStage& ws) const {
-        const uint32_t x = (uint32_t)xi, y = (uint32_t)yi, z = (uint32_t)zi;
+        const uint32_t x = (uint32_t)xi + 1u, y = (uint32_t)yi + ug.padY, z = (uint32_t)zi + ug.padZ;
         const uint64_t w = ug.wordBase + ((uint64_t)z * ug.AY + y) * ug.ipx + (x >> 5);
         const uint32_t b = x & 31u;
         const uint32_t bit = 0x80000000u >> b;
@@ -431,9 +433,9 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
     const uint32_t ex = (uint32_t)(r.hi[0] - r.lo[0] + 1), ey = (uint32_t)(r.hi[1] - r.lo[1] + 1);
     if (bb == 1) {
         // process1DTriangles (3306-3411): every voxel of the line, no test.
-        if (axis == 0) sink(r.lo[0] + (int)u + 1, r.lo[1] + 1, r.lo[2] + 1, key, ug, ws);
-        else if (axis == 1) sink(r.lo[0] + 1, r.lo[1] + (int)u + 1, r.lo[2] + 1, key, ug, ws);
-        else sink(r.lo[0] + 1, r.lo[1] + 1, r.lo[2] + (int)u + 1, key, ug, ws);
+        if (axis == 0) sink(r.lo[0] + (int)u, r.lo[1], r.lo[2], key, ug, ws);
+        else if (axis == 1) sink(r.lo[0], r.lo[1] + (int)u, r.lo[2], key, ug, ws);
+        else sink(r.lo[0], r.lo[1], r.lo[2] + (int)u, key, ug, ws);
         return;
     }
     if (bb == 2) {
@@ -442,17 +444,17 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
             const int j = r.lo[1] + (int)(u % ey), k = r.lo[2] + (int)(u / ey);
             if (overlapTest<site::OT_2D_YZ>(od, vbComp<site::PC_2D>(j, g.mnf[1], d),
                                             vbComp<site::PC_2D>(k, g.mnf[2], d)))
-                sink(r.lo[0] + 1, j + 1, k + 1, key, ug, ws);
+                sink(r.lo[0], j, k, key, ug, ws);
         } else if (axis == 1) {
             const int i = r.lo[0] + (int)(u % ex), k = r.lo[2] + (int)(u / ex);
             if (overlapTest<site::OT_2D_ZX>(od, vbComp<site::PC_2D>(k, g.mnf[2], d),
                                             vbComp<site::PC_2D>(i, g.mnf[0], d)))
-                sink(i + 1, r.lo[1] + 1, k + 1, key, ug, ws);
+                sink(i, r.lo[1], k, key, ug, ws);
         } else {
             const int i = r.lo[0] + (int)(u % ex), j = r.lo[1] + (int)(u / ex);
             if (overlapTest<site::OT_2D_XY>(od, vbComp<site::PC_2D>(i, g.mnf[0], d),
                                             vbComp<site::PC_2D>(j, g.mnf[1], d)))
-                sink(i + 1, j + 1, r.lo[2] + 1, key, ug, ws);
+                sink(i, j, r.lo[2], key, ug, ws);
         }
         return;
     }
@@ -472,11 +474,11 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
             const int lo = max(r.lo[0], (int)__ldg(sl + 2 * s)), hi = min(r.hi[0], (int)__ldg(sl + 2 * s + 1) - 1);
             if (lo > hi || d0 > hi || d1 < lo) continue;
             const int a = d0 < lo ? lo : d0, c = d1 > hi ? hi : d1;
-            if (a == c) { sink(a + 1, j + 1, k + 1, key, ug, ws); continue; }
+            if (a == c) { sink(a, j, k, key, ug, ws); continue; }
             for (int i = a; i <= c; ++i) {
                 p.x = vbComp<site::PC_3DL>(i, g.mnf[0], d);
                 if (overlapTest<site::OT_3DX_ZX>(ov->o[1], p.z, p.x) && overlapTest<site::OT_3DX_XY>(ov->o[2], p.x, p.y))
-                    sink(i + 1, j + 1, k + 1, key, ug, ws);
+                    sink(i, j, k, key, ug, ws);
             }
         }
     } else if (axis == 1) {
@@ -490,11 +492,11 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
             const int lo = max(r.lo[1], (int)__ldg(sl + 2 * s)), hi = min(r.hi[1], (int)__ldg(sl + 2 * s + 1) - 1);
             if (lo > hi || d0 > hi || d1 < lo) continue;
             const int a = d0 < lo ? lo : d0, c = d1 > hi ? hi : d1;
-            if (a == c) { sink(i + 1, a + 1, k + 1, key, ug, ws); continue; }
+            if (a == c) { sink(i, a, k, key, ug, ws); continue; }
             for (int j = a; j <= c; ++j) {
                 p.y = vbComp<site::PC_3DL>(j, g.mnf[1], d);
                 if (overlapTest<site::OT_3DY_XY>(ov->o[2], p.x, p.y) && overlapTest<site::OT_3DY_YZ>(ov->o[0], p.y, p.z))
-                    sink(i + 1, j + 1, k + 1, key, ug, ws);
+                    sink(i, j, k, key, ug, ws);
             }
         }
     } else {
@@ -508,11 +510,11 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
             const int lo = max(r.lo[2], (int)__ldg(sl + 2 * s)), hi = min(r.hi[2], (int)__ldg(sl + 2 * s + 1) - 1);
             if (lo > hi || d0 > hi || d1 < lo) continue;
             const int a = d0 < lo ? lo : d0, c = d1 > hi ? hi : d1;
-            if (a == c) { sink(i + 1, j + 1, a + 1, key, ug, ws); continue; }
+            if (a == c) { sink(i, j, a, key, ug, ws); continue; }
             for (int k = a; k <= c; ++k) {
                 p.z = vbComp<site::PC_3DL>(k, g.mnf[2], d);
                 if (overlapTest<site::OT_3DZ_YZ>(ov->o[0], p.y, p.z) && overlapTest<site::OT_3DZ_ZX>(ov->o[1], p.z, p.x))
-                    sink(i + 1, j + 1, k + 1, key, ug, ws);
+                    sink(i, j, k, key, ug, ws);
             }
         }
     }
@@ -578,7 +580,7 @@ __global__ void __launch_bounds__(kBlock) surfaceWorkKernel(Sink sink, Batch b, 
                                                : (uint64_t)r.key;
                 const Unit& U = b.units[r.unit];
                 const PassGeom g = U.g;
-                const UnitGrid ug{U.wordBase, g.AY, g.ipx};
+                const UnitGrid ug{U.wordBase, g.AY, g.ipx, g.padY, g.padZ};
                 const uint32_t sliceOff[3] = {U.sliceBase, U.sliceBase + U.sliceN[0],
                                               U.sliceBase + U.sliceN[0] + U.sliceN[1]};
                 const uint32_t sliceN[3] = {U.sliceN[0], U.sliceN[1], U.sliceN[2]};
