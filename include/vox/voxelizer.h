@@ -15,8 +15,9 @@
 // node output) but runs every partition on this voxelizer's device; the
 // NodePointers carry each partition's dim and loc.  Inside
 // simulateMultidevice the results are host arrays (new[]), as the
-// reference's collectData uploads them.  Slices along y and z are provided
-// (devConfig 1); slicing along x (the reference rotates the mesh) throws.
+// reference's collectData uploads them.  Slices are provided along x, y and
+// z (devConfig 1); slices along x turn the mesh as the reference does, but
+// leave the voxelizer's stored mesh as it is.
 #ifndef VOX_VOXELIZER_B200_H
 #define VOX_VOXELIZER_B200_H
 
@@ -206,8 +207,8 @@ public:
     NodePointer<Node> voxelizeToNodesToRAM(double cubeLength, uint3 voxSplitRes = make_uint3(1024, 512, 512),
                                            uint3 matSplitRes = make_uint3(512, 512, 512));
 
-    // Slices (src/host_side.cpp:1927-2262): direction 1 (y) or 2 (z); a
-    // three-layer node array whose middle layer is slice `slice`.
+    // Slices (src/host_side.cpp:1927-2262): direction 0 (x), 1 (y) or 2
+    // (z); a three-layer node array whose middle layer is slice `slice`.
     std::vector<NodePointer<Node> > voxelizeSlice(uint maxDimension, int direction, uint slice, uint devConfig = 1,
                                                   uint2 voxSplitRes = make_uint2(1024, 512),
                                                   uint2 matSplitRes = make_uint2(512, 512));

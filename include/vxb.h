@@ -112,9 +112,9 @@ vxb_status vxb_verbose_output(vxb_voxelizer* v, int enable);
 vxb_status vxb_plan(vxb_voxelizer* v, int nodes, const vxb_request* req, vxb_grid_info* info);
 
 /* getArrayDimensions(longestSizeInVoxels | cubeLength, maxInternalXSize,
- * sliceAlongX), src/host_side.cpp:3329-3475.  sliceAlongX (the dimensions of
- * the rotated model the reference slices along x) returns
- * VXB_EUNSUPPORTED, as slicing along x does. */
+ * sliceAlongX), src/host_side.cpp:3329-3475.  With sliceAlongX: the grid of
+ * the mesh turned as for slices along x, with x and y exchanged (FCC
+ * lattices: VXB_EUNSUPPORTED). */
 vxb_status vxb_get_array_dimensions(vxb_voxelizer* v, int by_cube_length, uint32_t max_dimension,
                                     double cube_length, uint32_t max_internal_x, int slice_along_x,
                                     vxb_uint3* dims);
@@ -164,8 +164,14 @@ vxb_status vxb_voxelize_parts_to_host(vxb_voxelizer* v, int nodes, const vxb_req
  * zero; boundary ids see the voxelized neighbour rows.  Slice 0 or past the
  * grid gives the zero array (sliceOOB).  Node output only; the request's
  * split sizes are used as given (the reference's uint2 (a, b) means
- * (a, b, b)).  Direction 0 (the reference rotates the mesh) and FCC lattices
- * return VXB_EUNSUPPORTED. */
+ * (a, b, b)).  Direction 0 (x) follows the reference's rotation
+ * (src/host_side.cpp:704-718, 1144-1223, 3261-3309): the mesh turned about z
+ * (x' = a - y, y' = b + x, from its bounding box) is sliced along y and the
+ * node array is turned back before the boundary ids, so the result is
+ * (3, X', Z') nodes of the turned grid with the middle x layer the slice;
+ * `slice` counts along the turned grid's y.  The voxelizer's own mesh stays
+ * as it is (the reference keeps its stored vertices turned after such a
+ * call).  FCC lattices return VXB_EUNSUPPORTED. */
 vxb_status vxb_plan_slice(vxb_voxelizer* v, const vxb_request* req, int direction, uint32_t slice,
                           vxb_grid_info* info);
 vxb_status vxb_voxelize_slice_to_device(vxb_voxelizer* v, const vxb_request* req, int direction, uint32_t slice,

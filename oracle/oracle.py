@@ -63,7 +63,7 @@ class _Params(ctypes.Structure):
                 ("by_cube_length", ctypes.c_int), ("max_dim", ctypes.c_uint32), ("cube_length", ctypes.c_double),
                 ("vox_split", ctypes.c_uint32 * 3), ("mat_split", ctypes.c_uint32 * 3),
                 ("fma_sites", ctypes.c_uint8 * 48), ("threads", ctypes.c_int), ("space", ctypes.c_int),
-                ("part", ctypes.c_uint32 * 4)]
+                ("part", ctypes.c_uint32 * 4), ("rotate_x", ctypes.c_int)]
 
 
 class Info(ctypes.Structure):
@@ -93,7 +93,7 @@ def lib():
     return _lib
 
 
-def _params(node_type, nodes, materials, size, vox, mat, fma_model, threads, part=None):
+def _params(node_type, nodes, materials, size, vox, mat, fma_model, threads, part=None, rotate_x=False):
     p = _Params()
     p.node_type = int(node_type)
     p.node_output = int(bool(nodes))
@@ -108,6 +108,7 @@ def _params(node_type, nodes, materials, size, vox, mat, fma_model, threads, par
     if part is not None:   # device space: yz partition (y0, y1, z0, z1) of the grid
         p.space = 1
         p.part[:] = [int(v) for v in part]
+    p.rotate_x = int(bool(rotate_x))
     return p
 
 
@@ -117,8 +118,8 @@ def out_dtype(node_type, nodes):
     return {1: np.uint8, 2: np.uint16, 4: np.uint32, 8: np.uint64}[NODE_BYTES[node_type]]
 
 
-def plan(mesh, node_type, nodes, size, vox=(1024, 512, 512), part=None):
-    p = _params(node_type, nodes, 0, size, vox, (512, 512, 512), None, 0, part)
+def plan(mesh, node_type, nodes, size, vox=(1024, 512, 512), part=None, rotate_x=False):
+    p = _params(node_type, nodes, 0, size, vox, (512, 512, 512), None, 0, part, rotate_x)
     info = Info()
     rc = lib().orc_plan(ctypes.byref(p), mesh.vertices.ctypes.data, mesh.n_vertices, ctypes.byref(info))
     if rc:
@@ -127,10 +128,10 @@ def plan(mesh, node_type, nodes, size, vox=(1024, 512, 512), part=None):
 
 
 def voxelize(mesh, node_type, nodes, materials, size, vox=(1024, 512, 512), mat=(512, 512, 512),
-             fma_model=None, threads=0, want_conflicts=False, part=None):
+             fma_model=None, threads=0, want_conflicts=False, part=None, rotate_x=False):
     """Returns (output array (flat), Info, conflict mask or None).  `part`
     (y0, y1, z0, z1) voxelizes that partition as a device space."""
-    p = _params(node_type, nodes, materials, size, vox, mat, fma_model, threads, part)
+    p = _params(node_type, nodes, materials, size, vox, mat, fma_model, threads, part, rotate_x)
     info = Info()
     L = lib()
     rc = L.orc_plan(ctypes.byref(p), mesh.vertices.ctypes.data, mesh.n_vertices, ctypes.byref(info))

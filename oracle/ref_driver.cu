@@ -14,6 +14,7 @@
 #include "common.h"
 #include "node_types.h"
 #include "host_device_interface.h"
+#include "device_code.h"   // declares the unRotateNodes kernel
 
 #include <cuda_runtime.h>
 #include <cmath>
@@ -110,6 +111,10 @@ struct Params {
     // (host_side.cpp:782-813) and voxelizeWorker runs it (911-1236).
     int space;
     uint part[4];
+    // Slices along x: the mesh turned by rotateVertices (host_side.cpp:
+    // 3261-3280) and the node array turned back before the boundary ids
+    // (1144-1179).
+    int rotate_x;
 };
 
 // host_side.cpp:2462-2488
@@ -175,10 +180,10 @@ struct Dev {
     uint* tileOverlaps = nullptr; uint* offsetBuffer = nullptr;
     uint* wqTris = nullptr; uint* wqTiles = nullptr; uint* tileList = nullptr; uint* tileOffsets = nullptr;
     VoxInt* voxels = nullptr; void* nodes = nullptr; bool* error = nullptr;
-    uint* triTypes = nullptr; uint* sortedTris = nullptr;
+    uint* triTypes = nullptr; uint* sortedTris = nullptr; void* nodesCopy = nullptr;
     void release() {
         void* ps[] = {verts, idx, mats, tileOverlaps, offsetBuffer, wqTris, wqTiles, tileList,
-                      tileOffsets, voxels, nodes, error, triTypes, sortedTris};
+                      tileOffsets, voxels, nodes, error, triTypes, sortedTris, nodesCopy};
         for (void* q : ps) if (q) cudaFree(q);
         *this = Dev();
     }
@@ -253,6 +258,20 @@ struct Runner {
         nV = nV_; nT = nT_;
         double3 mn, mx;
         boundingBox(verts, nV, mn, mx);
+        // rotateVertices, host_side.cpp:3261-3280, then calculateBoundingBox
+        std::vector<float> turned;
+        if (p.rotate_x) {
+            const double a = (mx.y - mn.y) / 2.0 + (mx.x - mn.x) / 2.0;
+            const double b = (mx.y - mn.y) / 2.0 - (mx.x - mn.x) / 2.0;
+            turned.assign(verts, verts + 3 * (size_t)nV);
+            for (uint i = 0; i < nV; ++i) {
+                const double tempX = turned[3 * i];
+                turned[3 * i] = float(a - double(turned[3 * i + 1]));
+                turned[3 * i + 1] = float(b + tempX);
+            }
+            verts = turned.data();
+            boundingBox(verts, nV, mn, mx);
+        }
         host.nrOfTriangles = nT; host.nrOfVertices = nV; host.nrOfUniqueMaterials = nMat;
         host.minVertex = mn; host.maxVertex = mx;
         double d; uint3 res;
@@ -305,6 +324,7 @@ struct Runner {
         uint3 outDim = fcc ? make_uint3(2 * ar.x, ar.y, 2 * ar.z) : ar;
         uint64_t need = p.node_output ? uint64_t(nNodes) * sizeof(Node) : uint64_t(nInts) * sizeof(VoxInt);
         dimsOut[0] = outDim.x; dimsOut[1] = outDim.y; dimsOut[2] = outDim.z;
+        if (p.rotate_x && p.space && p.node_output) std::swap(dimsOut[0], dimsOut[1]);   // turned back
         if (out == nullptr) return 0;             // plan only
         if (outBytes < need) return -2;
         cudaEvent_t e0, e1;
@@ -363,20 +383,47 @@ struct Runner {
                             calcOptSurfaceVoxelization<Node>(dev, host, g.verts, g.idx, g.triTypes, g.sortedTris,
                                                              g.mats, (Node*)g.nodes, ms.splits[i], 1, 0, false);
                     }
+                    void* result = g.nodes;
+                    uint3 dims = ar;
+                    if (p.rotate_x) {
+                        // restoreRotatedNodes over the turned allocation's
+                        // subspaces, then the turned-back allocation and its
+                        // subspaces (host_side.cpp:1144-1179; unRotateCoords
+                        // 3293-3309: (x, y, z) -> (y, xDim - 1 - x, z)).
+                        RCHK(cudaMalloc(&g.nodesCopy, uint64_t(nNodes) * sizeof(Node)));
+                        RCHK(cudaMemset(g.nodesCopy, 0, uint64_t(nNodes) * sizeof(Node)));
+                        for (size_t i = 0; i < allocYz.splits.size(); ++i) {
+                            unRotateNodes<Node><<<dev.blocks, dev.threads>>>((Node*)g.nodes, (Node*)g.nodesCopy,
+                                                                             dev.allocResolution, allocYz.splits[i]);
+                            RCHK(cudaGetLastError());
+                        }
+                        const Bounds<uint3> ap = dev.allocResolution;
+                        const uint3 m1 = make_uint3(ap.max.x - 1, ap.max.y - 1, ap.max.z - 1);
+                        const uint3 t0 = make_uint3(ap.min.y, ar.x - 1 - ap.min.x, ap.min.z);
+                        const uint3 t1 = make_uint3(m1.y, ar.x - 1 - m1.x, m1.z);
+                        dev.allocResolution.min = make_uint3(min(t0.x, t1.x), min(t0.y, t1.y), min(t0.z, t1.z));
+                        dev.allocResolution.max = make_uint3(max(t0.x, t1.x) + 1, max(t0.y, t1.y) + 1,
+                                                             max(t0.z, t1.z) + 1);
+                        allocYz = splitYZ(make_uint2(p.vox_split.y, p.vox_split.z), dev.allocResolution);
+                        result = g.nodesCopy;
+                        dims = make_uint3(ar.y, ar.x, ar.z);
+                    }
                     for (size_t i = 0; i < allocYz.splits.size(); ++i) {
                         bool e;
                         do {
                             e = false;
                             RCHK(cudaMemcpy(g.error, &e, sizeof(bool), cudaMemcpyHostToDevice));
-                            procNodeList<Node>(dev, (Node*)g.nodes, nullptr, g.error, allocYz.splits[i], false, 0, false);
+                            procNodeList<Node>(dev, (Node*)g.nodes, (Node*)g.nodesCopy, g.error, allocYz.splits[i],
+                                               p.rotate_x != 0, 0, false);
                             RCHK(cudaMemcpy(&e, g.error, sizeof(bool), cudaMemcpyDeviceToHost));
                         } while (e);
                     }
                     // host_side.cpp:1211-1222
                     if (dev.left || dev.right || dev.up || dev.down) {
-                        refZeroFaces<Node><<<dev.blocks, dev.threads>>>((Node*)g.nodes, ar);
+                        refZeroFaces<Node><<<dev.blocks, dev.threads>>>((Node*)result, dims);
                         RCHK(cudaGetLastError());
                     }
+                    if (p.rotate_x) std::swap(g.nodes, g.nodesCopy);   // the result is read from g.nodes
                 }
             } else {
                 // fccWorker, host_side.cpp:1432-1657
@@ -445,13 +492,14 @@ static char g_refError[512] = {0};
 extern "C" const char* ref_last_error() { return g_refError; }
 
 // ref_voxelize over one device space: `part` (y0, y1, z0, z1), or NULL for
-// the whole grid.
+// the whole grid; rotate_x turns the mesh as for slices along x (the
+// partition is then in the turned grid's coordinates).
 extern "C" int ref_voxelize_space(int node_type, int node_output, int materials, int by_cube_length,
                                   uint32_t max_dim, double cube_length, const uint32_t* vox_split,
                                   const uint32_t* mat_split, const float* verts, uint32_t nV,
                                   const uint32_t* idx, uint32_t nT, const uint8_t* mats, uint32_t nMat,
-                                  const uint32_t* part, void* out, uint64_t out_bytes, uint32_t* dims_out,
-                                  double* ms) {
+                                  const uint32_t* part, int rotate_x, void* out, uint64_t out_bytes,
+                                  uint32_t* dims_out, double* ms) {
     Params p;
     p.node_type = node_type; p.node_output = node_output; p.materials = materials;
     p.by_cube_length = by_cube_length; p.max_dim = max_dim; p.cube_length = cube_length;
@@ -459,6 +507,7 @@ extern "C" int ref_voxelize_space(int node_type, int node_output, int materials,
     p.mat_split = make_uint3(mat_split[0], mat_split[1], mat_split[2]);
     p.space = part ? 1 : 0;
     for (int k = 0; k < 4; ++k) p.part[k] = part ? part[k] : 0u;
+    p.rotate_x = rotate_x;
     try {
         switch (node_type) {
         case 0: { Runner<ShortNode> r(p); return r.run(verts, nV, idx, nT, mats, nMat, out, out_bytes, dims_out, ms); }
@@ -482,5 +531,5 @@ extern "C" int ref_voxelize(int node_type, int node_output, int materials, int b
                             const uint32_t* idx, uint32_t nT, const uint8_t* mats, uint32_t nMat,
                             void* out, uint64_t out_bytes, uint32_t* dims_out, double* ms) {
     return ref_voxelize_space(node_type, node_output, materials, by_cube_length, max_dim, cube_length, vox_split,
-                              mat_split, verts, nV, idx, nT, mats, nMat, nullptr, out, out_bytes, dims_out, ms);
+                              mat_split, verts, nV, idx, nT, mats, nMat, nullptr, 0, out, out_bytes, dims_out, ms);
 }

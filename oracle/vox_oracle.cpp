@@ -294,6 +294,28 @@ static Plan makePlan(const orc_params* p, const float* v, uint nV) {
     return pl;
 }
 
+// rotateVertices (src/host_side.cpp:3261-3280): the mesh turned about z by
+// x' = a - y, y' = b + x with a = cy + cx, b = cy - cx from the half extents
+// of its bounding box (in double), rounded to float.
+static std::vector<float> turnedVertices(const float* v, uint nV) {
+    std::vector<float> r(v, v + 3 * (size_t)nV);
+    if (nV == 0) return r;
+    double mn[2] = {v[0], v[1]}, mx[2] = {v[0], v[1]};
+    for (uint i = 1; i < nV; ++i)
+        for (int a = 0; a < 2; ++a) {
+            mn[a] = std::min(mn[a], (double)v[3 * i + a]);
+            mx[a] = std::max(mx[a], (double)v[3 * i + a]);
+        }
+    const double cx = (mx[0] - mn[0]) / 2.0, cy = (mx[1] - mn[1]) / 2.0;
+    const double a = cy + cx, b = cy - cx;
+    for (uint i = 0; i < nV; ++i) {
+        const double x = v[3 * i];
+        r[3 * i] = float(a - double(v[3 * i + 1]));
+        r[3 * i + 1] = float(b + x);
+    }
+    return r;
+}
+
 // The device space of partition p->part (voxelizeWorker,
 // src/host_side.cpp:911-1011): neighbour flags from the partition's
 // position, the box extended by one voxel towards each neighbour, its
@@ -1064,7 +1086,7 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
     typedef Tr<N> T;
     const Fma F(p->fma_sites);
     const bool fcc = T::fcc;
-    const u3 alloc = pl.alloc;
+    u3 alloc = pl.alloc;
     const uint nInts = (alloc.x * alloc.y * alloc.z) >> 5;
     std::vector<uint32_t> voxels(nInts, 0u);
     Bounds<u3> ext{u3{0, 0, 0}, pl.ext};
@@ -1072,6 +1094,9 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
     const u2 vs{p->vox_split[1], p->vox_split[2]};
     std::vector<Bounds<u2> > extYz = splitYZ(vs, ext);
     std::vector<Bounds<u2> > allocYz = splitYZ(vs, allocPart);
+    // Slices along x: nodes are built on the turned grid and turned back
+    // before the boundary ids (src/host_side.cpp:1144-1206).
+    const bool turn = p->rotate_x && p->node_output && !fcc;
     const bool mats = p->materials && p->node_output;
     if (!p->node_output) {
         for (auto& s : extYz)
@@ -1082,7 +1107,11 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
     }
     const size_t nNodes = fcc ? (size_t)(2 * alloc.x) * alloc.y * (2 * alloc.z) : (size_t)alloc.x * alloc.y * alloc.z;
     if (conflict) memset(conflict, 0, nNodes);
-    N* nodes = (N*)out;
+    std::vector<N> turned(turn ? nNodes : 0);
+    std::vector<uint8_t> turnedConf(turn && conflict ? nNodes : 0);
+    uint8_t* const outConflict = conflict;
+    if (turn && conflict) conflict = turnedConf.data();
+    N* nodes = turn ? turned.data() : (N*)out;
     N zero = T::make(0, 0);
 #pragma omp parallel for schedule(static)
     for (long long i = 0; i < (long long)nNodes; ++i) nodes[i] = zero;
@@ -1172,6 +1201,26 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
     }
     info->n_conflicts = nConf;
     info->n_surface = rec.size();
+    if (turn) {
+        // unRotateNodes (src/voxelizer.cu:2061-2124): (x, y, z) of the X x Y
+        // x Z array goes to (y, X - 1 - x, z) of the Y x X x Z array; the
+        // allocation and its yz subspaces become the turned-back ones.
+        N* dst = (N*)out;
+        const size_t X = alloc.x, Y = alloc.y;
+#pragma omp parallel for schedule(static)
+        for (long long z = 0; z < (long long)alloc.z; ++z)
+            for (size_t y = 0; y < Y; ++y)
+                for (size_t x = 0; x < X; ++x) {
+                    const size_t i = (size_t)z * X * Y + y * X + x, j = (size_t)z * X * Y + (X - 1 - x) * Y + y;
+                    dst[j] = nodes[i];
+                    if (outConflict) outConflict[j] = conflict[i];
+                }
+        nodes = dst;
+        conflict = outConflict;
+        alloc = u3{alloc.y, alloc.x, alloc.z};
+        allocPart = Bounds<u3>{u3{0, 0, 0}, alloc};
+        allocYz = splitYZ(vs, allocPart);
+    }
     if (!fcc) {
         // fillNodeList2 + the host loop, src/voxelizer.cu:1790-1913 and
         // src/host_side.cpp:1183-1206: per alloc yz split, in order, prune
@@ -1275,6 +1324,11 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
 }  // namespace
 
 extern "C" int orc_plan(const orc_params* p, const float* verts, uint32_t nV, orc_info* info) {
+    std::vector<float> tv;
+    if (p->rotate_x) {
+        tv = turnedVertices(verts, nV);
+        verts = tv.data();
+    }
     Plan pl = makePlan(p, verts, nV);
     applySpace(p, pl);
     memset(info, 0, sizeof(*info));
@@ -1286,6 +1340,7 @@ extern "C" int orc_plan(const orc_params* p, const float* verts, uint32_t nV, or
     if (p->node_output) {
         info->dims[0] = fcc ? 2 * pl.alloc.x : pl.alloc.x;
         info->dims[1] = pl.alloc.y;
+        if (p->rotate_x && p->space && !fcc) std::swap(info->dims[0], info->dims[1]);   // turned back
         info->dims[2] = fcc ? 2 * pl.alloc.z : pl.alloc.z;
         info->out_bytes = (uint64_t)info->dims[0] * info->dims[1] * info->dims[2] * nb[p->node_type];
     } else {
@@ -1306,6 +1361,11 @@ extern "C" int orc_voxelize(const orc_params* p, const float* verts, uint32_t nV
     int rc = orc_plan(p, verts, nV, info);
     if (rc) return rc;
     if (out_bytes < info->out_bytes) return -14;
+    std::vector<float> tv;
+    if (p->rotate_x) {
+        tv = turnedVertices(verts, nV);
+        verts = tv.data();
+    }
     Plan pl = makePlan(p, verts, nV);
     applySpace(p, pl);
 #ifdef _OPENMP

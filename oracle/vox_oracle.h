@@ -64,6 +64,11 @@ typedef struct {
      * the reference's devices do; 0 = the whole grid. */
     int space;
     uint32_t part[4];
+    /* Slices along x (src/host_side.cpp:704-718, 1144-1223): the mesh is
+     * turned about z as rotateVertices does, the turned grid voxelized (with
+     * `part` in its coordinates) and a node result turned back before the
+     * boundary ids. */
+    int rotate_x;
 } orc_params;
 
 typedef struct {

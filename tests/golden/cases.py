@@ -116,10 +116,12 @@ def partition(c, res_y, res_z):
     if not sp:
         return None
     if sp[0] == "slice":
+        # direction 0 (x) slices the turned grid along its y (res_y, res_z of
+        # the turned grid then)
         _, direction, s = sp
-        n = res_y if direction == 1 else res_z
+        n = res_z if direction == 2 else res_y
         s0 = 0 if (s == 0 or s > n) else s - 1   # sliceOOB voxelizes row 0 (and zeroes the result)
-        return (s0, s0 + 1, 0, res_z) if direction == 1 else (0, res_y, s0, s0 + 1)
+        return (0, res_y, s0, s0 + 1) if direction == 2 else (s0, s0 + 1, 0, res_z)
     _, dy, dz, k = sp
     ys, zs = split_parts(res_y, dy), split_parts(res_z, dz)
     y, z = k % dy, k // dy
@@ -130,8 +132,14 @@ def slice_oob(c, res_y, res_z):
     sp = c.get("space")
     if not sp or sp[0] != "slice":
         return False
-    n = res_y if sp[1] == 1 else res_z
+    n = res_z if sp[1] == 2 else res_y
     return sp[2] == 0 or sp[2] > n
+
+
+def turned(c):
+    """True for slices along x, which voxelize the mesh turned about z."""
+    sp = c.get("space")
+    return bool(sp) and sp[0] == "slice" and sp[1] == 0
 
 
 CASES = [
@@ -188,6 +196,13 @@ CASES = [
     case("room_lite_long_part22_3", "room_lite", LONG, 1, 1, 160, space=("part", 2, 2, 3)),
     case("ico4_partial_part31_1", "ico4", PARTIAL, 1, 1, 1.0 / 64.0, strict_mats=False, space=("part", 3, 1, 1)),
     case("room_lite_bits_part13_1", "room_lite", LONG, 0, 0, 160, space=("part", 1, 3, 1)),
+    # Slices along x: the mesh turned about z, sliced along the turned y.
+    case("torus_long_slice_x_mid", "torus", LONG, 1, 1, 120, space=("slice", 0, 40)),
+    case("torus_short_slice_x_first", "torus", SHORT, 1, 1, 120, space=("slice", 0, 1)),
+    case("ico3_long_slice_x_splits", "ico3_mixed", LONG, 1, 1, 90, vox=(64, 16, 16), mat=(16, 16, 16),
+         strict_mats=False, space=("slice", 0, 45)),
+    case("torus_partial_slice_x", "torus", PARTIAL, 1, 1, 96, strict_mats=False, space=("slice", 0, 30)),
+    case("torus_long_slice_x_oob", "torus", LONG, 1, 1, 120, space=("slice", 0, 500)),
 ]
 
 BY_NAME = {c["name"]: c for c in CASES}

@@ -43,8 +43,8 @@ def load_ref():
     f.restype = ctypes.c_int
     f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_double,
                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
-                  ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
-                  ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]
+                  ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int,
+                  ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]
     lib.ref_last_error.restype = ctypes.c_char_p
     f.last_error = lambda: lib.ref_last_error().decode()
     return f
@@ -104,7 +104,8 @@ def run_case(f, c):
     args = [c["node_type"], c["nodes"], c["materials"], int(c["by_cube"]), md, cl, vs, ms,
             m.vertices.ctypes.data, m.n_vertices, m.indices.ctypes.data, m.n_triangles,
             mats.ctypes.data, m.n_materials]
-    rc = f(*args, None, None, 0, dims, None)
+    rot = int(C.turned(c))
+    rc = f(*args, None, rot, None, 0, dims, None)
     if rc != 0:
         raise RuntimeError(f"{c['name']}: plan failed rc={rc}")
     part, oob = None, False
@@ -112,10 +113,10 @@ def run_case(f, c):
         res_y, res_z = int(dims[1]) - 2, int(dims[2]) - 2
         part = (ctypes.c_uint32 * 4)(*C.partition(c, res_y, res_z))
         oob = C.slice_oob(c, res_y, res_z)
-        rc = f(*args, part, None, 0, dims, None)
+        rc = f(*args, part, rot, None, 0, dims, None)
         if rc != 0:
             raise RuntimeError(f"{c['name']}: plan failed rc={rc}")
-    args.append(part)
+    args += [part, rot]
     dt = C.out_dtype(c)
     n = int(dims[0]) * int(dims[1]) * int(dims[2])
     count = n // 32 if not c["nodes"] else n

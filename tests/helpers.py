@@ -86,13 +86,13 @@ def oracle_case(c, m, want_conflicts=True):
     slice past the grid is the zero array (sliceOOB)."""
     import cases as C
     import oracle as O
-    part, oob = None, False
+    part, oob, rot = None, False, C.turned(c)
     if c.get("space"):
-        pl = O.plan(m, c["node_type"], c["nodes"], c["size"], c["vox"])
+        pl = O.plan(m, c["node_type"], c["nodes"], c["size"], c["vox"], rotate_x=rot)
         ry, rz = int(pl.resolution[1]), int(pl.resolution[2])
         part, oob = C.partition(c, ry, rz), C.slice_oob(c, ry, rz)
     out, info, conf = O.voxelize(m, c["node_type"], c["nodes"], c["materials"], c["size"], c["vox"], c["mat"],
-                                 want_conflicts=want_conflicts, part=part)
+                                 want_conflicts=want_conflicts, part=part, rotate_x=rot)
     if oob:
         out[:] = 0
         if conf is not None:

@@ -17,9 +17,9 @@ from voxelizer_b200._lib import VxbError
 from voxelizer_b200.api import LONG, SHORT, SHORT_FCC, Voxelizer
 
 
-def _oracle_space(m, node_type, nodes, size, vox, mat, part, oob=False):
+def _oracle_space(m, node_type, nodes, size, vox, mat, part, oob=False, rotate_x=False):
     out, info, _ = O.voxelize(m, node_type, nodes, int(nodes and m.materials is not None), size, vox, mat,
-                              part=part)
+                              part=part, rotate_x=rotate_x)
     if oob:
         out[:] = 0
     return masked(node_type, nodes, out), info
@@ -28,8 +28,10 @@ def _oracle_space(m, node_type, nodes, size, vox, mat, part, oob=False):
 def test_slice_argument_errors():
     m = C.mesh("torus")
     with Voxelizer(m.vertices, m.indices, node_type=LONG) as v:
-        with pytest.raises(VxbError, match="EUNSUPPORTED"):
-            v.planSlice(120, 0, 5)
+        info = v.planSlice(120, 0, 5)   # x: the turned grid sliced along its y, turned back
+        assert info.dims[0] == 3 and tuple(info.partition)[:2] == (4, 5)
+        turned = v.getArrayDimensions(120, 1024, True)
+        assert (info.dims[1], info.dims[2]) == (turned[1], turned[2])
         with pytest.raises(VxbError, match="EINVAL"):
             v.planSlice(120, 3, 5)
         info = v.planSlice(120, 1, 7)
@@ -51,23 +53,25 @@ def test_slice_argument_errors():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("direction", [1, 2])
+@pytest.mark.parametrize("direction", [0, 1, 2])
 def test_slice_sweep_matches_oracle(direction):
     m = C.mesh("torus")
     size, vox, mat = 64, (1024, 512, 512), (512, 512, 512)
+    rot = direction == 0   # slices along x cut the turned grid along its y
+    res = O.plan(m, LONG, 1, size, vox, rotate_x=rot).resolution
+    ry, rz = int(res[1]), int(res[2])
+    n = rz if direction == 2 else ry
     with Voxelizer(m.vertices, m.indices, node_type=LONG) as v:
         v.setMaterials(m.materials, m.n_materials)
-        full = v.plan(1, size)
-        n = full.resolution.y if direction == 1 else full.resolution.z
         for s in [0, 1, 2, n // 3, n // 2, n - 1, n, n + 1]:
             got, info = v.voxelizeSliceToRAM(size, direction, s, vox, mat)
             s0 = 0 if (s == 0 or s > n) else s - 1
-            part = (s0, s0 + 1, 0, full.resolution.z) if direction == 1 else (0, full.resolution.y, s0, s0 + 1)
-            want, _ = _oracle_space(m, LONG, 1, size, vox, mat, part, oob=(s == 0 or s > n))
+            part = (0, ry, s0, s0 + 1) if direction == 2 else (s0, s0 + 1, 0, rz)
+            want, _ = _oracle_space(m, LONG, 1, size, vox, mat, part, oob=(s == 0 or s > n), rotate_x=rot)
             assert np.array_equal(got, want), f"slice {s} along {direction}"
             X, Y, Z = info.dims
             g = got.reshape(Z, Y, X)
-            outer = g[:, [0, 2], :] if direction == 1 else g[[0, 2], :, :]
+            outer = g[:, :, [0, 2]] if direction == 0 else g[:, [0, 2], :] if direction == 1 else g[[0, 2], :, :]
             assert not outer.any(), "outer layers of a slice are zero"
 
 

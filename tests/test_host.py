@@ -52,10 +52,15 @@ def test_plan_matches_golden_dims(name):
         else:
             info = full
     assert info.dims == tuple(INDEX[name]["dims"])
-    part = C.partition(c, int(full.resolution.y), int(full.resolution.z))
+    rot = C.turned(c)
+    if rot:   # slices along x partition the turned grid
+        tp = O.plan(m, c["node_type"], c["nodes"], c["size"], c["vox"], rotate_x=True)
+        part = C.partition(c, int(tp.resolution[1]), int(tp.resolution[2]))
+    else:
+        part = C.partition(c, int(full.resolution.y), int(full.resolution.z))
     if part:
         assert tuple(info.partition) == part
-    oi = O.plan(m, c["node_type"], c["nodes"], c["size"], c["vox"], part=part)
+    oi = O.plan(m, c["node_type"], c["nodes"], c["size"], c["vox"], part=part, rotate_x=rot)
     assert info.dims == tuple(oi.dims)
     assert info.voxel_length == oi.voxel_length
     assert info.x_splits == oi.x_splits
@@ -100,5 +105,13 @@ def test_array_dimensions_match_plan():
             d = v.getArrayDimensions(1.0 / 100.0, 1024, False)
             info = v.plan(1, 1.0 / 100.0)
             assert d == info.dims
-            with pytest.raises(_lib.VxbError):
-                v.getArrayDimensions(1.0 / 100.0, 1024, True)
+            if nt >= 3:   # FCC lattices are not turned
+                with pytest.raises(_lib.VxbError):
+                    v.getArrayDimensions(1.0 / 100.0, 1024, True)
+                continue
+            # sliceAlongX: the turned mesh's grid with x and y exchanged
+            # (src/host_side.cpp:3333-3371)
+            t = O.plan(m, nt, 1, 1.0 / 100.0, rotate_x=True).dims
+            assert v.getArrayDimensions(1.0 / 100.0, 1024, True) == (t[1], t[0], t[2])
+            t = O.plan(m, nt, 1, 90, rotate_x=True).dims
+            assert v.getArrayDimensions(90, 1024, True) == (t[1], t[0], t[2])

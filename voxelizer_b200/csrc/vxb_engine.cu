@@ -44,6 +44,10 @@ struct vxb_voxelizer {
     bool meshOnDevice = false, matsOnDevice = false;
     bool hasMaterials = false;   // setMaterials was called (materials live on the host or the device)
     vxb::DevBuf dV, dI, dM, outStage;
+    // Slices along x: the rotated mesh (made on the first such call) and the
+    // rotated slice's node array before the boundary ids.
+    vxb::DevBuf dVrot, xStage, xFlag;
+    bool rotOnDevice = false;
     vxb::Pipeline pipe;
     vxb::StageTimer timer;
     uint32_t launches = 0;
@@ -54,8 +58,9 @@ struct vxb_voxelizer {
     bool busy = false;
 
     int plan(int nodes, const vxb_request* r, vxb::Plan& p, vxb_grid_info* info) const;
-    // The request's plan of the whole grid, without the output size checks.
-    int fullPlan(const vxb_request* r, vxb::Plan& p) const;
+    // The request's plan of the whole grid, without the output size checks
+    // (of the mesh's bounding box, or of bmn / bmx).
+    int fullPlan(const vxb_request* r, vxb::Plan& p, const double* bmn = nullptr, const double* bmx = nullptr) const;
     // Combinations the reference refuses (src/host_side.cpp:568-573,
     // 1744-1749, 1836-1841, 2280-2285) and missing materials.
     int validate(int nodes, const vxb_request* r) const {
@@ -91,14 +96,24 @@ struct vxb_voxelizer {
     // The device space of a slice (src/host_side.cpp:748-779): *oob for a
     // slice 0 or past the grid, whose result is all zeros.
     int sliceSpace(const vxb_request* r, int direction, uint32_t slice, Space* sp, bool* oob) const;
+    // Slices along x: rotateVertices (src/host_side.cpp:3261-3280) turns the
+    // mesh about z (x' = a - y, y' = b + x in double, rounded to float) and
+    // the rotated grid is sliced along y.  `rotation` gives a, b and the
+    // rotated bounding box (float rounding is monotone, so the box's corners
+    // are the rotated corners of the original box); planXSlice the rotated
+    // slice's device space and the un-rotated result's shape.
+    void rotation(double* a, double* b, double* rmn, double* rmx) const;
+    int planXSlice(const vxb_request* r, uint32_t slice, vxb::Plan* q, bool* oob, vxb_grid_info* info) const;
+    int runXSlice(const vxb_request* r, uint32_t slice, void* out, uint64_t bytes, cudaStream_t s,
+                  vxb_grid_info* info);
 };
 
-int vxb_voxelizer::fullPlan(const vxb_request* r, vxb::Plan& p) const {
+int vxb_voxelizer::fullPlan(const vxb_request* r, vxb::Plan& p, const double* bmn, const double* bmx) const {
     if (!r) return failf(VXB_EINVAL, "request is NULL");
     if (nV == 0 || nT == 0) return failf(VXB_EINVAL, "empty mesh");
     const uint32_t vs[3] = {r->vox_split_res.x, r->vox_split_res.y, r->vox_split_res.z};
     const uint32_t ms[3] = {r->mat_split_res.x, r->mat_split_res.y, r->mat_split_res.z};
-    if (vxb::makePlan(mn, mx, r->by_cube_length, r->max_dimension, r->cube_length, vs, ms, p))
+    if (vxb::makePlan(bmn ? bmn : mn, bmx ? bmx : mx, r->by_cube_length, r->max_dimension, r->cube_length, vs, ms, p))
         return failf(VXB_EINVAL, "invalid request (maxDimension >= 2 or cubeLength > 0, split sizes > 0 and an x "
                                  "pass of at most 1024 voxels are required)");
     return 0;
@@ -293,9 +308,117 @@ int vxb_voxelizer::partitions(const vxb_request* r, uint32_t devY, uint32_t devZ
     return 0;
 }
 
+void vxb_voxelizer::rotation(double* a, double* b, double* rmn, double* rmx) const {
+    const double cx = (mx[0] - mn[0]) / 2.0, cy = (mx[1] - mn[1]) / 2.0;
+    *a = cy + cx;
+    *b = cy - cx;
+    rmn[0] = (double)(float)(*a - mx[1]);
+    rmx[0] = (double)(float)(*a - mn[1]);
+    rmn[1] = (double)(float)(*b + mn[0]);
+    rmx[1] = (double)(float)(*b + mx[0]);
+    rmn[2] = mn[2];
+    rmx[2] = mx[2];
+}
+
+int vxb_voxelizer::planXSlice(const vxb_request* r, uint32_t slice, vxb::Plan* q, bool* oob,
+                              vxb_grid_info* info) const {
+    if (isFcc(nodeType)) return failf(VXB_EUNSUPPORTED, "device spaces of FCC lattices are not supported");
+    double a, b, rmn[3], rmx[3];
+    rotation(&a, &b, rmn, rmx);
+    vxb::Plan full;
+    int rc = fullPlan(r, full, rmn, rmx);
+    if (rc) return rc;
+    *oob = slice == 0 || slice > full.res[1];
+    const uint32_t s0 = *oob ? 0u : slice - 1;
+    const uint32_t vs[3] = {r->vox_split_res.x, r->vox_split_res.y, r->vox_split_res.z};
+    const uint32_t ms[3] = {r->mat_split_res.x, r->mat_split_res.y, r->mat_split_res.z};
+    if (vxb::devicePlan(full, s0, s0 + 1, 0, full.res[2], vs, ms, *q))
+        return failf(VXB_EINVAL, "slice outside the grid");
+    vxb_grid_info gi;
+    if ((rc = vxb::gridInfo(*q, nodeType, 1, &gi))) return rc;
+    // The un-rotated array: x and y trade places (unRotateCoords,
+    // src/host_side.cpp:1160-1175).
+    const uint32_t t = gi.dim.x;
+    gi.dim.x = gi.dim.y;
+    gi.dim.y = t;
+    gi.location = vxb_uint3{0, 0, 0};
+    if (info) *info = gi;
+    return 0;
+}
+
+int vxb_voxelizer::runXSlice(const vxb_request* r, uint32_t slice, void* out, uint64_t bytes, cudaStream_t s,
+                             vxb_grid_info* info) {
+    vxb::Plan q;
+    bool oob = false;
+    vxb_grid_info gi;
+    int rc = planXSlice(r, slice, &q, &oob, &gi);
+    if (rc) return rc;
+    if (info) *info = gi;
+    if ((rc = validate(1, r))) return rc;
+    if (!out || bytes < gi.bytes) return failf(VXB_EINVAL, "output buffer is NULL or too small");
+    VXB_CUDA(cudaSetDevice(device));
+    launches = 0;
+    timer.reset();
+    if (oob) {   // sliceOOB (src/host_side.cpp:1225-1236)
+        VXB_CUDA(cudaMemsetAsync(out, 0, gi.bytes, s));
+        VXB_CUDA(cudaStreamSynchronize(s));
+        return VXB_OK;
+    }
+    busy = true;
+    if ((rc = upload(s))) return rc;
+    double a, b, rmn[3], rmx[3];
+    rotation(&a, &b, rmn, rmx);
+    if (!rotOnDevice) {
+        if ((rc = dVrot.ensure(sizeof(float) * 3 * (size_t)nV))) return rc;
+        vxb::launch_rotate_vertices(dV.as<float>(), dVrot.as<float>(), nV, a, b, s, &launches);
+        VXB_CUDA(cudaGetLastError());
+        rotOnDevice = true;
+    }
+    if ((rc = xStage.ensure(gi.bytes))) return rc;
+    if ((rc = xFlag.ensure(4))) return rc;
+    vxb::MeshJob j;
+    job(1, r, xStage.p, gi.bytes, &j);
+    j.V = dVrot.as<float>();
+    for (int k = 0; k < 3; ++k) {
+        j.mn[k] = rmn[k];
+        j.mx[k] = rmx[k];
+    }
+    j.space = 1;
+    for (int k = 0; k < 4; ++k) j.part[k] = q.part[k];
+    j.raw = 1;
+    if ((rc = pipe.prepare(std::vector<vxb::MeshJob>{j}, s))) return rc;
+    if ((rc = pipe.enqueue(s, &timer))) return rc;
+    if ((rc = pipe.finish(s))) return rc;
+    launches += pipe.launches;
+    // restoreRotatedNodes, then fillNodeList2 over the un-rotated array one
+    // yz subspace at a time until no node loses its id, then zeroPadding
+    // (src/host_side.cpp:1144-1223).
+    const uint32_t nb = (uint32_t)(gi.bytes / gi.count);
+    const uint32_t X = q.alloc[0], Y = q.alloc[1], Z = q.alloc[2];
+    vxb::launch_unrotate(xStage.p, out, X, Y, Z, nb, s, &launches);
+    const uint32_t idMask = nodeType == VXB_SHORT_NODE ? 31u : 255u;
+    const std::vector<vxb::Range> ys = vxb::splitLength(X, r->vox_split_res.y);
+    const std::vector<vxb::Range> zs = vxb::splitLength(Z, r->vox_split_res.z);
+    uint32_t* flag = xFlag.as<uint32_t>();
+    for (const vxb::Range& zr : zs)
+        for (const vxb::Range& yr : ys)
+            for (uint64_t pass = 0;; ++pass) {
+                if (pass > (uint64_t)Y * X * Z) return failf(VXB_ETIMEDOUT, "boundary ids did not converge");
+                VXB_CUDA(cudaMemsetAsync(flag, 0, 4, s));
+                vxb::launch_id_pass(out, Y, X, Z, nb, idMask, yr.lo, yr.hi, zr.lo, zr.hi, flag, s, &launches);
+                uint32_t h = 0;
+                VXB_CUDA(cudaMemcpyAsync(&h, flag, 4, cudaMemcpyDeviceToHost, s));
+                VXB_CUDA(cudaStreamSynchronize(s));
+                if (!h) break;
+            }
+    if (q.border) vxb::launch_zero_faces(out, Y, X, Z, nb, s, &launches);
+    VXB_CUDA(cudaGetLastError());
+    VXB_CUDA(cudaStreamSynchronize(s));
+    busy = false;
+    return VXB_OK;
+}
+
 int vxb_voxelizer::sliceSpace(const vxb_request* r, int direction, uint32_t slice, Space* sp, bool* oob) const {
-    if (direction == 0)
-        return failf(VXB_EUNSUPPORTED, "slicing along x is not supported; rotate the model and slice along y or z");
     if (direction != 1 && direction != 2) return failf(VXB_EINVAL, "slice direction must be 0, 1 or 2");
     vxb::Plan full;
     int rc = fullPlan(r, full);
@@ -433,7 +556,26 @@ vxb_status vxb_plan(vxb_voxelizer* v, int nodes, const vxb_request* req, vxb_gri
 vxb_status vxb_get_array_dimensions(vxb_voxelizer* v, int by_cube_length, uint32_t max_dimension, double cube_length,
                                     uint32_t max_internal_x, int slice_along_x, vxb_uint3* dims) {
     if (!v || !dims) return failf(VXB_EINVAL, "NULL argument");
-    if (slice_along_x) return failf(VXB_EUNSUPPORTED, "slicing along x is not part of this library");
+    if (slice_along_x) {
+        // src/host_side.cpp:3333-3371: the rotated mesh's grid (padding
+        // included), its corners un-rotated: x and y trade places.
+        if (isFcc(v->nodeType)) return failf(VXB_EUNSUPPORTED, "sliceAlongX of FCC lattices is not supported");
+        vxb_request r;
+        r.by_cube_length = by_cube_length;
+        r.max_dimension = max_dimension;
+        r.cube_length = cube_length;
+        r.vox_split_res = vxb_uint3{max_internal_x, 512, 512};
+        r.mat_split_res = vxb_uint3{512, 512, 512};
+        double a, b, rmn[3], rmx[3];
+        v->rotation(&a, &b, rmn, rmx);
+        vxb::Plan p;
+        int rc = v->fullPlan(&r, p, rmn, rmx);
+        if (rc) return rc;
+        dims->x = p.alloc[1];
+        dims->y = p.alloc[0];
+        dims->z = p.alloc[2];
+        return VXB_OK;
+    }
     vxb_request r;
     r.by_cube_length = by_cube_length;
     r.max_dimension = max_dimension;
@@ -513,6 +655,11 @@ vxb_status vxb_voxelize_parts_to_host(vxb_voxelizer* v, int nodes, const vxb_req
 vxb_status vxb_plan_slice(vxb_voxelizer* v, const vxb_request* req, int direction, uint32_t slice,
                           vxb_grid_info* info) {
     if (!v || !info) return failf(VXB_EINVAL, "NULL argument");
+    if (direction == 0) {
+        vxb::Plan q;
+        bool oob = false;
+        return v->planXSlice(req, slice, &q, &oob, info);
+    }
     vxb_voxelizer::Space sp;
     bool oob = false;
     int rc = v->sliceSpace(req, direction, slice, &sp, &oob);
@@ -523,6 +670,8 @@ vxb_status vxb_plan_slice(vxb_voxelizer* v, const vxb_request* req, int directio
 vxb_status vxb_voxelize_slice_to_device(vxb_voxelizer* v, const vxb_request* req, int direction, uint32_t slice,
                                         void* dev_out, uint64_t dev_bytes, void* stream, vxb_grid_info* info) {
     if (!v) return failf(VXB_EINVAL, "voxelizer is NULL");
+    if (direction == 0)
+        return v->runXSlice(req, slice, dev_out, dev_bytes, reinterpret_cast<cudaStream_t>(stream), info);
     vxb_voxelizer::Space sp;
     bool oob = false;
     int rc = v->sliceSpace(req, direction, slice, &sp, &oob);

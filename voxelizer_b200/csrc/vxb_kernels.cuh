@@ -137,6 +137,22 @@ void launch_prune_list(const Batch& b, const PruneRegion* regions, uint32_t* sol
                        const uint32_t* surf, uint32_t* flags, uint32_t flagBase, uint32_t passes, uint32_t pass,
                        const unsigned long long* in, const uint32_t* inCount, unsigned long long* out,
                        uint32_t* outCount, uint32_t cap, uint32_t* overflow, cudaStream_t s, uint32_t* launches);
+// Slices along x (vxb_xslice.cu): vertex rotation, the node array before
+// the boundary ids, un-rotation, one in-place boundary-id pass over a yz
+// subspace (sets *changed when a node loses its id) and face zeroing.  The
+// node kernels treat nodes as `nodeBytes` bytes with the id in byte 0
+// (masked by idMask).
+void launch_rotate_vertices(const float* V, float* R, uint32_t n, double a, double b, cudaStream_t s,
+                            uint32_t* launches);
+void launch_emit_raw(int nodeKind, const Batch& b, uint64_t totalWords, const uint32_t* fill, const uint32_t* surf,
+                     const uint32_t* ranks, const void* keys, uint32_t keysCap, cudaStream_t s, uint32_t* launches);
+void launch_unrotate(const void* in, void* out, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nodeBytes,
+                     cudaStream_t s, uint32_t* launches);
+void launch_id_pass(void* nodes, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nodeBytes, uint32_t idMask,
+                    uint32_t y0, uint32_t y1, uint32_t z0, uint32_t z1, uint32_t* changed, cudaStream_t s,
+                    uint32_t* launches);
+void launch_zero_faces(void* nodes, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nodeBytes, cudaStream_t s,
+                       uint32_t* launches);
 // Keys at ranks >= keysCap read as 0.
 void launch_emit_cartesian(int nodeKind, const Batch& b, uint64_t totalWords, const uint32_t* finalSolid,
                            const uint32_t* fill, const uint32_t* surf, const uint32_t* ranks, const void* keys,

@@ -134,6 +134,10 @@ int Pipeline::prepare(const std::vector<MeshJob>& jobs, cudaStream_t s) {
             return failf(VXB_EINVAL, "all meshes of a batch need the same node type and output kind");
     const bool fcc = isFccType(nodeKind_);
     wide_ = nodeKind_ == VXB_PARTIAL_NODE;
+    raw_ = jobs[0].raw != 0;
+    for (const MeshJob& j : jobs)
+        if ((j.raw != 0) != raw_ || (raw_ && (!j.nodes || fcc)))
+            return failf(VXB_EINVAL, "raw node output is for Cartesian node grids of a whole batch");
     units_.clear();
     groups_.clear();
     std::vector<uint32_t> workBase{0};
@@ -359,7 +363,7 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
         mark(1, true);
     }
     // Split-ordered pruning (src/host_side.cpp:1183-1206).
-    if (anyCartesian_) {
+    if (anyCartesian_ && !raw_) {
         mark(2, false);
         if (anyMaterials_)
             launch_combine(fillP, surf.as<uint32_t>(), fin.as<uint32_t>(), totalWords_, s, &launches);
@@ -402,7 +406,10 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
     }
     // Node emission.
     mark(3, false);
-    if (anyCartesian_)
+    if (raw_)
+        launch_emit_raw(nodeKind_, b, totalWords_, fillP, surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_,
+                        s, &launches);
+    else if (anyCartesian_)
         launch_emit_cartesian(nodeKind_, b, totalWords_, fin.as<uint32_t>(), fillP, surf.as<uint32_t>(),
                               ranks.as<uint32_t>(), keys.p, keysCap_, s, &launches);
     if (nFcc_)
@@ -485,7 +492,7 @@ int Pipeline::finish(cudaStream_t s) {
             reemit = true;
         }
     }
-    if (anyCartesian_) {
+    if (anyCartesian_ && !raw_) {
         // The first subspace index with a region that changed in its last
         // queued pass has not converged; it and every later index (pruned
         // against a superset of its final state) get passes until stable.
@@ -505,7 +512,10 @@ int Pipeline::finish(cudaStream_t s) {
         }
     }
     if (reemit) {
-        if (anyCartesian_)
+        if (raw_)
+            launch_emit_raw(nodeKind_, b, totalWords_, fillP, surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p,
+                            keysCap_, s, &launches);
+        else if (anyCartesian_)
             launch_emit_cartesian(nodeKind_, b, totalWords_, fin.as<uint32_t>(), fillP, surf.as<uint32_t>(),
                                   ranks.as<uint32_t>(), keys.p, keysCap_, s, &launches);
         if (nFcc_)

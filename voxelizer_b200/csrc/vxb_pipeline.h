@@ -29,6 +29,10 @@ struct MeshJob {
     // = 1); 0 = the whole grid.
     int space = 0;
     uint32_t part[4] = {0, 0, 0, 0};
+    // Node output as it stands before the boundary ids (bid = solid bit,
+    // surface material and ratio), no pruning: the first half of a slice
+    // along x.  All jobs of a batch share it.
+    int raw = 0;
 };
 
 // Shape of a job's result (vxb_plan).  Returns 0 or a vxb status.
@@ -83,7 +87,7 @@ private:
     uint32_t nWork_ = 0, nRegions_ = 0, nFcc_ = 0;
     uint64_t totalWords_ = 0, totalRows_ = 0, totalGroups_ = 0;
     int nodeKind_ = 0, nodes_ = 1;
-    bool anyMaterials_ = false, anyCartesian_ = false, wide_ = false, aliasFill_ = false;
+    bool anyMaterials_ = false, anyCartesian_ = false, wide_ = false, aliasFill_ = false, raw_ = false;
     uint32_t listCap_ = 0, keysCap_ = 0, pruneCap_ = 0;
     // table offsets (bytes) in `tables`
     size_t oUnits_ = 0, oWork_ = 0, oRow_ = 0, oWord_ = 0, oSplits_ = 0, oSlices_ = 0, oLater_ = 0, oRegions_ = 0,

@@ -86,7 +86,7 @@ __device__ __forceinline__ bool outside(float t) { return t < 0.0f || t > 1.0f; 
 
 // Volume of voxel (x, y, z) (node coordinates) behind the plane through t0
 // with normal n.
-__device__ __noinline__ float cutVolume(F3 t0, F3 n, int x, int y, int z, F3 m, float d) {
+static __device__ __noinline__ float cutVolume(F3 t0, F3 n, int x, int y, int z, F3 m, float d) {
     const F3 vc = add(m, mul(d, F3{float(x), float(y), float(z)}));
     if (fabsf(n.x) == 1.0f) return (d * d) * ((d / 2.0f) + t0.x - vc.x);
     if (fabsf(n.y) == 1.0f) return (d * d) * ((d / 2.0f) + t0.y - vc.y);
