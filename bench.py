@@ -337,6 +337,12 @@ def run_batched(args, world, rank, local):
         torch.cuda.synchronize()
         return sum(a.elapsed_time(b) for a, b in evs) / steps
 
+    def tune_calls():
+        loop()
+        batch.run(stream=sh, graph=False)
+        stream.synchronize()
+
+    tuned = autotune(args, tune_calls)
     for _ in range(args.warmup):
         loop()
         batch.run(stream=sh, graph=True)
@@ -355,7 +361,8 @@ def run_batched(args, world, rank, local):
             "data": f"synthetic (seeded {args.batch_meshes}-mesh mix: icospheres/tori, 500-500k triangles, "
                     "maxDimension 32-512, 1-16 materials)",
             "config": {"workload": f"{args.batch_meshes} meshes, {n_tris:,} triangles, {n_nodes:,} nodes per step",
-                       "parallelism": f"replicas x{world}", "l2": "outputs of one step exceed the L2"},
+                       "parallelism": f"replicas x{world}", "l2": "outputs of one step exceed the L2",
+                       "autotune": tuned if tuned is not None else "off"},
             "per_mesh_loop": {"value": round(args.batch_meshes * world / (t_loop * 1e-3), 2), "unit": "meshes/s",
                               "ms_per_step": round(t_loop, 3)},
             "speedup_vs_loop": round(t_loop / t_batch, 3),
@@ -487,6 +494,20 @@ def run_served(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def autotune(args, call, rounds=8):
+    """With --autotune on: switch the launch-shape tuner on and make
+    `rounds` untimed calls (3 candidate shapes x 2 samples settle a size
+    bucket); returns the settled shapes (None when off)."""
+    if args.autotune != "on":
+        return None
+    from voxelizer_b200 import _lib
+    _lib.set_autotune(1)
+    for _ in range(rounds):
+        call()
+    shapes = json.loads(_lib.autotune_state()[1])
+    return shapes if len(shapes) <= 2 else {"buckets": len(shapes), "untimed_tuning_calls": rounds}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -501,6 +522,9 @@ def main():
     ap.add_argument("--batch-meshes", type=int, default=256)
     ap.add_argument("--serve-seconds", type=float, default=1.5)
     ap.add_argument("--serve-max-requests", type=int, default=3000)
+    ap.add_argument("--autotune", default="on", choices=["off", "on"],
+                    help="on: tune launch shapes per size bucket in untimed calls before the warm-up "
+                         "(results do not depend on the shapes)")
     ap.add_argument("--profile-run", type=int, default=0, metavar="MAXDIM",
                     help="no timing: voxelize the room scene at this maxDimension --steps times (a target for ncu)")
     args = ap.parse_args()
@@ -541,6 +565,7 @@ def main():
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
     vx.set_profiling(True)
+    tuned = autotune(args, lambda: (vx.voxelize_device(1, MAX_DIM, out, stream=sh), stream.synchronize()))
     for _ in range(args.warmup):
         vx.voxelize_device(1, MAX_DIM, out, stream=sh)
     stream.synchronize()
@@ -624,7 +649,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64+f32+u32", "data": "synthetic (seeded room scene)",
             "config": {"workload": WORKLOAD, "l2": "256 MB flush before every timed step",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"replicas x{world}", "autotune": tuned if tuned is not None else "off"},
             "roofline": roofs[0],
             "roofline_next_kernel": roofs[1],
             "work": stats,

@@ -179,6 +179,23 @@ vxb_status vxb_voxelize_slice_to_device(vxb_voxelizer* v, const vxb_request* req
 vxb_status vxb_voxelize_slice_to_host(vxb_voxelizer* v, const vxb_request* req, int direction, uint32_t slice,
                                       void* host_out, uint64_t host_bytes, vxb_grid_info* info);
 
+/* Launch-shape autotuner (no reference counterpart).  Several kernels can
+ * spread their work over the GPU in different ways (grid size, work items
+ * per warp) with identical results; the best shape depends on the size of
+ * the job.  mode 0: fixed default shapes; 1: tune online: the first calls of
+ * each size bucket (work triangles, grid words, node type, material output)
+ * try candidate shapes, timing each tuned kernel with CUDA events, and after
+ * two samples per candidate every kernel keeps its fastest shape; calls
+ * captured into a CUDA graph never run trials; 2: use the shapes read from
+ * `cache_path` and the defaults elsewhere.  With a `cache_path`, settled
+ * shapes are read from it when the mode is set and written back (JSON, one
+ * bucket per line) as buckets settle.  Process-wide; resets what was
+ * learned before. */
+vxb_status vxb_set_autotune(int mode, const char* cache_path);
+/* Buckets settled so far and their shapes as JSON (truncated to
+ * json_bytes - 1 characters; NULL to skip). */
+vxb_status vxb_autotune_state(uint32_t* settled, char* json, uint64_t json_bytes);
+
 /* Number of kernels the last voxelize call launched on the device. */
 vxb_status vxb_last_launch_count(vxb_voxelizer* v, uint32_t* launches);
 

@@ -27,7 +27,8 @@ EXPORTS = ["vxb_last_error", "vxb_version", "vxb_create", "vxb_destroy", "vxb_se
            "vxb_stage_times", "vxb_voxelize_bits_noalloc", "vxb_trim_cache", "vxb_batch_create",
            "vxb_batch_destroy", "vxb_batch_add", "vxb_batch_clear", "vxb_batch_run", "vxb_batch_last_launch_count",
            "vxb_last_stats", "vxb_plan_parts", "vxb_voxelize_parts_to_device", "vxb_voxelize_parts_to_host",
-           "vxb_plan_slice", "vxb_voxelize_slice_to_device", "vxb_voxelize_slice_to_host"]
+           "vxb_plan_slice", "vxb_voxelize_slice_to_device", "vxb_voxelize_slice_to_host", "vxb_set_autotune",
+           "vxb_autotune_state"]
 
 BATCH_GRAPH = 1
 
@@ -114,6 +115,8 @@ def lib():
                                                         P(GridInfo)]),
         "vxb_voxelize_parts_to_host": (ctypes.c_int, [vp, ctypes.c_int, P(Request), ctypes.c_uint32,
                                                       ctypes.c_uint32, P(vp), P(ctypes.c_uint64), P(GridInfo)]),
+        "vxb_set_autotune": (ctypes.c_int, [ctypes.c_int, ctypes.c_char_p]),
+        "vxb_autotune_state": (ctypes.c_int, [P(ctypes.c_uint32), ctypes.c_char_p, ctypes.c_uint64]),
         "vxb_plan_slice": (ctypes.c_int, [vp, P(Request), ctypes.c_int, ctypes.c_uint32, P(GridInfo)]),
         "vxb_voxelize_slice_to_device": (ctypes.c_int, [vp, P(Request), ctypes.c_int, ctypes.c_uint32, vp,
                                                         ctypes.c_uint64, vp, P(GridInfo)]),
@@ -149,3 +152,17 @@ def make_request(size, vox_split=(1024, 512, 512), mat_split=(512, 512, 512)):
     r.vox_split_res = Uint3(*[int(v) for v in vox_split])
     r.mat_split_res = Uint3(*[int(v) for v in mat_split])
     return r
+
+
+def set_autotune(mode, cache_path=None):
+    """vxb_set_autotune: 0 default launch shapes, 1 tune online, 2 use the
+    cache file's shapes."""
+    check(lib().vxb_set_autotune(int(mode), cache_path.encode() if cache_path else None))
+
+
+def autotune_state():
+    """(settled buckets, JSON text of their shapes)."""
+    n = ctypes.c_uint32()
+    buf = ctypes.create_string_buffer(1 << 16)
+    check(lib().vxb_autotune_state(ctypes.byref(n), buf, len(buf)))
+    return int(n.value), buf.value.decode()

@@ -70,8 +70,10 @@ void launch_scan(const uint32_t* in, uint32_t* offsets, uint32_t n, uint32_t* bl
 // Candidates per work triangle, the toggles of the listed candidates into
 // the `fill` arena, then the row prefix XOR over all rows of the batch.
 void launch_solid_count(const Batch& b, uint32_t nWork, uint32_t* counts, cudaStream_t s, uint32_t* launches);
+// blocksPerSm: launch shape (the autotuner's choice; results do not depend
+// on it), here and in the launchers below that take one.
 void launch_solid_toggle(const Batch& b, uint32_t nWork, const uint32_t* offsets, const uint32_t* total,
-                         uint32_t* fill, cudaStream_t s, uint32_t* launches);
+                         uint32_t* fill, uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches);
 void launch_row_fill(const Batch& b, uint64_t nRows, uint32_t* fill, cudaStream_t s, uint32_t* launches);
 
 // ---- Surface voxelization: src/voxelizer.cu:2358-2989, 3040-4201 ----
@@ -97,8 +99,8 @@ void launch_surface_prepare(const Batch& b, uint32_t nWork, uint32_t* codes, uin
 void launch_surface_work(int mode, int wide, const Batch& b, const void* recs, const void* ovl,
                          const uint32_t* offsets, uint32_t nWork, const uint32_t* total, const uint32_t* buckets,
                          uint32_t* surf, const uint32_t* ranks, void* keys, uint32_t keysCap,
-                         unsigned long long* list, uint32_t* listCount, uint32_t listCap, cudaStream_t s,
-                         uint32_t* launches);
+                         unsigned long long* list, uint32_t* listCount, uint32_t listCap, uint32_t blocksPerSm,
+                         uint32_t batch, cudaStream_t s, uint32_t* launches);
 // Exclusive popcount prefix over `words` surface words; *total = surface voxels.
 void launch_surface_rank(const uint32_t* bits, uint64_t words, uint32_t* ranks, uint32_t* tileSums, uint32_t* total,
                          cudaStream_t s, uint32_t* launches);
@@ -108,7 +110,7 @@ void launch_surface_keys_zero(void* keys, const uint32_t* count, uint32_t cap, i
 // Keys at ranks >= keysCap are dropped (the host re-merges after growing).
 void launch_surface_merge(const unsigned long long* list, const uint32_t* listCount, uint32_t listCap,
                           const uint32_t* bits, const uint32_t* ranks, uint32_t* keys, uint32_t keysCap,
-                          cudaStream_t s, uint32_t* launches);
+                          uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches);
 
 // ---- Node classification: src/voxelizer.cu:1626-2048 ----
 void launch_combine(const uint32_t* a, const uint32_t* b, uint32_t* out, uint64_t n, cudaStream_t s,
@@ -156,7 +158,7 @@ void launch_zero_faces(void* nodes, uint32_t X, uint32_t Y, uint32_t Z, uint32_t
 // Keys at ranks >= keysCap read as 0.
 void launch_emit_cartesian(int nodeKind, const Batch& b, uint64_t totalWords, const uint32_t* finalSolid,
                            const uint32_t* fill, const uint32_t* surf, const uint32_t* ranks, const void* keys,
-                           uint32_t keysCap, cudaStream_t s, uint32_t* launches);
+                           uint32_t keysCap, uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches);
 
 // An FCC mesh: its four sub-lattice units are units [unit0, unit0 + 4).
 struct FccMesh {

@@ -582,7 +582,7 @@ void launch_prune_list(const Batch& b, const PruneRegion* regions, uint32_t* sol
 
 void launch_emit_cartesian(int nodeKind, const Batch& b, uint64_t totalWords, const uint32_t* finalSolid,
                            const uint32_t* fill, const uint32_t* surf, const uint32_t* ranks, const void* keys,
-                           uint32_t keysCap, cudaStream_t s, uint32_t* launches) {
+                           uint32_t keysCap, uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches) {
     EmitArgs a;
     a.keysCap = keysCap;
     a.b = b;
@@ -591,7 +591,7 @@ void launch_emit_cartesian(int nodeKind, const Batch& b, uint64_t totalWords, co
     a.surf = surf;
     a.ranks = ranks;
     a.keys = keys;
-    const uint32_t grid = gridFor(totalWords, 256, 148u * 16u);
+    const uint32_t grid = gridFor(totalWords, 256, 148u * blocksPerSm);
     switch (nodeKind) {
     case kShort: emitNarrowKernel<kShort><<<grid, 256, 0, s>>>(a, totalWords); break;
     case kLong: emitNarrowKernel<kLong><<<grid, 256, 0, s>>>(a, totalWords); break;

@@ -325,13 +325,23 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
     auto mark = [&](int stage, bool end) {
         if (timer) timer->mark(stage, end, s);
     };
+    // Launch shapes of this run; tuning trials are timed per kernel (not
+    // while a graph is being captured).
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    VXB_CUDA(cudaStreamIsCapturing(s, &cap));
+    bucket_ = tuneBucket(nWork_, totalWords_, nodeKind_, anyMaterials_);
+    shape = tunePick(bucket_, &trial_, cap == cudaStreamCaptureStatusNone);
+    for (bool& u : tuneUsed_) u = false;
     // Solid voxelization.
     mark(0, false);
     VXB_CUDA(cudaMemsetAsync(fillP, 0, wordBytes, s));
     launch_solid_count(b, nWork_, counts.as<uint32_t>(), s, &launches);
     launch_scan(counts.as<uint32_t>(), offsets.as<uint32_t>(), nWork_, tileSums.as<uint32_t>(), st + kSolidTotal,
                 st + kSolidOverflow, s, &launches);
-    launch_solid_toggle(b, nWork_, offsets.as<uint32_t>(), st + kSolidTotal, fillP, s, &launches);
+    tuneMark(kKnobToggle, false, s);
+    launch_solid_toggle(b, nWork_, offsets.as<uint32_t>(), st + kSolidTotal, fillP, shape.toggleBlocksPerSm, s,
+                        &launches);
+    tuneMark(kKnobToggle, true, s);
     launch_row_fill(b, totalRows_, fillP, s, &launches);
     mark(0, true);
     if (!nodes_) {
@@ -354,9 +364,12 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
         launch_scan(counts.as<uint32_t>(), offsets.as<uint32_t>(), nWork_, tileSums.as<uint32_t>(), st + kSurfTotal,
                     st + kSurfOverflow, s, &launches);
         mark(5, false);
+        tuneMark(kKnobSurface, false, s);
         launch_surface_work(0, wide_ ? 1 : 0, b, recs.p, ovl.p, offsets.as<uint32_t>(), nWork_, st + kSurfTotal,
                             buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_,
-                            hitList.as<unsigned long long>(), st + kHitCount, listCap_, s, &launches);
+                            hitList.as<unsigned long long>(), st + kHitCount, listCap_, shape.surfBlocksPerSm,
+                            shape.surfBatch, s, &launches);
+        tuneMark(kKnobSurface, true, s);
         mark(5, true);
         launch_surface_rank(surf.as<uint32_t>(), totalWords_, ranks.as<uint32_t>(), rankTiles.as<uint32_t>(),
                             st + kSurfaceVoxels, s, &launches);
@@ -395,13 +408,16 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
     if (anyMaterials_) {
         mark(4, false);
         launch_surface_keys_zero(keys.p, st + kSurfaceVoxels, keysCap_, wide_ ? 1 : 0, s, &launches);
+        tuneMark(kKnobMerge, false, s);
         if (!wide_)
             launch_surface_merge(hitList.as<unsigned long long>(), st + kHitCount, listCap_, surf.as<uint32_t>(),
-                                  ranks.as<uint32_t>(), keys.as<uint32_t>(), keysCap_, s, &launches);
+                                  ranks.as<uint32_t>(), keys.as<uint32_t>(), keysCap_, shape.mergeBlocksPerSm, s,
+                                  &launches);
         else
             launch_surface_work(1, 1, b, recs.p, ovl.p, offsets.as<uint32_t>(), nWork_, st + kSurfTotal,
                                 buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_,
-                                nullptr, st + kHitCount, 0, s, &launches);
+                                nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch, s, &launches);
+        tuneMark(kKnobMerge, true, s);
         mark(4, true);
     }
     // Node emission.
@@ -409,9 +425,12 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
     if (raw_)
         launch_emit_raw(nodeKind_, b, totalWords_, fillP, surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_,
                         s, &launches);
-    else if (anyCartesian_)
+    else if (anyCartesian_) {
+        tuneMark(kKnobEmit, false, s);
         launch_emit_cartesian(nodeKind_, b, totalWords_, fin.as<uint32_t>(), fillP, surf.as<uint32_t>(),
-                              ranks.as<uint32_t>(), keys.p, keysCap_, s, &launches);
+                              ranks.as<uint32_t>(), keys.p, keysCap_, shape.emitBlocksPerSm, s, &launches);
+        tuneMark(kKnobEmit, true, s);
+    }
     if (nFcc_)
         launch_emit_fcc(nodeKind_, b, reinterpret_cast<const FccMesh*>(tables.as<uint8_t>() + oFcc_),
                         reinterpret_cast<const uint64_t*>(tables.as<uint8_t>() + oGroupBase_), nFcc_, totalGroups_,
@@ -447,9 +466,43 @@ int Pipeline::pruneGroupUntilStable(const Group& gr, cudaStream_t s) {
     }
 }
 
+Pipeline::~Pipeline() {
+    for (cudaEvent_t& e : tuneEv_)
+        if (e) cudaEventDestroy(e);
+}
+
+void Pipeline::tuneMark(int knob, bool end, cudaStream_t s) {
+    if (trial_ < 0) return;
+    cudaEvent_t& e = tuneEv_[2 * knob + (end ? 1 : 0)];
+    if (!e && cudaEventCreate(&e) != cudaSuccess) {
+        cudaGetLastError();
+        e = nullptr;
+        return;
+    }
+    cudaEventRecord(e, s);
+    if (end) tuneUsed_[knob] = true;
+}
+
+// Reports the kernel times of a tuning trial (the stream has drained).
+void Pipeline::tuneFinish() {
+    if (trial_ < 0) return;
+    float ms[kKnobs];
+    for (int k = 0; k < kKnobs; ++k) {
+        ms[k] = -1.0f;
+        if (tuneUsed_[k] && tuneEv_[2 * k] && tuneEv_[2 * k + 1] &&
+            cudaEventElapsedTime(&ms[k], tuneEv_[2 * k], tuneEv_[2 * k + 1]) != cudaSuccess) {
+            cudaGetLastError();
+            ms[k] = -1.0f;
+        }
+    }
+    tuneReport(bucket_, trial_, ms);
+    trial_ = -1;
+}
+
 int Pipeline::finish(cudaStream_t s) {
     if (!nodes_) {
         VXB_CUDA(cudaStreamSynchronize(s));
+        tuneFinish();
         uint32_t h[2];
         VXB_CUDA(cudaMemcpy(h, status.p, sizeof(h), cudaMemcpyDeviceToHost));
         if (h[kSolidOverflow]) return failf(VXB_EOVERFLOW, "solid work list exceeds 2^32 entries");
@@ -460,6 +513,7 @@ int Pipeline::finish(cudaStream_t s) {
     uint32_t bk[kSurfaceBuckets] = {0};
     if (anyMaterials_) VXB_CUDA(cudaMemcpyAsync(bk, buckets.p, sizeof(bk), cudaMemcpyDeviceToHost, s));
     VXB_CUDA(cudaStreamSynchronize(s));
+    tuneFinish();
     memset(&stats, 0, sizeof(stats));
     stats.units = (uint32_t)units_.size();
     stats.work_triangles = nWork_;
@@ -488,7 +542,7 @@ int Pipeline::finish(cudaStream_t s) {
             launch_surface_keys_zero(keys.p, st + kSurfaceVoxels, keysCap_, wide_ ? 1 : 0, s, &launches);
             launch_surface_work(1, wide_ ? 1 : 0, b, recs.p, ovl.p, offsets.as<uint32_t>(), nWork_, st + kSurfTotal,
                                 buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_,
-                                nullptr, st + kHitCount, 0, s, &launches);
+                                nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch, s, &launches);
             reemit = true;
         }
     }
@@ -517,7 +571,7 @@ int Pipeline::finish(cudaStream_t s) {
                             keysCap_, s, &launches);
         else if (anyCartesian_)
             launch_emit_cartesian(nodeKind_, b, totalWords_, fin.as<uint32_t>(), fillP, surf.as<uint32_t>(),
-                                  ranks.as<uint32_t>(), keys.p, keysCap_, s, &launches);
+                                  ranks.as<uint32_t>(), keys.p, keysCap_, shape.emitBlocksPerSm, s, &launches);
         if (nFcc_)
             launch_emit_fcc(nodeKind_, b, reinterpret_cast<const FccMesh*>(tables.as<uint8_t>() + oFcc_),
                             reinterpret_cast<const uint64_t*>(tables.as<uint8_t>() + oGroupBase_), nFcc_,

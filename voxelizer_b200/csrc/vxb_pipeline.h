@@ -7,6 +7,9 @@
 #include "vxb_host.h"
 #include "vxb_kernels.cuh"
 #include "vxb_plan.h"
+#include "vxb_tune.h"
+
+#include <string>
 
 #include <vector>
 
@@ -74,7 +77,20 @@ public:
 
     static constexpr uint32_t kPasses = 8;   // pruning passes queued per subspace
 
+    // Launch shape of the last enqueue (the autotuner's choice).
+    LaunchShape shape{};
+    ~Pipeline();
+
 private:
+    // Autotuner trial of the current run: events around the tuned kernels,
+    // reported once finish has waited for them.
+    std::string bucket_;
+    int trial_ = -1;
+    cudaEvent_t tuneEv_[2 * kKnobs] = {};
+    bool tuneUsed_[kKnobs] = {};
+    void tuneMark(int knob, bool end, cudaStream_t s);
+    void tuneFinish();
+
     struct Group {            // pruning regions of one subspace index
         uint32_t first, count, words, flagBase;
     };

@@ -288,8 +288,8 @@ void launch_solid_count(const Batch& b, uint32_t nWork, uint32_t* counts, cudaSt
 }
 
 void launch_solid_toggle(const Batch& b, uint32_t nWork, const uint32_t* offsets, const uint32_t* total,
-                         uint32_t* fill, cudaStream_t s, uint32_t* launches) {
-    solidToggleKernel<<<148 * 3, kBlock, 0, s>>>(b, nWork, offsets, total, fill);
+                         uint32_t* fill, uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches) {
+    solidToggleKernel<<<148u * blocksPerSm, kBlock, 0, s>>>(b, nWork, offsets, total, fill);
     *launches += 1;
 }
 

@@ -39,7 +39,6 @@ namespace {
 
 constexpr int kBlock = 256;
 constexpr uint32_t kFull = 0xffffffffu;
-constexpr uint32_t kBatch = 16;  // 32-item chunks per owner search
 constexpr uint32_t kNone = 0xFFu;
 
 __device__ __forceinline__ void loadTriF(const float* __restrict__ V, const uint32_t* __restrict__ I, uint32_t t,
@@ -520,7 +519,8 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
     }
 }
 
-// Pass 4: the work list.  Warps take batches of kBatch consecutive 32-item
+// Pass 4: the work list.  Warps take batches of kBatch (8, 16 or 32, the
+// launch shape) consecutive 32-item
 // chunks; within a batch the owner of each chunk's first item follows from
 // the previous chunk.  Every partitioned triangle has at least one unit, so
 // a chunk's 32 items belong to at most 32 consecutive triangles: lane l
@@ -528,6 +528,7 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
 // gives every lane its owner.  The class and axis of a position follow from
 // the bucket bounds, so the projection edge functions load together with
 // the record.
+template <uint32_t kBatch>
 __global__ void __launch_bounds__(kBlock) surfaceWorkKernel(Sink sink, Batch b, const SurfRec* __restrict__ recs,
                                                             const SurfOvl* __restrict__ ovl,
                                                             const uint32_t* __restrict__ off, uint32_t n,
@@ -737,8 +738,8 @@ void launch_surface_prepare(const Batch& b, uint32_t nWork, uint32_t* codes, uin
 void launch_surface_work(int mode, int wide, const Batch& b, const void* recs, const void* ovl,
                          const uint32_t* offsets, uint32_t nWork, const uint32_t* total, const uint32_t* buckets,
                          uint32_t* surf, const uint32_t* ranks, void* keys, uint32_t keysCap,
-                         unsigned long long* list, uint32_t* listCount, uint32_t listCap, cudaStream_t s,
-                         uint32_t* launches) {
+                         unsigned long long* list, uint32_t* listCount, uint32_t listCap, uint32_t blocksPerSm,
+                         uint32_t batch, cudaStream_t s, uint32_t* launches) {
     Sink sink;
     sink.bits = surf;
     sink.wordRank = ranks;
@@ -749,8 +750,12 @@ void launch_surface_work(int mode, int wide, const Batch& b, const void* recs, c
     sink.listCap = listCap;
     sink.mode = mode;
     sink.wide = wide;
-    surfaceWorkKernel<<<148 * 8, kBlock, 0, s>>>(sink, b, static_cast<const SurfRec*>(recs),
-                                                  static_cast<const SurfOvl*>(ovl), offsets, nWork, total, buckets);
+    const uint32_t grid = 148u * blocksPerSm;
+    const SurfRec* R = static_cast<const SurfRec*>(recs);
+    const SurfOvl* O = static_cast<const SurfOvl*>(ovl);
+    if (batch == 8) surfaceWorkKernel<8><<<grid, kBlock, 0, s>>>(sink, b, R, O, offsets, nWork, total, buckets);
+    else if (batch == 32) surfaceWorkKernel<32><<<grid, kBlock, 0, s>>>(sink, b, R, O, offsets, nWork, total, buckets);
+    else surfaceWorkKernel<16><<<grid, kBlock, 0, s>>>(sink, b, R, O, offsets, nWork, total, buckets);
     *launches += 1;
 }
 
@@ -771,8 +776,8 @@ void launch_surface_keys_zero(void* keys, const uint32_t* count, uint32_t cap, i
 
 void launch_surface_merge(const unsigned long long* list, const uint32_t* listCount, uint32_t listCap,
                           const uint32_t* bits, const uint32_t* ranks, uint32_t* keys, uint32_t keysCap,
-                          cudaStream_t s, uint32_t* launches) {
-    mergeKeysKernel<<<148 * 8, 256, 0, s>>>(list, listCount, listCap, bits, ranks, keys, keysCap);
+                          uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches) {
+    mergeKeysKernel<<<148u * blocksPerSm, 256, 0, s>>>(list, listCount, listCap, bits, ranks, keys, keysCap);
     *launches += 1;
 }
 

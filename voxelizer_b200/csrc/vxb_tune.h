@@ -1,0 +1,48 @@
+// Launch-shape autotuner.  The shapes below change how the work of a kernel
+// is spread over the GPU (grid size, items per warp), never what it computes,
+// so every choice gives the same result.  Shapes are chosen per size bucket
+// (work triangles, grid words, node kind, material output): in tuning mode a
+// bucket's first calls run candidate shapes, each kernel's time is taken with
+// CUDA events, and once every candidate has its samples each kernel keeps its
+// fastest shape.  Chosen shapes can be saved to and read from a JSON file.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+namespace vxb {
+
+struct LaunchShape {
+    uint32_t surfBlocksPerSm = 16;   // surfaceWorkKernel blocks per SM
+    uint32_t surfBatch = 8;          // surfaceWorkKernel 32-item chunks per owner search
+    uint32_t mergeBlocksPerSm = 8;   // mergeKeysKernel
+    uint32_t emitBlocksPerSm = 16;   // emitNarrowKernel
+    uint32_t toggleBlocksPerSm = 3;  // solidToggleKernel
+};
+
+// The tuned kernels, in the order of their timing events.
+enum TuneKnob { kKnobSurface = 0, kKnobMerge = 1, kKnobEmit = 2, kKnobToggle = 3, kKnobs = 4 };
+constexpr int kTuneCandidates = 3;
+constexpr int kTuneSamples = 2;
+
+enum TuneMode { kTuneOff = 0, kTuneOn = 1, kTuneFrozen = 2 };
+
+// Size bucket of a batch.
+std::string tuneBucket(uint32_t workTriangles, uint64_t gridWords, int nodeKind, bool materials);
+
+// The shape for the next run of `bucket`.  *trial >= 0 when the run is a
+// tuning trial (its kernel times go to tuneReport); -1 otherwise.
+LaunchShape tunePick(const std::string& bucket, int* trial, bool allowTrial = true);
+// Kernel times (ms, < 0 for a kernel that did not run) of trial `trial`.
+void tuneReport(const std::string& bucket, int trial, const float* ms);
+
+int tuneSetMode(int mode, const char* cachePath);
+int tuneMode();
+// Number of buckets whose shapes are settled, and the JSON text of all of
+// them.
+uint32_t tuneSettled();
+std::string tuneJson();
+
+}  // namespace vxb
