@@ -90,7 +90,11 @@ template <class Node> __global__ void refZeroFaces(Node* nodes, uint3 dim) {
     const uint n = dim.x * dim.y * dim.z;
     for (uint i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint x = i % dim.x, y = (i % (dim.x * dim.y)) / dim.x, z = i / (dim.x * dim.y);
-        if (x == 0 || x == dim.x - 1 || y == 0 || y == dim.y - 1 || z == 0 || z == dim.z - 1) nodes[i] = Node();
+        if (Node::isFCCNode()) {
+            if (x < 2 || x > dim.x - 3 || y == 0 || y == dim.y - 1 || z < 2 || z > dim.z - 3) nodes[i] = Node();
+        } else if (x == 0 || x == dim.x - 1 || y == 0 || y == dim.y - 1 || z == 0 || z == dim.z - 1) {
+            nodes[i] = Node();
+        }
     }
 }
 
@@ -295,7 +299,8 @@ struct Runner {
         // grid, or the requested partition of it)
         dev.resolution = host.resolution;
         if (p.space) {
-            if (fcc || !(p.part[0] < p.part[1] && p.part[1] <= res.y && p.part[2] < p.part[3] && p.part[3] <= res.z))
+            if ((fcc && p.rotate_x) ||
+                !(p.part[0] < p.part[1] && p.part[1] <= res.y && p.part[2] < p.part[3] && p.part[3] <= res.z))
                 return -3;
             dev.resolution.min = make_uint3(0, p.part[0], p.part[2]);
             dev.resolution.max = make_uint3(res.x, p.part[1], p.part[3]);
@@ -469,6 +474,11 @@ struct Runner {
                 }
                 for (size_t i = 0; i < allocYz.splits.size(); ++i)
                     launchCalculateFCCBoundaries<Node>(dev, (Node*)g.nodes, nullptr, allocYz.splits[i], false, 0, false);
+                // host_side.cpp:1663-1673
+                if (dev.left || dev.right || dev.up || dev.down) {
+                    refZeroFaces<Node><<<dev.blocks, dev.threads>>>((Node*)g.nodes, outDim);
+                    RCHK(cudaGetLastError());
+                }
             }
         }
         if (p.node_output)

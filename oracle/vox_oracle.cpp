@@ -1141,10 +1141,11 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
         const double h = pl.d / 2.0;
         for (int g = 1; g <= 4; ++g) {
             d3 sh = g == 1 ? d3{0, 0, 0} : g == 2 ? d3{h, h, 0} : g == 3 ? d3{0, h, h} : d3{h, 0, h};
-            d3 m{pl.mn.x + sh.x, pl.mn.y + sh.y, pl.mn.z + sh.z};
+            d3 m{pl.mnExt.x + sh.x, pl.mnExt.y + sh.y, pl.mnExt.z + sh.z};
             std::fill(voxels.begin(), voxels.end(), 0u);
             for (auto& s : extYz)
-                performVoxelization(V, I, nT, m, pl.d, ext, s, pl.xRes, pl.xSplits, voxels.data(), alloc, F, 1, 1);
+                performVoxelization(V, I, nT, m, pl.d, ext, s, pl.xRes, pl.xSplits, voxels.data(), alloc, F, pl.padY,
+                                    pl.padZ);
             // convertToFCCGrid, src/voxelizer.cu:1710-1776
             const uint rx = alloc.x, ry = alloc.y;
 #pragma omp parallel for schedule(static)
@@ -1167,8 +1168,8 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
         if (mats) {
             for (int g = 1; g <= 4; ++g) {
                 d3 sh = g == 1 ? d3{0, 0, 0} : g == 2 ? d3{h, h, 0} : g == 3 ? d3{0, h, h} : d3{h, 0, h};
-                f3 m{float(pl.mn.x + sh.x), float(pl.mn.y + sh.y), float(pl.mn.z + sh.z)};
-                SurfaceCtx c{V, I, M, m, float(pl.d), alloc, true, g, &F, 1, 1};
+                f3 m{float(pl.mnExt.x + sh.x), float(pl.mnExt.y + sh.y), float(pl.mnExt.z + sh.z)};
+                SurfaceCtx c{V, I, M, m, float(pl.d), alloc, true, g, &F, (int)pl.padY, (int)pl.padZ};
                 surfacePass(c, nT, matSplits, rec);
             }
         }
@@ -1317,6 +1318,16 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
                     if (up && ((!xe && outy) || xe) && solid[n + npy + yo]) b += 2048;
                     T::setBid(nodes[n], b);
                 }
+        // zeroPadding (src/voxelizer.cu:4827-4834) of an FCC device space with
+        // neighbours: two node layers at the x and z faces, one at the y faces.
+        if (pl.border) {
+#pragma omp parallel for schedule(static)
+            for (long long z = 0; z < (long long)NZ; ++z)
+                for (uint y = 0; y < NY; ++y)
+                    for (uint x = 0; x < NX; ++x)
+                        if (x < 2 || x + 2 >= NX || y == 0 || y + 1 == NY || z < 2 || z + 2 >= (long long)NZ)
+                            nodes[(size_t)z * npy + (size_t)y * npx + x] = zero;
+        }
     }
     return 0;
 }
@@ -1336,7 +1347,7 @@ extern "C" int orc_plan(const orc_params* p, const float* verts, uint32_t nV, or
     bool fcc = p->node_type == ORC_SHORT_FCC || p->node_type == ORC_LONG_FCC;
     static const uint nb[5] = {1, 2, 8, 2, 4};
     if (p->node_type < 0 || p->node_type > 4) return -13;
-    if (p->space && fcc && p->node_output) return -13;   // device spaces of FCC lattices: not restated
+    if (p->rotate_x && fcc && p->node_output) return -13;   // slices of FCC lattices along x: not restated
     if (p->node_output) {
         info->dims[0] = fcc ? 2 * pl.alloc.x : pl.alloc.x;
         info->dims[1] = pl.alloc.y;

@@ -196,6 +196,14 @@ CASES = [
     case("room_lite_long_part22_3", "room_lite", LONG, 1, 1, 160, space=("part", 2, 2, 3)),
     case("ico4_partial_part31_1", "ico4", PARTIAL, 1, 1, 1.0 / 64.0, strict_mats=False, space=("part", 3, 1, 1)),
     case("room_lite_bits_part13_1", "room_lite", LONG, 0, 0, 160, space=("part", 1, 3, 1)),
+    # FCC device spaces: y / z slices and devConfig partitions.
+    case("ico4_sfcc_slice_y_mid", "ico4", SHORT_FCC, 1, 1, FCC_A, space=("slice", 1, 30)),
+    case("ico4_lfcc_slice_z_mid", "ico4", LONG_FCC, 1, 0, FCC_A, space=("slice", 2, 33)),
+    case("ico4_sfcc_slice_oob", "ico4", SHORT_FCC, 1, 1, FCC_A, space=("slice", 2, 0)),
+    case("ico4_sfcc_part22_0", "ico4", SHORT_FCC, 1, 1, FCC_A, space=("part", 2, 2, 0)),
+    case("ico4_sfcc_part22_3", "ico4", SHORT_FCC, 1, 1, FCC_A, space=("part", 2, 2, 3)),
+    case("stress_lfcc_part31_1", "stress_fcc", LONG_FCC, 1, 1, FCC_A, vox=(64, 32, 32), mat=(32, 32, 32),
+         strict_mats=False, space=("part", 3, 1, 1)),
     # Slices along x: the mesh turned about z, sliced along the turned y.
     case("torus_long_slice_x_mid", "torus", LONG, 1, 1, 120, space=("slice", 0, 40)),
     case("torus_short_slice_x_first", "torus", SHORT, 1, 1, 120, space=("slice", 0, 1)),

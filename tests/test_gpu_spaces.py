@@ -14,7 +14,7 @@ import cases as C
 import oracle as O
 from helpers import masked
 from voxelizer_b200._lib import VxbError
-from voxelizer_b200.api import LONG, SHORT, SHORT_FCC, Voxelizer
+from voxelizer_b200.api import LONG, LONG_FCC, SHORT, SHORT_FCC, Voxelizer
 
 
 def _oracle_space(m, node_type, nodes, size, vox, mat, part, oob=False, rotate_x=False):
@@ -49,7 +49,14 @@ def test_slice_argument_errors():
         assert parts[0][0] == 0 and parts[2][1] == full.resolution.y and parts[5][3] == full.resolution.z
     with Voxelizer(m.vertices, m.indices, node_type=SHORT_FCC) as v:
         with pytest.raises(VxbError, match="EUNSUPPORTED"):
-            v.planSlice(1.0 / 64.0, 1, 5)
+            v.planSlice(1.0 / 64.0, 0, 5)   # FCC slices along x are not built
+        full = v.plan(1, 1.0 / 64.0)
+        info = v.planSlice(1.0 / 64.0, 1, 5)   # FCC: x and z doubled, three voxel rows along y
+        assert info.dims == (full.dims[0], 3, full.dims[2])
+        info = v.planSlice(1.0 / 64.0, 2, 5)
+        assert info.dims == (full.dims[0], full.dims[1], 6)
+        infos = v.planParts(1, 1.0 / 64.0, (2, 1))
+        assert sum(i.dims[1] - 2 for i in infos) == full.dims[1] - 2
 
 
 @pytest.mark.gpu
@@ -96,3 +103,35 @@ def test_partitions_match_oracle(dev, nodes):
         want, oi = _oracle_space(mm, SHORT, nodes, size, vox, mat, part)
         assert info.dims == tuple(oi.dims)
         assert np.array_equal(got, want), f"partition {k} of {dev}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("node_type", [SHORT_FCC, LONG_FCC])
+def test_fcc_spaces_match_oracle(node_type):
+    """FCC lattices in device spaces: each sub-lattice voxelized over the
+    extended partition from its shifted corner, the faces of an allocation
+    with neighbours zeroed two node layers deep along x and z."""
+    m = C.mesh("ico4")
+    mats = (1 + np.arange(m.n_triangles) % 9).astype(np.uint8)
+    mm = m.__class__(m.vertices, m.indices, mats, 10)
+    size, vox, mat = C.FCC_A, (1024, 512, 512), (512, 512, 512)
+    res = O.plan(mm, node_type, 1, size, vox).resolution
+    ry, rz = int(res[1]), int(res[2])
+    with Voxelizer(mm.vertices, mm.indices, node_type=node_type) as v:
+        v.setMaterials(mats, 10)
+        for direction, n in ((1, ry), (2, rz)):
+            for s in [0, 1, n // 2, n, n + 1]:
+                got, info = v.voxelizeSliceToRAM(size, direction, s, vox, mat)
+                s0 = 0 if (s == 0 or s > n) else s - 1
+                part = (0, ry, s0, s0 + 1) if direction == 2 else (s0, s0 + 1, 0, rz)
+                want, oi = _oracle_space(mm, node_type, 1, size, vox, mat, part, oob=(s == 0 or s > n))
+                assert info.dims == tuple(oi.dims)
+                assert np.array_equal(masked(node_type, 1, got), want), f"slice {s} along {direction}"
+        for dev in [(2, 2), (3, 1)]:
+            ys, zs = C.split_parts(ry, dev[0]), C.split_parts(rz, dev[1])
+            for k, (got, info) in enumerate(v.voxelizePartsToRAM(1, size, dev, vox, mat)):
+                y, z = k % dev[0], k // dev[0]
+                part = (ys[y][0], ys[y][1], zs[z][0], zs[z][1])
+                want, oi = _oracle_space(mm, node_type, 1, size, vox, mat, part)
+                assert info.dims == tuple(oi.dims)
+                assert np.array_equal(masked(node_type, 1, got), want), f"partition {k} of {dev}"

@@ -105,13 +105,9 @@ def test_array_dimensions_match_plan():
             d = v.getArrayDimensions(1.0 / 100.0, 1024, False)
             info = v.plan(1, 1.0 / 100.0)
             assert d == info.dims
-            if nt >= 3:   # FCC lattices are not turned
-                with pytest.raises(_lib.VxbError):
-                    v.getArrayDimensions(1.0 / 100.0, 1024, True)
-                continue
-            # sliceAlongX: the turned mesh's grid with x and y exchanged
-            # (src/host_side.cpp:3333-3371)
-            t = O.plan(m, nt, 1, 1.0 / 100.0, rotate_x=True).dims
-            assert v.getArrayDimensions(1.0 / 100.0, 1024, True) == (t[1], t[0], t[2])
-            t = O.plan(m, nt, 1, 90, rotate_x=True).dims
-            assert v.getArrayDimensions(90, 1024, True) == (t[1], t[0], t[2])
+            # sliceAlongX: the turned mesh's grid with x and y exchanged,
+            # FCC lattices with x and z doubled (src/host_side.cpp:3333-3371)
+            f = 2 if nt >= 3 else 1
+            for size in (1.0 / 100.0, 90):
+                t = O.plan(m, 0, 1, size, rotate_x=True).dims
+                assert v.getArrayDimensions(size, 1024, True) == (f * t[1], t[0], f * t[2])

@@ -139,6 +139,56 @@ def test_cli_argument_errors(tmp_path, capsys, sphere):
     a = cli.parser().parse_args([path, "-r", "64", "-L", "-F", "-m", "-V", "64", "32", "32"])
     assert a.resolution == 64 and a.long and a.fcc and a.materials
     assert cli._node_type(a) == cli.api.LONG_FCC and a.voxRes == [64, 32, 32]
+    # The tester's checks of the slice and multi-device options.
+    for args, msg in ([["-r", "32", "-V", "64", "32"], "--voxRes requires 3 arguments."],
+                      [["-r", "32", "-S", "1", "4", "-V", "64", "32", "32"], "--voxRes requires 2 arguments with"],
+                      [["-r", "32", "-S", "1", "4", "-M", "64"], "--matRes requires 2 arguments with"],
+                      [["-r", "32", "-S", "1"], "--slice requires 2 arguments."],
+                      [["-r", "32", "-S", "3", "1"], "The direction of slice is > 2."],
+                      [["-r", "32", "-A", "3"], "The direction has to be between 0 and 2."],
+                      [["-r", "32", "-D", "2"], "--multiDevice: Device configuration needs two values."]):
+        assert cli.main([path, *args]) == 1
+        assert msg in capsys.readouterr().out
+
+
+def test_cli_apply_slice_and_stitch():
+    """applySlice and stitchNodeArrays placements (tests/src/main.cpp:1227-1262,
+    1396-1434) on labelled arrays."""
+    from types import SimpleNamespace as NS
+    from voxelizer_b200 import cli
+    X, Y, Z = 5, 4, 3
+    for d in range(3):
+        nodes = np.zeros(X * Y * Z, np.int64)
+        n = (X, Y, Z)[d]
+        for k in range(n):
+            shape = [Z, Y, X]
+            shape[2 - d] = 3
+            sl = np.full(shape, -1, np.int64)
+            idx = [slice(None)] * 3
+            idx[2 - d] = 1
+            sl[tuple(idx)] = 100 * k + np.arange(sl[tuple(idx)].size).reshape(sl[tuple(idx)].shape)
+            cli.apply_slice(sl.reshape(-1), k, nodes, (X, Y, Z), d)
+        full = nodes.reshape(Z, Y, X)
+        for k in range(n):
+            layer = np.take(full, k, axis=2 - d)
+            assert np.array_equal(layer.reshape(-1), 100 * k + np.arange(layer.size))
+    # Two partitions along y of a 6 x 6 x 4 grid (allocations of 6 x 5 x 4):
+    # inner nodes land one step further along every axis.
+    parts = []
+    for ly in range(2):
+        a = np.arange(6 * 5 * 4, dtype=np.int64) + 1000 * ly
+        parts.append((a, NS(dims=(6, 5, 4), location=NS(y=ly, z=0))))
+    out, dims = cli.stitch(parts, 2, 1)
+    assert dims == (6, 8, 4)
+    full = out.reshape(4, 8, 6)
+    for ly, (a, _) in enumerate(parts):
+        src = a.reshape(4, 5, 6)
+        for z in range(1, 3):
+            for y in range(1, 4):
+                for x in range(1, 5):
+                    zp, yp, xp = 1 + z, 1 + ly * 3 + y, 1 + x
+                    if zp < 4 and yp < 8 and xp < 6:
+                        assert full[zp, yp, xp] == src[z, y, x]
 
 
 # --- GPU: a mesh from a file voxelizes exactly like the same mesh from memory ---
@@ -176,3 +226,32 @@ def test_cli_file_matches_memory(tmp_path, fmt, flags):
     ref, _, _ = O.voxelize(om, node_type, int(not a.voxels), int(a.materials), size)
     nodes = not a.voxels
     np.testing.assert_array_equal(masked(node_type, nodes, got), masked(node_type, nodes, ref))
+
+
+@pytest.mark.gpu
+def test_cli_slice_modes(tmp_path):
+    """-S, -A and -D give the API's slices and partitions, placed as the
+    tester places them."""
+    from voxelizer_b200 import api, cli
+    mesh = Mesh(*torus(48, 24, 0.6, 0.25, (0.05, 0.0, -0.1)))
+    path = str(tmp_path / "t.obj")
+    meshio.save_obj(path, mesh.vertices, mesh.indices)
+    out = str(tmp_path / "out.npy")
+    with api.Voxelizer(mesh.vertices, mesh.indices, node_type=api.LONG) as vz:
+        vz.setMaterials((1 + np.arange(mesh.n_triangles) % 7).astype(np.uint8), 8)
+        vz.setMaterialOutput(True)
+        assert cli.main([path, "-r", "40", "-L", "-m", "-S", "2", "7", "-o", out]) == 0
+        want, _ = vz.voxelizeSliceToRAM(40, 2, 7, (1024, 512), (1024, 512))
+        np.testing.assert_array_equal(np.load(out).reshape(-1), want)
+        for d in range(3):
+            assert cli.main([path, "-r", "40", "-L", "-m", "-A", str(d), "-o", out]) == 0
+            got = np.load(out).reshape(-1)
+            dims = vz.getArrayDimensions(40, 1024, d == 0)
+            want = np.zeros(dims[0] * dims[1] * dims[2], np.uint16)
+            for k in range(dims[d]):
+                cli.apply_slice(vz.voxelizeSliceToRAM(40, d, k, (1024, 512), (1024, 512))[0], k, want, dims, d)
+            np.testing.assert_array_equal(got, want)
+            assert np.count_nonzero(got)
+        assert cli.main([path, "-r", "40", "-L", "-m", "-D", "2", "2", "-o", out]) == 0
+        want, _ = cli.stitch(vz.voxelizePartsToRAM(True, 40, (2, 2)), 2, 2)
+        np.testing.assert_array_equal(np.load(out).reshape(-1), want)

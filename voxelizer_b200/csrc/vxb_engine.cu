@@ -43,7 +43,7 @@ struct vxb_voxelizer {
     double mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
     bool meshOnDevice = false, matsOnDevice = false;
     bool hasMaterials = false;   // setMaterials was called (materials live on the host or the device)
-    vxb::DevBuf dV, dI, dM, outStage;
+    vxb::DevBuf dV, dI, dM, outStage, dCheck;
     // Slices along x: the rotated mesh (made on the first such call) and the
     // rotated slice's node array before the boundary ids.
     vxb::DevBuf dVrot, xStage, xFlag;
@@ -241,7 +241,6 @@ int vxb_voxelizer::planSpaces(int nodes, const vxb_request* r, const std::vector
     vxb::Plan full;
     int rc = fullPlan(r, full);
     if (rc) return rc;
-    if (isFcc(nodeType)) return failf(VXB_EUNSUPPORTED, "device spaces of FCC lattices are not supported");
     const uint32_t vs[3] = {r->vox_split_res.x, r->vox_split_res.y, r->vox_split_res.z};
     const uint32_t ms[3] = {r->mat_split_res.x, r->mat_split_res.y, r->mat_split_res.z};
     for (size_t i = 0; i < sp.size(); ++i) {
@@ -322,7 +321,7 @@ void vxb_voxelizer::rotation(double* a, double* b, double* rmn, double* rmx) con
 
 int vxb_voxelizer::planXSlice(const vxb_request* r, uint32_t slice, vxb::Plan* q, bool* oob,
                               vxb_grid_info* info) const {
-    if (isFcc(nodeType)) return failf(VXB_EUNSUPPORTED, "device spaces of FCC lattices are not supported");
+    if (isFcc(nodeType)) return failf(VXB_EUNSUPPORTED, "slices of FCC lattices along x are not supported");
     double a, b, rmn[3], rmx[3];
     rotation(&a, &b, rmn, rmx);
     vxb::Plan full;
@@ -481,26 +480,57 @@ vxb_status vxb_create(vxb_voxelizer** out, int node_type, const float* vertices,
     *out = nullptr;
     if (node_type < 0 || node_type > 4) return failf(VXB_EINVAL, "unknown node type %d", node_type);
     if ((!vertices && n_vertices) || (!indices && n_triangles)) return failf(VXB_EINVAL, "NULL mesh arrays");
-    uint32_t maxIndex = 0;
-    for (uint64_t i = 0; i < 3ull * n_triangles; ++i) maxIndex = std::max(maxIndex, indices[i]);
-    if (n_triangles && maxIndex >= n_vertices)
-        for (uint64_t i = 0; i < 3ull * n_triangles; ++i)
-            if (indices[i] >= n_vertices)
-                return failf(VXB_EINVAL, "index %u of triangle %llu is out of range", indices[i],
-                             (unsigned long long)(i / 3));
+    auto badIndex = [&](uint64_t i) {
+        return failf(VXB_EINVAL, "index %u of triangle %llu is out of range", indices[i], (unsigned long long)(i / 3));
+    };
     vxb_voxelizer* v = new (std::nothrow) vxb_voxelizer();
     if (!v) return failf(VXB_ENOMEM, "out of host memory");
     v->nodeType = node_type;
     v->device = device;
     v->nV = n_vertices;
     v->nT = n_triangles;
-    if (n_vertices) vxb::boundingBox(vertices, n_vertices, v->mn, v->mx);
     // The copy the reference keeps on the host goes straight to the device
-    // when there is one; without a device (planning only) it stays on the
-    // host until the first voxelization.
-    if (!v->uploadFrom(vertices, indices)) {
-        v->vertices.assign(vertices, vertices + 3 * (size_t)n_vertices);
-        v->indices.assign(indices, indices + 3 * (size_t)n_triangles);
+    // when there is one, and the index check and the bounding box run there
+    // on that copy; without a device (planning only) the mesh stays on the
+    // host until the first voxelization and the checks run here.
+    unsigned long long chk[8];
+    const bool uploaded = n_vertices && n_triangles && v->uploadFrom(vertices, indices);
+    const bool checked = uploaded && onDevice(device, [&]() {
+                             return v->dCheck.ensure(sizeof(chk)) == 0 &&
+                                    vxb::meshCheck(v->dV.as<float>(), n_vertices, v->dI.as<uint32_t>(),
+                                                   3ull * n_triangles, v->dCheck.as<unsigned long long>(), chk,
+                                                   0) == 0;
+                         });
+    if (checked) {
+        if (chk[7] != ~0ull) {
+            delete v;
+            return badIndex(chk[7]);
+        }
+        for (int a = 0; a < 3; ++a) {
+            v->mn[a] = v->mx[a] = vertices[a];
+            if (chk[a] != ~0ull) {
+                const float f = vertices[3 * (size_t)(uint32_t)chk[a] + a];
+                if (f < v->mn[a]) v->mn[a] = f;
+            }
+            if (chk[3 + a] != ~0ull) {
+                const float f = vertices[3 * (size_t)(uint32_t)chk[3 + a] + a];
+                if (f > v->mx[a]) v->mx[a] = f;
+            }
+        }
+    } else {
+        uint32_t maxIndex = 0;
+        for (uint64_t i = 0; i < 3ull * n_triangles; ++i) maxIndex = std::max(maxIndex, indices[i]);
+        if (n_triangles && maxIndex >= n_vertices)
+            for (uint64_t i = 0; i < 3ull * n_triangles; ++i)
+                if (indices[i] >= n_vertices) {
+                    delete v;
+                    return badIndex(i);
+                }
+        if (n_vertices) vxb::boundingBox(vertices, n_vertices, v->mn, v->mx);
+        if (!uploaded) {
+            v->vertices.assign(vertices, vertices + 3 * (size_t)n_vertices);
+            v->indices.assign(indices, indices + 3 * (size_t)n_triangles);
+        }
     }
     *out = v;
     return VXB_OK;
@@ -558,8 +588,8 @@ vxb_status vxb_get_array_dimensions(vxb_voxelizer* v, int by_cube_length, uint32
     if (!v || !dims) return failf(VXB_EINVAL, "NULL argument");
     if (slice_along_x) {
         // src/host_side.cpp:3333-3371: the rotated mesh's grid (padding
-        // included), its corners un-rotated: x and y trade places.
-        if (isFcc(v->nodeType)) return failf(VXB_EUNSUPPORTED, "sliceAlongX of FCC lattices is not supported");
+        // included), its corners un-rotated: x and y trade places; FCC
+        // lattices double x and z.
         vxb_request r;
         r.by_cube_length = by_cube_length;
         r.max_dimension = max_dimension;
@@ -571,9 +601,10 @@ vxb_status vxb_get_array_dimensions(vxb_voxelizer* v, int by_cube_length, uint32
         vxb::Plan p;
         int rc = v->fullPlan(&r, p, rmn, rmx);
         if (rc) return rc;
-        dims->x = p.alloc[1];
+        const uint32_t f = isFcc(v->nodeType) ? 2u : 1u;
+        dims->x = f * p.alloc[1];
         dims->y = p.alloc[0];
-        dims->z = p.alloc[2];
+        dims->z = f * p.alloc[2];
         return VXB_OK;
     }
     vxb_request r;

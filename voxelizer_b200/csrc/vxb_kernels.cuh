@@ -112,6 +112,14 @@ void launch_surface_merge(const unsigned long long* list, const uint32_t* listCo
                           const uint32_t* bits, const uint32_t* ranks, uint32_t* keys, uint32_t keysCap,
                           uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches);
 
+// Mesh checks of vxb_create (vxb_meshcheck.cu): hostOut[0..2] / [3..5]
+// name the first vertex (after vertex 0) holding the smallest / largest
+// non-NaN coordinate per axis as (order code << 32 | vertex), ~0 if none;
+// hostOut[6] is the largest index, hostOut[7] the first position of an
+// index >= nV (~0 if none).  Synchronizes `s`.
+int meshCheck(const float* dV, uint32_t nV, const uint32_t* dI, uint64_t nIdx, unsigned long long* dOut,
+              unsigned long long* hostOut, cudaStream_t s);
+
 // ---- Node classification: src/voxelizer.cu:1626-2048 ----
 void launch_combine(const uint32_t* a, const uint32_t* b, uint32_t* out, uint64_t n, cudaStream_t s,
                     uint32_t* launches);

@@ -543,7 +543,11 @@ __global__ void emitFccKernel(FccArgs A, uint64_t totalGroups) {
                 const uint32_t r = __ldg(A.ranks + G.wordBase[gt] + w) + (bt ? __popc(sw >> (32 - bt)) : 0u);
                 mat = r < A.keysCap ? NT::keyMat(reinterpret_cast<const uint32_t*>(A.keys)[r]) : 0u;
             }
-            const uint64_t val = NT::pack(bid, mat, 0.0f);
+            // zeroPadding of an FCC device space with neighbours
+            // (src/voxelizer.cu:4827-4834): two node layers at the x and z
+            // faces, one at the y faces.
+            const bool face = g.border && (X2 < 2 || X2 + 2 >= NX || y == 0 || y + 1 == NY || Z2 < 2 || Z2 + 2 >= NZ);
+            const uint64_t val = face ? 0ull : NT::pack(bid, mat, 0.0f);
             if (NT::bytes == 2) reinterpret_cast<uint16_t*>(&outv)[n] = (uint16_t)val;
             else reinterpret_cast<uint32_t*>(&outv)[n] = (uint32_t)val;
         }

@@ -159,7 +159,6 @@ int Pipeline::prepare(const std::vector<MeshJob>& jobs, cudaStream_t s) {
             return failf(VXB_EINVAL, "invalid request (maxDimension >= 2 or cubeLength > 0, split sizes > 0 and an x "
                                      "pass of at most 1024 voxels are required)");
         if (j.space) {
-            if (fcc) return failf(VXB_EUNSUPPORTED, "device spaces of FCC lattices are not supported");
             Plan full = p;
             if (devicePlan(full, j.part[0], j.part[1], j.part[2], j.part[3], vs, ms, p))
                 return failf(VXB_EINVAL, "empty or out-of-range partition");

@@ -27,7 +27,7 @@ namespace {
 
 constexpr double kDblMin = 2.2250738585072014e-308;  // DBL_MIN, src/voxelizer.cu:1443
 constexpr int kBlock = 256;
-constexpr uint32_t kSlots = 96;
+constexpr uint32_t kSlots = 160;   // 160 staged triangles: 44 KB of static shared memory
 
 __device__ __forceinline__ void loadTriD(const float* __restrict__ V, const uint32_t* __restrict__ I, uint32_t t,
                                          D3* v) {
