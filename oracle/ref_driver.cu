@@ -299,8 +299,7 @@ struct Runner {
         // grid, or the requested partition of it)
         dev.resolution = host.resolution;
         if (p.space) {
-            if ((fcc && p.rotate_x) ||
-                !(p.part[0] < p.part[1] && p.part[1] <= res.y && p.part[2] < p.part[3] && p.part[3] <= res.z))
+            if (!(p.part[0] < p.part[1] && p.part[1] <= res.y && p.part[2] < p.part[3] && p.part[3] <= res.z))
                 return -3;
             dev.resolution.min = make_uint3(0, p.part[0], p.part[2]);
             dev.resolution.max = make_uint3(res.x, p.part[1], p.part[3]);
@@ -329,7 +328,10 @@ struct Runner {
         uint3 outDim = fcc ? make_uint3(2 * ar.x, ar.y, 2 * ar.z) : ar;
         uint64_t need = p.node_output ? uint64_t(nNodes) * sizeof(Node) : uint64_t(nInts) * sizeof(VoxInt);
         dimsOut[0] = outDim.x; dimsOut[1] = outDim.y; dimsOut[2] = outDim.z;
-        if (p.rotate_x && p.space && p.node_output) std::swap(dimsOut[0], dimsOut[1]);   // turned back
+        if (p.rotate_x && p.space && p.node_output) {   // turned back (an FCC 2X x Y array becomes 2Y x X)
+            dimsOut[0] = fcc ? 2 * outDim.y : outDim.y;
+            dimsOut[1] = fcc ? outDim.x / 2 : outDim.x;
+        }
         if (out == nullptr) return 0;             // plan only
         if (outBytes < need) return -2;
         cudaEvent_t e0, e1;
@@ -431,20 +433,27 @@ struct Runner {
                     if (p.rotate_x) std::swap(g.nodes, g.nodesCopy);   // the result is read from g.nodes
                 }
             } else {
-                // fccWorker, host_side.cpp:1432-1657
+                // fccWorker, host_side.cpp:1432-1657; slicing along x shifts
+                // z the other way round and writes grid gt to slot
+                // (gt + 1) % 4 + 1 (1442-1476).
+                const bool xs = p.rotate_x != 0;
                 RCHK(cudaMemset(g.nodes, 0, uint64_t(nNodes) * sizeof(Node)));
                 double3 bbMin = dev.extMinVertex;
                 double h = d / 2.0;
+                auto gridShift = [&](int gt) {
+                    return gt == 1 ? make_double3(0.0, 0.0, xs ? h : 0.0)
+                         : gt == 2 ? make_double3(h, h, xs ? h : 0.0)
+                         : gt == 3 ? make_double3(0.0, h, xs ? 0.0 : h)
+                                   : make_double3(h, 0.0, xs ? 0.0 : h);
+                };
                 for (int gt = 1; gt < 5; ++gt) {
-                    double3 sh = gt == 1 ? make_double3(0.0, 0.0, 0.0)
-                               : gt == 2 ? make_double3(h, h, 0.0)
-                               : gt == 3 ? make_double3(0.0, h, h)
-                                         : make_double3(h, 0.0, h);
+                    double3 sh = gridShift(gt);
                     dev.extMinVertex = make_double3(bbMin.x + sh.x, bbMin.y + sh.y, bbMin.z + sh.z);
                     for (size_t i = 0; i < extYz.splits.size(); ++i)
                         performVoxelization(extYz.splits[i], xRes, xSplits);
                     for (size_t i = 0; i < allocYz.splits.size(); ++i)
-                        launchConvertToFCCGrid<Node>(dev, g.voxels, (Node*)g.nodes, allocYz.splits[i], gt, 0, false);
+                        launchConvertToFCCGrid<Node>(dev, g.voxels, (Node*)g.nodes, allocYz.splits[i],
+                                                     xs ? (gt + 1) % 4 + 1 : gt, 0, false);
                     // resetDataStructures, host_side.cpp:3514-3520
                     RCHK(cudaMemset(g.voxels, 0, uint64_t(nInts) * sizeof(VoxInt)));
                     if (g.wqTris) RCHK(cudaMemset(g.wqTris, 0, sizeof(uint) * dev.maxWorkQueueSize));
@@ -460,25 +469,51 @@ struct Runner {
                 if (materials) {
                     Split3 ms = split3(p.mat_split, ext);
                     for (int gt = 1; gt < 5; ++gt) {
-                        double3 sh = gt == 1 ? make_double3(0.0, 0.0, 0.0)
-                                   : gt == 2 ? make_double3(h, h, 0.0)
-                                   : gt == 3 ? make_double3(0.0, h, h)
-                                             : make_double3(h, 0.0, h);
+                        double3 sh = gridShift(gt);
                         dev.extMinVertex = make_double3(bbMin.x + sh.x, bbMin.y + sh.y, bbMin.z + sh.z);
                         calcTriangleClassification(dev, host, g.verts, g.idx, g.triTypes, g.sortedTris, 0, false);
                         for (size_t i = 0; i < ms.splits.size(); ++i)
                             calcOptSurfaceVoxelization<Node>(dev, host, g.verts, g.idx, g.triTypes, g.sortedTris,
-                                                             g.mats, (Node*)g.nodes, ms.splits[i], gt, 0, false);
+                                                             g.mats, (Node*)g.nodes, ms.splits[i],
+                                                             xs ? (gt + 1) % 4 + 1 : gt, 0, false);
                     }
                     dev.extMinVertex = bbMin;
                 }
+                uint3 zeroDim = outDim;
+                if (xs) {
+                    // restoreRotatedNodes into the copy, then the turned-back
+                    // allocation from unRotateCoords' FCC branch
+                    // (host_side.cpp:1601-1628, 3293-3309).
+                    RCHK(cudaMalloc(&g.nodesCopy, uint64_t(nNodes) * sizeof(Node)));
+                    RCHK(cudaMemset(g.nodesCopy, 0, uint64_t(nNodes) * sizeof(Node)));
+                    for (size_t i = 0; i < allocYz.splits.size(); ++i) {
+                        unRotateNodes<Node><<<dev.blocks, dev.threads>>>((Node*)g.nodes, (Node*)g.nodesCopy,
+                                                                         dev.allocResolution, allocYz.splits[i]);
+                        RCHK(cudaGetLastError());
+                    }
+                    const Bounds<uint3> ap = dev.allocResolution;
+                    const uint xDim = ap.max.x - ap.min.x;
+                    auto unrot = [&](uint3 v) {
+                        return make_uint3(2 * v.y + (v.x + v.z + 1) % 2, xDim / 2 - 1 - v.x / 2, v.z);
+                    };
+                    const uint3 t0 = unrot(ap.min);
+                    const uint3 t1 = unrot(make_uint3(ap.max.x - 1, ap.max.y - 1, ap.max.z - 1));
+                    dev.allocResolution.min = make_uint3(t0.x - 1, t1.y, t0.z);
+                    dev.allocResolution.max = make_uint3(t1.x + 1, t0.y + 1, t1.z + 1);
+                    allocYz = splitYZ(make_uint2(p.vox_split.y, p.vox_split.z), dev.allocResolution);
+                    zeroDim = make_uint3(dev.allocResolution.max.x - dev.allocResolution.min.x,
+                                         dev.allocResolution.max.y - dev.allocResolution.min.y,
+                                         dev.allocResolution.max.z - dev.allocResolution.min.z);
+                }
                 for (size_t i = 0; i < allocYz.splits.size(); ++i)
-                    launchCalculateFCCBoundaries<Node>(dev, (Node*)g.nodes, nullptr, allocYz.splits[i], false, 0, false);
+                    launchCalculateFCCBoundaries<Node>(dev, (Node*)g.nodes, (Node*)g.nodesCopy, allocYz.splits[i], xs,
+                                                       0, false);
                 // host_side.cpp:1663-1673
                 if (dev.left || dev.right || dev.up || dev.down) {
-                    refZeroFaces<Node><<<dev.blocks, dev.threads>>>((Node*)g.nodes, outDim);
+                    refZeroFaces<Node><<<dev.blocks, dev.threads>>>((Node*)(xs ? g.nodesCopy : g.nodes), zeroDim);
                     RCHK(cudaGetLastError());
                 }
+                if (xs) std::swap(g.nodes, g.nodesCopy);   // the result is read from g.nodes
             }
         }
         if (p.node_output)

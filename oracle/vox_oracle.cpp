@@ -1096,7 +1096,7 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
     std::vector<Bounds<u2> > allocYz = splitYZ(vs, allocPart);
     // Slices along x: nodes are built on the turned grid and turned back
     // before the boundary ids (src/host_side.cpp:1144-1206).
-    const bool turn = p->rotate_x && p->node_output && !fcc;
+    const bool turn = p->rotate_x && p->node_output;
     const bool mats = p->materials && p->node_output;
     if (!p->node_output) {
         for (auto& s : extYz)
@@ -1138,9 +1138,18 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
             surfacePass(c, nT, matSplits, rec);
         }
     } else {
+        // Sub-lattice g goes to FCC slot g (1 + (x & 1) + 2 (z & 1)).  For a
+        // turned mesh the reference shifts grid g by the z-swapped pattern and
+        // writes it to slot (g + 1) % 4 + 1 (src/host_side.cpp:1438-1476),
+        // i.e. slot g gets its usual shift with the y part toggled.
         const double h = pl.d / 2.0;
-        for (int g = 1; g <= 4; ++g) {
+        auto shift = [&](int g) {
             d3 sh = g == 1 ? d3{0, 0, 0} : g == 2 ? d3{h, h, 0} : g == 3 ? d3{0, h, h} : d3{h, 0, h};
+            if (turn) sh.y = sh.y == 0.0 ? h : 0.0;
+            return sh;
+        };
+        for (int g = 1; g <= 4; ++g) {
+            d3 sh = shift(g);
             d3 m{pl.mnExt.x + sh.x, pl.mnExt.y + sh.y, pl.mnExt.z + sh.z};
             std::fill(voxels.begin(), voxels.end(), 0u);
             for (auto& s : extYz)
@@ -1167,7 +1176,7 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
         }
         if (mats) {
             for (int g = 1; g <= 4; ++g) {
-                d3 sh = g == 1 ? d3{0, 0, 0} : g == 2 ? d3{h, h, 0} : g == 3 ? d3{0, h, h} : d3{h, 0, h};
+                d3 sh = shift(g);
                 f3 m{float(pl.mnExt.x + sh.x), float(pl.mnExt.y + sh.y), float(pl.mnExt.z + sh.z)};
                 SurfaceCtx c{V, I, M, m, float(pl.d), alloc, true, g, &F, (int)pl.padY, (int)pl.padZ};
                 surfacePass(c, nT, matSplits, rec);
@@ -1204,15 +1213,19 @@ static int run(const orc_params* p, const Plan& pl, const float* V, uint nV, con
     info->n_surface = rec.size();
     if (turn) {
         // unRotateNodes (src/voxelizer.cu:2061-2124): (x, y, z) of the X x Y
-        // x Z array goes to (y, X - 1 - x, z) of the Y x X x Z array; the
-        // allocation and its yz subspaces become the turned-back ones.
+        // x Z array goes to (y, X - 1 - x, z) of the Y x X x Z array; an FCC
+        // node (x, y, z) of the 2X x Y x 2Z array goes to (2y + (x + z + 1) %
+        // 2, X - 1 - x / 2, z) of the 2Y x X x 2Z array.  The allocation and
+        // its yz subspaces become the turned-back ones.
         N* dst = (N*)out;
-        const size_t X = alloc.x, Y = alloc.y;
+        const size_t X = fcc ? 2 * (size_t)alloc.x : alloc.x, Y = alloc.y, Zn = fcc ? 2 * (size_t)alloc.z : alloc.z;
 #pragma omp parallel for schedule(static)
-        for (long long z = 0; z < (long long)alloc.z; ++z)
+        for (long long z = 0; z < (long long)Zn; ++z)
             for (size_t y = 0; y < Y; ++y)
                 for (size_t x = 0; x < X; ++x) {
-                    const size_t i = (size_t)z * X * Y + y * X + x, j = (size_t)z * X * Y + (X - 1 - x) * Y + y;
+                    const size_t i = (size_t)z * X * Y + y * X + x;
+                    const size_t j = fcc ? (size_t)z * X * Y + (X / 2 - 1 - x / 2) * (2 * Y) + 2 * y + (x + z + 1) % 2
+                                         : (size_t)z * X * Y + (X - 1 - x) * Y + y;
                     dst[j] = nodes[i];
                     if (outConflict) outConflict[j] = conflict[i];
                 }
@@ -1347,11 +1360,11 @@ extern "C" int orc_plan(const orc_params* p, const float* verts, uint32_t nV, or
     bool fcc = p->node_type == ORC_SHORT_FCC || p->node_type == ORC_LONG_FCC;
     static const uint nb[5] = {1, 2, 8, 2, 4};
     if (p->node_type < 0 || p->node_type > 4) return -13;
-    if (p->rotate_x && fcc && p->node_output) return -13;   // slices of FCC lattices along x: not restated
     if (p->node_output) {
-        info->dims[0] = fcc ? 2 * pl.alloc.x : pl.alloc.x;
-        info->dims[1] = pl.alloc.y;
-        if (p->rotate_x && p->space && !fcc) std::swap(info->dims[0], info->dims[1]);   // turned back
+        const bool back = p->rotate_x && p->space;   // turned back: x and y trade places
+        const uint ax = back ? pl.alloc.y : pl.alloc.x, ay = back ? pl.alloc.x : pl.alloc.y;
+        info->dims[0] = fcc ? 2 * ax : ax;
+        info->dims[1] = ay;
         info->dims[2] = fcc ? 2 * pl.alloc.z : pl.alloc.z;
         info->out_bytes = (uint64_t)info->dims[0] * info->dims[1] * info->dims[2] * nb[p->node_type];
     } else {

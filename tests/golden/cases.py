@@ -211,6 +211,10 @@ CASES = [
          strict_mats=False, space=("slice", 0, 45)),
     case("torus_partial_slice_x", "torus", PARTIAL, 1, 1, 96, strict_mats=False, space=("slice", 0, 30)),
     case("torus_long_slice_x_oob", "torus", LONG, 1, 1, 120, space=("slice", 0, 500)),
+    case("ico4_sfcc_slice_x_mid", "ico4", SHORT_FCC, 1, 1, FCC_A, space=("slice", 0, 30)),
+    case("ico4_lfcc_slice_x_first", "ico4", LONG_FCC, 1, 0, FCC_A, space=("slice", 0, 1)),
+    case("stress_sfcc_slice_x", "stress_fcc", SHORT_FCC, 1, 1, FCC_A, vox=(64, 32, 32), mat=(32, 32, 32),
+         strict_mats=False, space=("slice", 0, 40)),
 ]
 
 BY_NAME = {c["name"]: c for c in CASES}

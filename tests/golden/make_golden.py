@@ -110,7 +110,8 @@ def run_case(f, c):
         raise RuntimeError(f"{c['name']}: plan failed rc={rc}")
     part, oob = None, False
     if c.get("space"):
-        res_y, res_z = int(dims[1]) - 2, int(dims[2]) - 2
+        fcc = c["nodes"] and c["node_type"] in (C.SHORT_FCC, C.LONG_FCC)   # FCC arrays double z
+        res_y, res_z = int(dims[1]) - 2, (int(dims[2]) // 2 if fcc else int(dims[2])) - 2
         part = (ctypes.c_uint32 * 4)(*C.partition(c, res_y, res_z))
         oob = C.slice_oob(c, res_y, res_z)
         rc = f(*args, part, rot, None, 0, dims, None)

@@ -48,9 +48,10 @@ def test_slice_argument_errors():
         full = v.plan(1, 120)
         assert parts[0][0] == 0 and parts[2][1] == full.resolution.y and parts[5][3] == full.resolution.z
     with Voxelizer(m.vertices, m.indices, node_type=SHORT_FCC) as v:
-        with pytest.raises(VxbError, match="EUNSUPPORTED"):
-            v.planSlice(1.0 / 64.0, 0, 5)   # FCC slices along x are not built
         full = v.plan(1, 1.0 / 64.0)
+        info = v.planSlice(1.0 / 64.0, 0, 5)   # FCC along x: the turned lattice turned back
+        turned = v.getArrayDimensions(1.0 / 64.0, 1024, True)
+        assert info.dims == (6, turned[1], turned[2])
         info = v.planSlice(1.0 / 64.0, 1, 5)   # FCC: x and z doubled, three voxel rows along y
         assert info.dims == (full.dims[0], 3, full.dims[2])
         info = v.planSlice(1.0 / 64.0, 2, 5)
@@ -117,14 +118,18 @@ def test_fcc_spaces_match_oracle(node_type):
     size, vox, mat = C.FCC_A, (1024, 512, 512), (512, 512, 512)
     res = O.plan(mm, node_type, 1, size, vox).resolution
     ry, rz = int(res[1]), int(res[2])
+    tres = O.plan(mm, node_type, 1, size, vox, rotate_x=True).resolution   # slices along x cut the turned grid
     with Voxelizer(mm.vertices, mm.indices, node_type=node_type) as v:
         v.setMaterials(mats, 10)
-        for direction, n in ((1, ry), (2, rz)):
+        for direction, n in ((1, ry), (2, rz), (0, int(tres[1]))):
+            rot = direction == 0
+            sy, sz = (int(tres[1]), int(tres[2])) if rot else (ry, rz)
             for s in [0, 1, n // 2, n, n + 1]:
                 got, info = v.voxelizeSliceToRAM(size, direction, s, vox, mat)
                 s0 = 0 if (s == 0 or s > n) else s - 1
-                part = (0, ry, s0, s0 + 1) if direction == 2 else (s0, s0 + 1, 0, rz)
-                want, oi = _oracle_space(mm, node_type, 1, size, vox, mat, part, oob=(s == 0 or s > n))
+                part = (0, sy, s0, s0 + 1) if direction == 2 else (s0, s0 + 1, 0, sz)
+                want, oi = _oracle_space(mm, node_type, 1, size, vox, mat, part, oob=(s == 0 or s > n),
+                                         rotate_x=rot)
                 assert info.dims == tuple(oi.dims)
                 assert np.array_equal(masked(node_type, 1, got), want), f"slice {s} along {direction}"
         for dev in [(2, 2), (3, 1)]:

@@ -321,7 +321,6 @@ void vxb_voxelizer::rotation(double* a, double* b, double* rmn, double* rmx) con
 
 int vxb_voxelizer::planXSlice(const vxb_request* r, uint32_t slice, vxb::Plan* q, bool* oob,
                               vxb_grid_info* info) const {
-    if (isFcc(nodeType)) return failf(VXB_EUNSUPPORTED, "slices of FCC lattices along x are not supported");
     double a, b, rmn[3], rmx[3];
     rotation(&a, &b, rmn, rmx);
     vxb::Plan full;
@@ -336,10 +335,11 @@ int vxb_voxelizer::planXSlice(const vxb_request* r, uint32_t slice, vxb::Plan* q
     vxb_grid_info gi;
     if ((rc = vxb::gridInfo(*q, nodeType, 1, &gi))) return rc;
     // The un-rotated array: x and y trade places (unRotateCoords,
-    // src/host_side.cpp:1160-1175).
+    // src/host_side.cpp:1160-1175, 1610-1625; an FCC array of 2X x Y x Z
+    // nodes becomes 2Y x X x Z).
     const uint32_t t = gi.dim.x;
-    gi.dim.x = gi.dim.y;
-    gi.dim.y = t;
+    gi.dim.x = isFcc(nodeType) ? 2 * gi.dim.y : gi.dim.y;
+    gi.dim.y = isFcc(nodeType) ? t / 2 : t;
     gi.location = vxb_uint3{0, 0, 0};
     if (info) *info = gi;
     return 0;
@@ -385,14 +385,28 @@ int vxb_voxelizer::runXSlice(const vxb_request* r, uint32_t slice, void* out, ui
     j.space = 1;
     for (int k = 0; k < 4; ++k) j.part[k] = q.part[k];
     j.raw = 1;
+    j.turned = 1;
     if ((rc = pipe.prepare(std::vector<vxb::MeshJob>{j}, s))) return rc;
     if ((rc = pipe.enqueue(s, &timer))) return rc;
     if ((rc = pipe.finish(s))) return rc;
     launches += pipe.launches;
+    const uint32_t nb = (uint32_t)(gi.bytes / gi.count);
+    if (isFcc(nodeType)) {
+        // fccWorker with xSlicing (src/host_side.cpp:1597-1673):
+        // restoreRotatedNodes, calculateFCCBoundaries on the un-rotated
+        // array, zeroPadding.
+        const uint32_t NX = 2 * q.alloc[0], NY = q.alloc[1], NZ = 2 * q.alloc[2];
+        vxb::launch_unrotate_fcc(xStage.p, out, NX, NY, NZ, nb, s, &launches);
+        vxb::launch_fcc_boundaries(out, 2 * NY, NX / 2, NZ, nb, s, &launches);
+        if (q.border) vxb::launch_zero_faces(out, 2 * NY, NX / 2, NZ, nb, true, s, &launches);
+        VXB_CUDA(cudaGetLastError());
+        VXB_CUDA(cudaStreamSynchronize(s));
+        busy = false;
+        return VXB_OK;
+    }
     // restoreRotatedNodes, then fillNodeList2 over the un-rotated array one
     // yz subspace at a time until no node loses its id, then zeroPadding
     // (src/host_side.cpp:1144-1223).
-    const uint32_t nb = (uint32_t)(gi.bytes / gi.count);
     const uint32_t X = q.alloc[0], Y = q.alloc[1], Z = q.alloc[2];
     vxb::launch_unrotate(xStage.p, out, X, Y, Z, nb, s, &launches);
     const uint32_t idMask = nodeType == VXB_SHORT_NODE ? 31u : 255u;
@@ -410,7 +424,7 @@ int vxb_voxelizer::runXSlice(const vxb_request* r, uint32_t slice, void* out, ui
                 VXB_CUDA(cudaStreamSynchronize(s));
                 if (!h) break;
             }
-    if (q.border) vxb::launch_zero_faces(out, Y, X, Z, nb, s, &launches);
+    if (q.border) vxb::launch_zero_faces(out, Y, X, Z, nb, false, s, &launches);
     VXB_CUDA(cudaGetLastError());
     VXB_CUDA(cudaStreamSynchronize(s));
     busy = false;

@@ -161,8 +161,14 @@ void launch_unrotate(const void* in, void* out, uint32_t X, uint32_t Y, uint32_t
 void launch_id_pass(void* nodes, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nodeBytes, uint32_t idMask,
                     uint32_t y0, uint32_t y1, uint32_t z0, uint32_t z1, uint32_t* changed, cudaStream_t s,
                     uint32_t* launches);
-void launch_zero_faces(void* nodes, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nodeBytes, cudaStream_t s,
+void launch_zero_faces(void* nodes, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nodeBytes, bool fcc, cudaStream_t s,
                        uint32_t* launches);
+// FCC lattices: unRotateNodes' FCC branch (X x Y x Z -> 2Y x X/2 x Z) and
+// calculateFCCBoundaries in place.
+void launch_unrotate_fcc(const void* in, void* out, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nodeBytes,
+                         cudaStream_t s, uint32_t* launches);
+void launch_fcc_boundaries(void* nodes, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nodeBytes, cudaStream_t s,
+                           uint32_t* launches);
 // Keys at ranks >= keysCap read as 0.
 void launch_emit_cartesian(int nodeKind, const Batch& b, uint64_t totalWords, const uint32_t* finalSolid,
                            const uint32_t* fill, const uint32_t* surf, const uint32_t* ranks, const void* keys,
@@ -174,10 +180,11 @@ struct FccMesh {
     void* out;
 };
 // FCC node grids; groupBase[m] is the first 16-byte output group of mesh m
-// (nMeshes + 1 entries).
+// (nMeshes + 1 entries).  raw: the nodes before calculateFCCBoundaries (id =
+// solid bit, the surface material), for slices along x.
 void launch_emit_fcc(int nodeKind, const Batch& b, const FccMesh* meshes, const uint64_t* groupBase,
                      uint32_t nMeshes, uint64_t totalGroups, const uint32_t* fill, const uint32_t* surf,
-                     const uint32_t* ranks, const void* keys, uint32_t keysCap, cudaStream_t s,
+                     const uint32_t* ranks, const void* keys, uint32_t keysCap, bool raw, cudaStream_t s,
                      uint32_t* launches);
 
 }  // namespace vxb

@@ -456,6 +456,7 @@ struct FccArgs {
     const uint32_t* ranks;
     const void* keys;
     uint32_t keysCap;
+    uint32_t raw;   // nodes before the boundaries: id = solid bit, no face clearing
 };
 
 // The four sub-lattice grids of one FCC mesh.
@@ -518,7 +519,9 @@ __global__ void emitFccKernel(FccArgs A, uint64_t totalGroups) {
             const uint32_t sw = G.surf[gt] ? __ldg(G.surf[gt] + w) : 0u;
             const uint32_t sb = (sw >> q) & 1u;
             uint32_t bid = 0;
-            if (fb | sb) {
+            if ((fb | sb) && A.raw) {
+                bid = 1;
+            } else if (fb | sb) {
                 const bool left = X2 > 0, right = X2 < NX - 1, in = y > 0, out = y < NY - 1;
                 const bool down = Z2 > 0, up = Z2 < NZ - 1, xe = ((X2 + Z2) & 1u) == 0;
                 const uint32_t ym = xe ? y - 1 : y;   // y - xEven
@@ -546,7 +549,7 @@ __global__ void emitFccKernel(FccArgs A, uint64_t totalGroups) {
             // zeroPadding of an FCC device space with neighbours
             // (src/voxelizer.cu:4827-4834): two node layers at the x and z
             // faces, one at the y faces.
-            const bool face = g.border && (X2 < 2 || X2 + 2 >= NX || y == 0 || y + 1 == NY || Z2 < 2 || Z2 + 2 >= NZ);
+            const bool face = g.border && !A.raw && (X2 < 2 || X2 + 2 >= NX || y == 0 || y + 1 == NY || Z2 < 2 || Z2 + 2 >= NZ);
             const uint64_t val = face ? 0ull : NT::pack(bid, mat, 0.0f);
             if (NT::bytes == 2) reinterpret_cast<uint16_t*>(&outv)[n] = (uint16_t)val;
             else reinterpret_cast<uint32_t*>(&outv)[n] = (uint32_t)val;
@@ -606,10 +609,11 @@ void launch_emit_cartesian(int nodeKind, const Batch& b, uint64_t totalWords, co
 
 void launch_emit_fcc(int nodeKind, const Batch& b, const FccMesh* meshes, const uint64_t* groupBase,
                      uint32_t nMeshes, uint64_t totalGroups, const uint32_t* fill, const uint32_t* surf,
-                     const uint32_t* ranks, const void* keys, uint32_t keysCap, cudaStream_t s,
+                     const uint32_t* ranks, const void* keys, uint32_t keysCap, bool raw, cudaStream_t s,
                      uint32_t* launches) {
     FccArgs A;
     A.keysCap = keysCap;
+    A.raw = raw ? 1u : 0u;
     A.b = b;
     A.meshes = meshes;
     A.groupBase = groupBase;

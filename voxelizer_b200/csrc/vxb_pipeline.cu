@@ -73,13 +73,17 @@ int gridInfo(const Plan& p, int nodeType, int nodes, vxb_grid_info* info) {
     return 0;
 }
 
-// Shifts of the four FCC sub-lattices (src/host_side.cpp:1438-1462).
-PassGeom makeGeom(const Plan& p, int lattice) {
+// Shifts of the four FCC sub-lattices by their slot in the FCC array (slot
+// 1 + (x & 1) + 2 (z & 1), src/host_side.cpp:1438-1462).  For a turned mesh
+// (slices along x) the reference shifts grid g by the z-swapped pattern and
+// writes it to slot (g + 1) % 4 + 1, which toggles each slot's y shift.
+PassGeom makeGeom(const Plan& p, int lattice, bool turned) {
     const double h = p.d / 2.0;
     const double sh[4][3] = {{0.0, 0.0, 0.0}, {h, h, 0.0}, {0.0, h, h}, {h, 0.0, h}};
+    const double shTurned[4][3] = {{0.0, h, 0.0}, {h, 0.0, 0.0}, {0.0, 0.0, h}, {h, h, h}};
     PassGeom g;
     for (int a = 0; a < 3; ++a) {
-        g.mn[a] = p.mn[a] + sh[lattice][a];
+        g.mn[a] = p.mn[a] + (turned ? shTurned : sh)[lattice][a];
         g.mnf[a] = (float)g.mn[a];
     }
     g.d = p.d;
@@ -136,8 +140,8 @@ int Pipeline::prepare(const std::vector<MeshJob>& jobs, cudaStream_t s) {
     wide_ = nodeKind_ == VXB_PARTIAL_NODE;
     raw_ = jobs[0].raw != 0;
     for (const MeshJob& j : jobs)
-        if ((j.raw != 0) != raw_ || (raw_ && (!j.nodes || fcc)))
-            return failf(VXB_EINVAL, "raw node output is for Cartesian node grids of a whole batch");
+        if ((j.raw != 0) != raw_ || (raw_ && !j.nodes))
+            return failf(VXB_EINVAL, "raw node output is for node grids of a whole batch");
     units_.clear();
     groups_.clear();
     std::vector<uint32_t> workBase{0};
@@ -175,7 +179,7 @@ int Pipeline::prepare(const std::vector<MeshJob>& jobs, cudaStream_t s) {
         for (int l = 0; l < lattices; ++l) {
             Unit u;
             memset(&u, 0, sizeof(u));
-            u.g = makeGeom(p, l);
+            u.g = makeGeom(p, l, fcc && j.turned);
             u.V = j.V;
             u.I = j.I;
             u.M = j.M;
@@ -421,7 +425,7 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
     }
     // Node emission.
     mark(3, false);
-    if (raw_)
+    if (raw_ && anyCartesian_)
         launch_emit_raw(nodeKind_, b, totalWords_, fillP, surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_,
                         s, &launches);
     else if (anyCartesian_) {
@@ -433,7 +437,7 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
     if (nFcc_)
         launch_emit_fcc(nodeKind_, b, reinterpret_cast<const FccMesh*>(tables.as<uint8_t>() + oFcc_),
                         reinterpret_cast<const uint64_t*>(tables.as<uint8_t>() + oGroupBase_), nFcc_, totalGroups_,
-                        fillP, surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_, s, &launches);
+                        fillP, surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_, raw_, s, &launches);
     mark(3, true);
     VXB_CUDA(cudaGetLastError());
     return 0;
@@ -565,7 +569,7 @@ int Pipeline::finish(cudaStream_t s) {
         }
     }
     if (reemit) {
-        if (raw_)
+        if (raw_ && anyCartesian_)
             launch_emit_raw(nodeKind_, b, totalWords_, fillP, surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p,
                             keysCap_, s, &launches);
         else if (anyCartesian_)
@@ -574,7 +578,8 @@ int Pipeline::finish(cudaStream_t s) {
         if (nFcc_)
             launch_emit_fcc(nodeKind_, b, reinterpret_cast<const FccMesh*>(tables.as<uint8_t>() + oFcc_),
                             reinterpret_cast<const uint64_t*>(tables.as<uint8_t>() + oGroupBase_), nFcc_,
-                            totalGroups_, fillP, surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_, s, &launches);
+                            totalGroups_, fillP, surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_, raw_, s,
+                            &launches);
         VXB_CUDA(cudaGetLastError());
         VXB_CUDA(cudaStreamSynchronize(s));
     }

@@ -36,6 +36,9 @@ struct MeshJob {
     // surface material and ratio), no pruning: the first half of a slice
     // along x.  All jobs of a batch share it.
     int raw = 0;
+    // The mesh is turned about z (slices along x): FCC sub-lattices take the
+    // turned shifts.
+    int turned = 0;
 };
 
 // Shape of a job's result (vxb_plan).  Returns 0 or a vxb status.

@@ -9,7 +9,9 @@
 //  * unRotateNodes (src/voxelizer.cu:2061-2124), the boundary-id passes of
 //    fillNodeList2 (1790-1913) over the un-rotated array, in place, one yz
 //    subspace at a time until no node loses its id, and zeroPadding
-//    (4811-4844).
+//    (4811-4844);
+//  * for FCC lattices, unRotateNodes' FCC branch, calculateFCCBoundaries
+//    (1929-2048) on the un-rotated array and zeroPadding's FCC branch.
 // Slices are small (three node layers), so these are plain node-per-thread
 // kernels.
 
@@ -17,6 +19,8 @@
 #include "vxb_device.cuh"
 #include "vxb_kernels.cuh"
 #include "vxb_ratio.cuh"
+
+#include <type_traits>
 
 namespace vxb {
 
@@ -116,13 +120,67 @@ __global__ void idPassKernel(uint8_t* nodes, uint32_t X, uint32_t Y, uint32_t Z,
     }
 }
 
-// zeroPadding: every node on a face of the array becomes zero.
-__global__ void zeroFacesKernel(uint8_t* nodes, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nb) {
+// zeroPadding: every node on a face of the array becomes zero; FCC arrays
+// lose two node layers at the x and z faces (src/voxelizer.cu:4811-4844).
+__global__ void zeroFacesKernel(uint8_t* nodes, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nb, uint32_t fcc) {
+    const uint64_t n = (uint64_t)X * Y * Z;
+    const uint32_t w = fcc ? 2u : 1u;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t x = (uint32_t)(i % X), y = (uint32_t)(i / X % Y), z = (uint32_t)(i / X / Y);
+        if (x < w || x + w >= X || y == 0 || y + 1 == Y || z < w || z + w >= Z)
+            for (uint32_t k = 0; k < nb; ++k) nodes[i * nb + k] = 0;
+    }
+}
+
+// unRotateNodes, FCC branch (src/voxelizer.cu:2104-2110): node (x, y, z) of
+// the turned X x Y x Z FCC array goes to (2y + (x + z + 1) % 2, X / 2 - 1 -
+// x / 2, z) of the 2Y x X/2 x Z array.
+__global__ void unrotateFccKernel(const uint8_t* __restrict__ in, uint8_t* __restrict__ out, uint32_t X, uint32_t Y,
+                                  uint32_t Z, uint32_t nb) {
     const uint64_t n = (uint64_t)X * Y * Z;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t x = (uint32_t)(i % X), y = (uint32_t)(i / X % Y), z = (uint32_t)(i / X / Y);
-        if (x == 0 || x + 1 == X || y == 0 || y + 1 == Y || z == 0 || z + 1 == Z)
-            for (uint32_t k = 0; k < nb; ++k) nodes[i * nb + k] = 0;
+        const uint32_t nx = 2 * y + (x + z + 1) % 2, ny = X / 2 - 1 - x / 2;
+        const uint64_t j = (uint64_t)X * Y * z + (uint64_t)(2 * Y) * ny + nx;
+        for (uint32_t k = 0; k < nb; ++k) out[j * nb + k] = in[i * nb + k];
+    }
+}
+
+// calculateFCCBoundaries (src/voxelizer.cu:1929-2048) in place over an X x Y
+// x Z FCC node array of 2-byte (12-bit id) or 4-byte (16-bit id) nodes: a
+// solid node's id becomes the mask of its solid FCC neighbours.  A node
+// whose mask is zero has no solid neighbour, so no other node reads it; the
+// in-place pass equals a snapshot evaluation.
+template <int NB>
+__global__ void fccBoundaryKernel(uint8_t* nodes, uint32_t X, uint32_t Y, uint32_t Z) {
+    typedef typename std::conditional<NB == 2, uint16_t, uint32_t>::type T;
+    constexpr uint32_t kId = NB == 2 ? 0x0FFFu : 0xFFFFu;
+    T* v = reinterpret_cast<T*>(nodes);
+    const uint64_t n = (uint64_t)X * Y * Z;
+    const uint64_t px = 1, py = X, pz = (uint64_t)X * Y;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const T cur = v[i];
+        if ((cur & kId) == 0) continue;
+        const uint32_t x = (uint32_t)(i % X), y = (uint32_t)(i / X % Y), z = (uint32_t)(i / X / Y);
+        const bool left = x > 0, right = x + 1 < X, in = y > 0, out = y + 1 < Y, down = z > 0, up = z + 1 < Z;
+        const bool xe = ((x + z) & 1u) == 0;
+        const bool cIn = (xe && in) || !xe, cOut = (!xe && out) || xe;
+        const uint64_t ye = xe ? py : 0, yo = xe ? 0 : py;
+        auto on = [&](uint64_t j) { return (v[j] & kId) != 0; };
+        uint32_t b = 0;
+        if (down && cIn && on(i - pz - ye)) b |= 1u;
+        if (down && left && on(i - pz - px)) b |= 2u;
+        if (down && right && on(i - pz + px)) b |= 4u;
+        if (down && cOut && on(i - pz + yo)) b |= 8u;
+        if (left && cIn && on(i - px - ye)) b |= 16u;
+        if (right && cIn && on(i + px - ye)) b |= 32u;
+        if (left && cOut && on(i - px + yo)) b |= 64u;
+        if (right && cOut && on(i + px + yo)) b |= 128u;
+        if (up && cIn && on(i + pz - ye)) b |= 256u;
+        if (up && left && on(i + pz - px)) b |= 512u;
+        if (up && right && on(i + pz + px)) b |= 1024u;
+        if (up && cOut && on(i + pz + yo)) b |= 2048u;
+        v[i] = (T)((cur & ~(T)kId) | (T)b);
     }
 }
 
@@ -160,10 +218,25 @@ void launch_id_pass(void* nodes, uint32_t X, uint32_t Y, uint32_t Z, uint32_t no
     *launches += 1;
 }
 
-void launch_zero_faces(void* nodes, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nodeBytes, cudaStream_t s,
+void launch_zero_faces(void* nodes, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nodeBytes, bool fcc, cudaStream_t s,
                        uint32_t* launches) {
     zeroFacesKernel<<<gridFor((uint64_t)X * Y * Z, 256, 148u * 8u), 256, 0, s>>>(static_cast<uint8_t*>(nodes), X, Y,
-                                                                                  Z, nodeBytes);
+                                                                                  Z, nodeBytes, fcc ? 1u : 0u);
+    *launches += 1;
+}
+
+void launch_unrotate_fcc(const void* in, void* out, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nodeBytes,
+                         cudaStream_t s, uint32_t* launches) {
+    unrotateFccKernel<<<gridFor((uint64_t)X * Y * Z, 256, 148u * 8u), 256, 0, s>>>(
+        static_cast<const uint8_t*>(in), static_cast<uint8_t*>(out), X, Y, Z, nodeBytes);
+    *launches += 1;
+}
+
+void launch_fcc_boundaries(void* nodes, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nodeBytes, cudaStream_t s,
+                           uint32_t* launches) {
+    const uint32_t grid = gridFor((uint64_t)X * Y * Z, 256, 148u * 8u);
+    if (nodeBytes == 2) fccBoundaryKernel<2><<<grid, 256, 0, s>>>(static_cast<uint8_t*>(nodes), X, Y, Z);
+    else fccBoundaryKernel<4><<<grid, 256, 0, s>>>(static_cast<uint8_t*>(nodes), X, Y, Z);
     *launches += 1;
 }
 
