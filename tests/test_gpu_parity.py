@@ -21,7 +21,8 @@ import cases as C
 import oracle as O
 from helpers import (CONFLICT_MAT, CONFLICT_RATIO, PARTIAL, RATIO_REF_TOL, RATIO_TOL, RATIO_UNSTABLE, bid_of,
                      bit_rows_mask, describe_diff, mat_of, masked, oracle_case, ratio_bad, ratio_of)
-from voxelizer_b200.api import Voxelizer
+from voxelizer_b200.api import LONG, SHORT, Voxelizer
+from voxelizer_b200.scenes import Mesh
 
 pytestmark = pytest.mark.gpu
 
@@ -155,3 +156,25 @@ def test_device_entry_matches_host_entry():
         s.synchronize()
         assert v.last_launch_count() > 0
     assert np.array_equal(dev.cpu().numpy().view(np.uint16), host)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [0, 1])
+def test_triangle_soup_pruning_matches_oracle(seed):
+    """Random overlapping triangles (thin, self-intersecting solids whose
+    pruning cascades over several passes) in many small yz subspaces: the
+    node grid equals the oracle's bit for bit."""
+    rng = np.random.default_rng(seed)
+    n = 4000
+    centres = rng.uniform(0.0, 1.0, size=(n, 1, 3))
+    v = (centres + rng.normal(scale=0.04, size=(n, 3, 3))).reshape(-1, 3).astype(np.float32)
+    f = np.arange(3 * n, dtype=np.uint32).reshape(n, 3)
+    m = Mesh(v, f, None, 0)
+    size, vox = 96, (1024, 8, 8)
+    for nt in (SHORT, LONG):
+        with Voxelizer(m.vertices, m.indices, node_type=nt) as vx:
+            got, info = vx.voxelizeToNodesToRAM(size, vox)
+        want, oi, _ = O.voxelize(m, nt, 1, 0, size, vox)
+        assert info.dims == tuple(oi.dims)
+        assert np.array_equal(got, want), describe_diff(got, want, info.dims)
+        assert np.count_nonzero(bid_of(nt, got))

@@ -143,6 +143,16 @@ void launch_prune(const Batch& b, const PruneRegion* regions, uint32_t n, uint32
                   const uint32_t* fill, const uint32_t* surf, uint32_t* flags, uint32_t flagBase, uint32_t passes,
                   unsigned long long* list, uint32_t* count, uint32_t cap, uint32_t* overflow, cudaStream_t s,
                   uint32_t* launches);
+// Passes firstPass .. passes - 1 of one subspace index in one block-sized
+// launch (lists alternating between list0 and list1, counts[p] the count of
+// pass p); it stops at an empty list, and a list longer than escapeAt marks
+// all nRegions regions as changed in the last pass (the host then runs full
+// passes until stable).
+void launch_prune_list_loop(const Batch& b, const PruneRegion* regions, uint32_t nRegions, uint32_t* solid,
+                            const uint32_t* fill, const uint32_t* surf, uint32_t* flags, uint32_t flagBase,
+                            uint32_t passes, uint32_t firstPass, unsigned long long* list0, unsigned long long* list1,
+                            uint32_t* counts, uint32_t cap, uint32_t escapeAt, uint32_t* overflow, cudaStream_t s,
+                            uint32_t* launches);
 void launch_prune_list(const Batch& b, const PruneRegion* regions, uint32_t* solid, const uint32_t* fill,
                        const uint32_t* surf, uint32_t* flags, uint32_t flagBase, uint32_t passes, uint32_t pass,
                        const unsigned long long* in, const uint32_t* inCount, unsigned long long* out,

@@ -76,24 +76,27 @@ __device__ __forceinline__ PruneView pruneView(const Batch& b, const PruneRegion
 }
 
 // The pruned value of word (k, y, z) given its current neighbourhood.
+// kFresh reads the solid words past L1.
+template <bool kFresh = false>
 __device__ __forceinline__ uint32_t prunedWord(const PruneView& v, uint32_t w, uint32_t idx, uint32_t k, uint32_t y,
                                                uint32_t z) {
-    const uint32_t* S = v.S;
+    uint32_t* S = v.S;
+    auto ld = [&](uint32_t i) { return kFresh ? __ldcg(S + i) : S[i]; };
     const uint32_t plane = v.ipx * v.AY;
-    const uint32_t prev = k > 0 ? S[idx - 1] : 0u;
-    const uint32_t next = k + 1 < v.ipx ? S[idx + 1] : 0u;
+    const uint32_t prev = k > 0 ? ld(idx - 1) : 0u;
+    const uint32_t next = k + 1 < v.ipx ? ld(idx + 1) : 0u;
     const uint32_t L = (w >> 1) | (prev << 31), Rt = (w << 1) | (next >> 31);
-    const uint32_t In = y > 0 ? S[idx - v.ipx] : 0u;
+    const uint32_t In = y > 0 ? ld(idx - v.ipx) : 0u;
     uint32_t Out = 0u, Up = 0u;
     if (y + 1 < v.AY) {
         if (v.yLater[y]) Out = __ldg(v.F + idx + v.ipx) | (v.Sf ? __ldg(v.Sf + idx + v.ipx) : 0u);
-        else Out = S[idx + v.ipx];
+        else Out = ld(idx + v.ipx);
     }
-    const uint32_t Dn = z > 0 ? S[idx - plane] : 0u;
+    const uint32_t Dn = z > 0 ? ld(idx - plane) : 0u;
     if (z + 1 < v.AZ) {
         const uint8_t* zLater = v.yLater + v.AY;
         if (zLater[z]) Up = __ldg(v.F + idx + plane) | (v.Sf ? __ldg(v.Sf + idx + plane) : 0u);
-        else Up = S[idx + plane];
+        else Up = ld(idx + plane);
     }
     return w & (L | Rt) & (In | Out) & (Dn | Up);
 }
@@ -163,6 +166,45 @@ __global__ void pruneKernel(Batch b, const PruneRegion* __restrict__ regions, ui
     if (dirty != 0xFFFFFFFFu && lane == (uint32_t)(__ffs(peers) - 1)) atomicOr(flags + (flagBase + dirty) * passes, 1u);
 }
 
+// One entry of a list pass (pass >= 1): the listed word and its six
+// neighbours inside the region's subspace.  kFresh reads the solid words
+// past L1 (passes of one launch see the previous pass's atomics).
+template <bool kFresh>
+__device__ __forceinline__ void pruneListEntry(const Batch& b, const PruneRegion* __restrict__ regions,
+                                               uint32_t* solid, const uint32_t* __restrict__ fill,
+                                               const uint32_t* __restrict__ surf, uint32_t* flags, uint32_t flagBase,
+                                               uint32_t passes, uint32_t pass, unsigned long long ent,
+                                               unsigned long long* out, uint32_t* outCount, uint32_t cap,
+                                               uint32_t* overflow) {
+    const uint32_t rg = (uint32_t)(ent >> 32), c = (uint32_t)ent;
+    const PruneView v = pruneView(b, regions[rg], solid, fill, surf);
+    const uint32_t plane = v.ipx * v.AY;
+    const uint32_t cz = c / plane, rem = c - cz * plane, cy = rem / v.ipx, ck = rem - cy * v.ipx;
+    bool changed = false;
+#pragma unroll 1
+    for (int q = 0; q < 7; ++q) {
+        uint32_t k = ck, y = cy, z = cz;
+        if (q == 1) { if (k == 0) continue; --k; }
+        else if (q == 2) { if (k + 1 >= v.ipx) continue; ++k; }
+        else if (q == 3) { if (y == v.y0) continue; --y; }
+        else if (q == 4) { if (y + 1 >= v.y1) continue; ++y; }
+        else if (q == 5) { if (z == v.z0) continue; --z; }
+        else if (q == 6) { if (z + 1 >= v.z1) continue; ++z; }
+        const uint32_t idx = (z * v.AY + y) * v.ipx + k;
+        const uint32_t w = kFresh ? __ldcg(v.S + idx) : v.S[idx];
+        if (w == 0) continue;
+        const uint32_t nw = prunedWord<kFresh>(v, w, idx, k, y, z);
+        if (nw != w) {
+            const uint32_t old = atomicAnd(v.S + idx, nw);
+            if (old & ~nw) {
+                listAppend(out, outCount, cap, overflow, rg, idx);
+                changed = true;
+            }
+        }
+    }
+    if (changed) atomicOr(flags + (flagBase + rg) * passes + pass, 1u);
+}
+
 // Pass `pass` >= 1: the words next to the previous pass's changes (and the
 // changed words themselves), inside their region's subspace.
 __global__ void pruneListKernel(Batch b, const PruneRegion* __restrict__ regions, uint32_t* solid,
@@ -171,35 +213,38 @@ __global__ void pruneListKernel(Batch b, const PruneRegion* __restrict__ regions
                                 const unsigned long long* __restrict__ in, const uint32_t* __restrict__ inCount,
                                 unsigned long long* out, uint32_t* outCount, uint32_t cap, uint32_t* overflow) {
     const uint32_t nIn = min(*inCount, cap);
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < nIn; e += gridDim.x * blockDim.x) {
-        const unsigned long long ent = in[e];
-        const uint32_t rg = (uint32_t)(ent >> 32), c = (uint32_t)ent;
-        const PruneView v = pruneView(b, regions[rg], solid, fill, surf);
-        const uint32_t plane = v.ipx * v.AY;
-        const uint32_t cz = c / plane, rem = c - cz * plane, cy = rem / v.ipx, ck = rem - cy * v.ipx;
-        bool changed = false;
-#pragma unroll 1
-        for (int q = 0; q < 7; ++q) {
-            uint32_t k = ck, y = cy, z = cz;
-            if (q == 1) { if (k == 0) continue; --k; }
-            else if (q == 2) { if (k + 1 >= v.ipx) continue; ++k; }
-            else if (q == 3) { if (y == v.y0) continue; --y; }
-            else if (q == 4) { if (y + 1 >= v.y1) continue; ++y; }
-            else if (q == 5) { if (z == v.z0) continue; --z; }
-            else if (q == 6) { if (z + 1 >= v.z1) continue; ++z; }
-            const uint32_t idx = (z * v.AY + y) * v.ipx + k;
-            const uint32_t w = v.S[idx];
-            if (w == 0) continue;
-            const uint32_t nw = prunedWord(v, w, idx, k, y, z);
-            if (nw != w) {
-                const uint32_t old = atomicAnd(v.S + idx, nw);
-                if (old & ~nw) {
-                    listAppend(out, outCount, cap, overflow, rg, idx);
-                    changed = true;
-                }
-            }
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < nIn; e += gridDim.x * blockDim.x)
+        pruneListEntry<false>(b, regions, solid, fill, surf, flags, flagBase, passes, pass, in[e], out, outCount, cap,
+                              overflow);
+}
+
+// Passes firstPass .. passes - 1 in one block with a block barrier between
+// passes (the lists alternate as they do between single-pass launches).  It
+// stops once a list is empty.  A list longer than `escapeAt` is left to the
+// host: every region of the subspace index is marked as changed in the last
+// pass, so the host runs full passes until the index is stable.
+__global__ void __launch_bounds__(1024) pruneListLoopKernel(Batch b, const PruneRegion* __restrict__ regions,
+                                                            uint32_t nRegions, uint32_t* solid,
+                                                            const uint32_t* __restrict__ fill,
+                                                            const uint32_t* __restrict__ surf, uint32_t* flags,
+                                                            uint32_t flagBase, uint32_t passes, uint32_t firstPass,
+                                                            unsigned long long* list0, unsigned long long* list1,
+                                                            uint32_t* counts, uint32_t cap, uint32_t escapeAt,
+                                                            uint32_t* overflow) {
+    for (uint32_t pass = firstPass; pass < passes; ++pass) {
+        __syncthreads();
+        const uint32_t nIn = min(*reinterpret_cast<volatile uint32_t*>(counts + pass - 1), cap);
+        if (nIn == 0) return;
+        if (nIn > escapeAt) {
+            for (uint32_t r = threadIdx.x; r < nRegions; r += blockDim.x)
+                atomicOr(flags + (flagBase + r) * passes + passes - 1, 1u);
+            return;
         }
-        if (changed) atomicOr(flags + (flagBase + rg) * passes + pass, 1u);
+        const unsigned long long* in = (pass - 1) & 1u ? list1 : list0;
+        unsigned long long* out = pass & 1u ? list1 : list0;
+        for (uint32_t e = threadIdx.x; e < nIn; e += blockDim.x)
+            pruneListEntry<true>(b, regions, solid, fill, surf, flags, flagBase, passes, pass, __ldcg(in + e), out,
+                                 counts + pass, cap, overflow);
     }
 }
 
@@ -575,6 +620,16 @@ void launch_prune(const Batch& b, const PruneRegion* regions, uint32_t n, uint32
     pruneKernel<<<gridFor(groupWords, 256, 148u * 8u), 256, 0, s>>>(b, regions, n, groupWords, solid, fill, surf,
                                                                     flags, flagBase, passes, list, count, cap,
                                                                     overflow);
+    *launches += 1;
+}
+
+void launch_prune_list_loop(const Batch& b, const PruneRegion* regions, uint32_t nRegions, uint32_t* solid,
+                            const uint32_t* fill, const uint32_t* surf, uint32_t* flags, uint32_t flagBase,
+                            uint32_t passes, uint32_t firstPass, unsigned long long* list0, unsigned long long* list1,
+                            uint32_t* counts, uint32_t cap, uint32_t escapeAt, uint32_t* overflow, cudaStream_t s,
+                            uint32_t* launches) {
+    pruneListLoopKernel<<<1, 1024, 0, s>>>(b, regions, nRegions, solid, fill, surf, flags, flagBase, passes, firstPass,
+                                           list0, list1, counts, cap, escapeAt, overflow);
     *launches += 1;
 }
 

@@ -400,10 +400,13 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
             uint32_t* c = counts + gi * kPasses;
             launch_prune(b, regions + gr.first, gr.count, gr.words, fin.as<uint32_t>(), fillP, surfP, st + kFlags,
                          gr.flagBase, kPasses, lists[0], c, pruneCap_, overflow, s, &launches);
-            for (uint32_t pass = 1; pass < kPasses; ++pass)
-                launch_prune_list(b, regions + gr.first, fin.as<uint32_t>(), fillP, surfP, st + kFlags, gr.flagBase,
-                                  kPasses, pass, lists[(pass - 1) & 1], c + pass - 1, lists[pass & 1], c + pass,
-                                  pruneCap_, overflow, s, &launches);
+            // Pass 1 over the whole device; later lists are short (usually
+            // empty), so passes 2 .. kPasses - 1 run in one block.
+            launch_prune_list(b, regions + gr.first, fin.as<uint32_t>(), fillP, surfP, st + kFlags, gr.flagBase,
+                              kPasses, 1, lists[0], c, lists[1], c + 1, pruneCap_, overflow, s, &launches);
+            launch_prune_list_loop(b, regions + gr.first, gr.count, fin.as<uint32_t>(), fillP, surfP, st + kFlags,
+                                   gr.flagBase, kPasses, 2, lists[0], lists[1], c, pruneCap_, kLoopListMax, overflow, s,
+                                   &launches);
         }
         mark(2, true);
     }

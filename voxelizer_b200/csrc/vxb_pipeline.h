@@ -79,6 +79,7 @@ public:
     vxb_stats stats{};
 
     static constexpr uint32_t kPasses = 8;   // pruning passes queued per subspace
+    static constexpr uint32_t kLoopListMax = 32768;   // longest list the one-block passes take
 
     // Launch shape of the last enqueue (the autotuner's choice).
     LaunchShape shape{};
