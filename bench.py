@@ -439,7 +439,9 @@ def run_served(args, world, rank, local):
                 srv.release(req)
                 return t
 
-            _drive(submit, wait, pool[:8], _poisson(1000, 16, rng))   # warm-up
+            # Warm-up at the measured rate over the whole pool: the lanes'
+            # batch buffers grow to the sizes this load needs before timing.
+            _drive(submit, wait, pool, _poisson(rate, min(len(pool), n), rng))
             lat_s, span_s = _drive(submit, wait, pool, arrivals)
             batches = srv.batches
         # Plain path: one worker, one call per request, in arrival order.
