@@ -153,6 +153,23 @@ def _reference_cuda():
     return f, lib
 
 
+def max_over_ranks(x, dist):
+    """The largest x over the ranks of the process group (a job's time is
+    its slowest replica's).  NCCL reduces a device tensor, gloo a host one."""
+    import torch
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(units_per_replica, world, ms):
+    """Whole-job units per second: every replica processes the same units
+    in (at most) `ms` milliseconds."""
+    return units_per_replica * world / (ms * 1e-3)
+
+
 def run_reference_cuda(args, world, ref):
     """Full workload through the reference's CUDA path on cuda:0: host arrays
     in, node grid back in host memory, wall clock per call (the reference's
@@ -592,12 +609,10 @@ def main():
     torch.cuda.synchronize()
     total_ms = sum(a.elapsed_time(b) for a, b in evs)
     if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = max_over_ranks(total_ms, dist)
         dist.barrier()
     ms = total_ms / args.steps
-    value = n_nodes * world / (ms * 1e-3) / 1e9
+    value = replica_throughput(n_nodes, world, ms) / 1e9
 
     # e2e through the reference-facing entry with host buffers.
     vx.set_profiling(False)
@@ -616,10 +631,8 @@ def main():
             e2e_ms.append(1e3 * (time.perf_counter() - t0))
     e2e = sorted(e2e_ms)[len(e2e_ms) // 2]   # median: the PCIe copy of a shared host varies
     if dist:
-        t = torch.tensor([e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e = float(t.item())
-    e2e_value = n_nodes * world / (e2e * 1e-3) / 1e9
+        e2e = max_over_ranks(e2e, dist)
+    e2e_value = replica_throughput(n_nodes, world, e2e) / 1e9
 
     peak, peak_kind = peaks()
     stats = vx.last_stats()
