@@ -171,10 +171,35 @@ def test_triangle_soup_pruning_matches_oracle(seed):
     f = np.arange(3 * n, dtype=np.uint32).reshape(n, 3)
     m = Mesh(v, f, None, 0)
     size, vox = 96, (1024, 8, 8)
+    import torch
+
     for nt in (SHORT, LONG):
         with Voxelizer(m.vertices, m.indices, node_type=nt) as vx:
             got, info = vx.voxelizeToNodesToRAM(size, vox)
+            pinned = torch.empty(int(info.bytes), dtype=torch.uint8).pin_memory().numpy().view(got.dtype)
+            streamed, _ = vx.voxelizeToNodesToRAM(size, vox, out=pinned)
         want, oi, _ = O.voxelize(m, nt, 1, 0, size, vox)
         assert info.dims == tuple(oi.dims)
         assert np.array_equal(got, want), describe_diff(got, want, info.dims)
+        assert np.array_equal(streamed, want)
         assert np.count_nonzero(bid_of(nt, got))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["room_lite_long", "torus_short_splits", "ico4_partial_mat", "ico4_sfcc_mat"])
+def test_pinned_host_output_matches(name):
+    """A pinned host buffer takes the node array range by range while it is
+    emitted (copies overlapped with the emission); the bytes equal the
+    pageable path's."""
+    import torch
+
+    c = C.BY_NAME[name]
+    m, v = make_voxelizer(c)
+    with v:
+        want, info = v.voxelizeToNodesToRAM(c["size"], c["vox"], c["mat"])
+        pinned = torch.empty(int(info.bytes), dtype=torch.uint8).pin_memory().numpy().view(want.dtype)
+        for _ in range(2):
+            pinned[:] = 0
+            got, _ = v.voxelizeToNodesToRAM(c["size"], c["vox"], c["mat"], out=pinned)
+            assert got.ctypes.data == pinned.ctypes.data
+            assert np.array_equal(masked(c["node_type"], 1, got), masked(c["node_type"], 1, want))

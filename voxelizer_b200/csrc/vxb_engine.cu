@@ -44,6 +44,10 @@ struct vxb_voxelizer {
     bool meshOnDevice = false, matsOnDevice = false;
     bool hasMaterials = false;   // setMaterials was called (materials live on the host or the device)
     vxb::DevBuf dV, dI, dM, outStage, dCheck;
+    cudaStream_t copyStream = nullptr;   // device-to-host copies of streamed output
+    ~vxb_voxelizer() {
+        if (copyStream) cudaStreamDestroy(copyStream);
+    }
     // Slices along x: the rotated mesh (made on the first such call) and the
     // rotated slice's node array before the boundary ids.
     vxb::DevBuf dVrot, xStage, xFlag;
@@ -769,8 +773,20 @@ vxb_status vxb_voxelize_to_host(vxb_voxelizer* v, int nodes, const vxb_request* 
     if (host_bytes < gi.bytes) return failf(VXB_EINVAL, "output buffer too small");
     VXB_CUDA(cudaSetDevice(v->device));
     if ((rc = v->outStage.ensure(gi.bytes))) return rc;
+    // A pinned destination takes the node array range by range while it is
+    // emitted (the copy overlaps the rest of the emission).
+    cudaPointerAttributes pa;
+    const bool pinned = cudaPointerGetAttributes(&pa, host_out) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    if (pinned && !v->copyStream) VXB_CUDA(cudaStreamCreateWithFlags(&v->copyStream, cudaStreamNonBlocking));
+    v->pipe.streamOutput(pinned && nodes ? host_out : nullptr, gi.bytes, v->copyStream);
     rc = v->run(nodes, req, v->outStage.p, gi.bytes, 0, info);
-    if (rc == 0) {
+    const bool copied = v->pipe.hostCopied();
+    v->pipe.streamOutput(nullptr, 0, nullptr);
+    if (copied) {
+        cudaError_t e = cudaStreamSynchronize(v->copyStream);
+        if (rc == 0 && e != cudaSuccess) rc = failf(VXB_ECUDA, "%s", cudaGetErrorString(e));
+    } else if (rc == 0) {
         cudaError_t e = cudaMemcpy(host_out, v->outStage.p, gi.bytes, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) rc = failf(VXB_ECUDA, "%s", cudaGetErrorString(e));
     }

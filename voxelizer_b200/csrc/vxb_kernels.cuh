@@ -180,7 +180,9 @@ void launch_unrotate_fcc(const void* in, void* out, uint32_t X, uint32_t Y, uint
 void launch_fcc_boundaries(void* nodes, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nodeBytes, cudaStream_t s,
                            uint32_t* launches);
 // Keys at ranks >= keysCap read as 0.
-void launch_emit_cartesian(int nodeKind, const Batch& b, uint64_t totalWords, const uint32_t* finalSolid,
+// Words [wordBegin, totalWords) of the arena (wordBegin a multiple of 32).
+void launch_emit_cartesian(int nodeKind, const Batch& b, uint64_t wordBegin, uint64_t totalWords,
+                           const uint32_t* finalSolid,
                            const uint32_t* fill, const uint32_t* surf, const uint32_t* ranks, const void* keys,
                            uint32_t keysCap, uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches);
 

@@ -342,7 +342,7 @@ __device__ __forceinline__ uint32_t permOf(const WordNbrs& n, uint32_t q) {
 // one.  The warp's 32 rows are then stored as one contiguous span.  Unit
 // word bases are multiples of 32, so a warp's words belong to one unit.
 template <int K>
-__global__ void __launch_bounds__(256, 6) emitNarrowKernel(EmitArgs a, uint64_t totalWords) {
+__global__ void __launch_bounds__(256, 6) emitNarrowKernel(EmitArgs a, uint64_t wordBegin, uint64_t totalWords) {
     typedef NodeT<K> NT;
     static_assert(NT::bytes <= 2, "narrow nodes only");
     constexpr int NB = NT::bytes;
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(256, 6) emitNarrowKernel(EmitArgs a, uint64_t 
     uint64_t uBase = 0;
     uint8_t* uOut = nullptr;
     UnitWords uw{};
-    for (uint64_t gbase = ((uint64_t)blockIdx.x * 8u + warp) * 32u; gbase < totalWords;
+    for (uint64_t gbase = wordBegin + ((uint64_t)blockIdx.x * 8u + warp) * 32u; gbase < totalWords;
          gbase += (uint64_t)gridDim.x * 8u * 32u) {
         const uint32_t u = a.b.nUnits > 1 ? unitOf(a.b.wordBase, a.b.nUnits, gbase) : 0u;
         if (u != cur) {
@@ -439,12 +439,12 @@ __global__ void __launch_bounds__(256, 6) emitNarrowKernel(EmitArgs a, uint64_t 
 // 8-byte PartialNodes: one lane per word, nodes stored from registers.  The
 // ratio of a node is 1 where the parity fill is set and the node is not a
 // surface node.
-__global__ void __launch_bounds__(256) emitPartialKernel(EmitArgs a, uint64_t totalWords) {
+__global__ void __launch_bounds__(256) emitPartialKernel(EmitArgs a, uint64_t wordBegin, uint64_t totalWords) {
     typedef NodeT<kPartial> NT;
     __shared__ uint8_t lut[64];
     if (threadIdx.x < 64) lut[threadIdx.x] = kOrientTable[threadIdx.x];
     __syncthreads();
-    for (uint64_t gw = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gw < totalWords;
+    for (uint64_t gw = wordBegin + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gw < totalWords;
          gw += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t u = unitOf(a.b.wordBase, a.b.nUnits, gw);
         const Unit& U = a.b.units[u];
@@ -642,7 +642,8 @@ void launch_prune_list(const Batch& b, const PruneRegion* regions, uint32_t* sol
     *launches += 1;
 }
 
-void launch_emit_cartesian(int nodeKind, const Batch& b, uint64_t totalWords, const uint32_t* finalSolid,
+void launch_emit_cartesian(int nodeKind, const Batch& b, uint64_t wordBegin, uint64_t totalWords,
+                           const uint32_t* finalSolid,
                            const uint32_t* fill, const uint32_t* surf, const uint32_t* ranks, const void* keys,
                            uint32_t keysCap, uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches) {
     EmitArgs a;
@@ -653,11 +654,12 @@ void launch_emit_cartesian(int nodeKind, const Batch& b, uint64_t totalWords, co
     a.surf = surf;
     a.ranks = ranks;
     a.keys = keys;
-    const uint32_t grid = gridFor(totalWords, 256, 148u * blocksPerSm);
+    const uint64_t words = totalWords - wordBegin;
+    const uint32_t grid = gridFor(words, 256, 148u * blocksPerSm);
     switch (nodeKind) {
-    case kShort: emitNarrowKernel<kShort><<<grid, 256, 0, s>>>(a, totalWords); break;
-    case kLong: emitNarrowKernel<kLong><<<grid, 256, 0, s>>>(a, totalWords); break;
-    default: emitPartialKernel<<<gridFor(totalWords, 256, 148u * 8u), 256, 0, s>>>(a, totalWords); break;
+    case kShort: emitNarrowKernel<kShort><<<grid, 256, 0, s>>>(a, wordBegin, totalWords); break;
+    case kLong: emitNarrowKernel<kLong><<<grid, 256, 0, s>>>(a, wordBegin, totalWords); break;
+    default: emitPartialKernel<<<gridFor(words, 256, 148u * 8u), 256, 0, s>>>(a, wordBegin, totalWords); break;
     }
     *launches += 1;
 }

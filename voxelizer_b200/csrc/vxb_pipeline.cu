@@ -433,8 +433,31 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
                         s, &launches);
     else if (anyCartesian_) {
         tuneMark(kKnobEmit, false, s);
-        launch_emit_cartesian(nodeKind_, b, totalWords_, fin.as<uint32_t>(), fillP, surf.as<uint32_t>(),
-                              ranks.as<uint32_t>(), keys.p, keysCap_, shape.emitBlocksPerSm, s, &launches);
+        if (hostOut_ && units_.size() == 1) {
+            // The node array in kOutChunks word ranges, each copied to the
+            // caller's pinned host buffer on the copy stream as soon as it
+            // is written, so the copy of the first ranges overlaps the rest.
+            const Unit& u = units_[0];
+            const uint64_t words = (uint64_t)u.g.ipx * u.g.AY * u.g.AZ;
+            const uint64_t wordBytes = hostBytes_ / words;
+            for (uint32_t k = 0; k < kOutChunks; ++k) {
+                const uint64_t w0 = (words * k / kOutChunks) & ~uint64_t(31);
+                const uint64_t w1 = k + 1 == kOutChunks ? words : (words * (k + 1) / kOutChunks) & ~uint64_t(31);
+                if (w1 <= w0) continue;
+                launch_emit_cartesian(nodeKind_, b, w0, w1, fin.as<uint32_t>(), fillP, surf.as<uint32_t>(),
+                                      ranks.as<uint32_t>(), keys.p, keysCap_, shape.emitBlocksPerSm, s, &launches);
+                if (!outEv_[k]) VXB_CUDA(cudaEventCreateWithFlags(&outEv_[k], cudaEventDisableTiming));
+                VXB_CUDA(cudaEventRecord(outEv_[k], s));
+                VXB_CUDA(cudaStreamWaitEvent(copyStream_, outEv_[k], 0));
+                VXB_CUDA(cudaMemcpyAsync(static_cast<uint8_t*>(hostOut_) + w0 * wordBytes,
+                                         static_cast<const uint8_t*>(u.out) + w0 * wordBytes, (w1 - w0) * wordBytes,
+                                         cudaMemcpyDeviceToHost, copyStream_));
+            }
+            hostCopied_ = true;
+        } else {
+            launch_emit_cartesian(nodeKind_, b, 0, totalWords_, fin.as<uint32_t>(), fillP, surf.as<uint32_t>(),
+                                  ranks.as<uint32_t>(), keys.p, keysCap_, shape.emitBlocksPerSm, s, &launches);
+        }
         tuneMark(kKnobEmit, true, s);
     }
     if (nFcc_)
@@ -474,6 +497,8 @@ int Pipeline::pruneGroupUntilStable(const Group& gr, cudaStream_t s) {
 
 Pipeline::~Pipeline() {
     for (cudaEvent_t& e : tuneEv_)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : outEv_)
         if (e) cudaEventDestroy(e);
 }
 
@@ -576,7 +601,7 @@ int Pipeline::finish(cudaStream_t s) {
             launch_emit_raw(nodeKind_, b, totalWords_, fillP, surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p,
                             keysCap_, s, &launches);
         else if (anyCartesian_)
-            launch_emit_cartesian(nodeKind_, b, totalWords_, fin.as<uint32_t>(), fillP, surf.as<uint32_t>(),
+            launch_emit_cartesian(nodeKind_, b, 0, totalWords_, fin.as<uint32_t>(), fillP, surf.as<uint32_t>(),
                                   ranks.as<uint32_t>(), keys.p, keysCap_, shape.emitBlocksPerSm, s, &launches);
         if (nFcc_)
             launch_emit_fcc(nodeKind_, b, reinterpret_cast<const FccMesh*>(tables.as<uint8_t>() + oFcc_),
@@ -585,6 +610,11 @@ int Pipeline::finish(cudaStream_t s) {
                             &launches);
         VXB_CUDA(cudaGetLastError());
         VXB_CUDA(cudaStreamSynchronize(s));
+        if (hostCopied_) {
+            // The chunks already copied predate the re-emission.
+            VXB_CUDA(cudaStreamSynchronize(copyStream_));
+            VXB_CUDA(cudaMemcpy(hostOut_, units_[0].out, hostBytes_, cudaMemcpyDeviceToHost));
+        }
     }
     return 0;
 }

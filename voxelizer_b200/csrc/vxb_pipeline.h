@@ -75,11 +75,23 @@ public:
     int finish(cudaStream_t s);
     // Kernels launched by the last enqueue + finish.
     uint32_t launches = 0;
+    // Node output of a one-mesh Cartesian run copied to pinned host memory
+    // while it is emitted (in kOutChunks ranges, on `copyStream`): set
+    // before enqueue; hostCopied() tells whether the run did it (the caller
+    // then waits for copyStream instead of copying).
+    void streamOutput(void* host, uint64_t bytes, cudaStream_t copyStream) {
+        hostOut_ = host;
+        hostBytes_ = bytes;
+        copyStream_ = copyStream;
+        hostCopied_ = false;
+    }
+    bool hostCopied() const { return hostCopied_; }
     // Counters of the last finish (vxb_last_stats).
     vxb_stats stats{};
 
     static constexpr uint32_t kPasses = 8;   // pruning passes queued per subspace
     static constexpr uint32_t kLoopListMax = 32768;   // longest list the one-block passes take
+    static constexpr uint32_t kOutChunks = 4;         // emit / host-copy ranges of streamed output
 
     // Launch shape of the last enqueue (the autotuner's choice).
     LaunchShape shape{};
@@ -91,6 +103,11 @@ private:
     std::string bucket_;
     int trial_ = -1;
     cudaEvent_t tuneEv_[2 * kKnobs] = {};
+    void* hostOut_ = nullptr;
+    uint64_t hostBytes_ = 0;
+    cudaStream_t copyStream_ = nullptr;
+    bool hostCopied_ = false;
+    cudaEvent_t outEv_[kOutChunks] = {};
     bool tuneUsed_[kKnobs] = {};
     void tuneMark(int knob, bool end, cudaStream_t s);
     void tuneFinish();
