@@ -23,7 +23,8 @@ SITES = ["P_BIN", "E_BIN", "D_BIN", "TN", "P_GEN", "CR_GEN", "D_GEN", "E_GEN", "
          "DE_2D_YZ", "DE_2D_ZX", "DE_2D_XY", "DE_3D_YZ", "DE_3D_ZX", "DE_3D_XY",
          "OT_2D_YZ", "OT_2D_ZX", "OT_2D_XY", "OT_3D_YZ", "OT_3D_ZX", "OT_3D_XY",
          "OT_3DX_ZX", "OT_3DX_XY", "OT_3DY_XY", "OT_3DY_YZ", "OT_3DZ_YZ", "OT_3DZ_ZX",
-         "DT_3DX", "DT_3DY", "DT_3DZ"]
+         "DT_3DX", "DT_3DY", "DT_3DZ", "OT_2DP_YZ", "OT_2DP_ZX", "OT_2DP_XY", "UNR_2D",
+         "OT_3DXP_ZX", "OT_3DXP_XY", "OT_3DYP_XY", "OT_3DYP_YZ", "OT_3DZP_YZ", "OT_3DZP_ZX", "UNR_3DL"]
 SITE = {n: i for i, n in enumerate(SITES)}
 
 # Contraction modes of the reference build, pinned against the reference's
@@ -34,24 +35,32 @@ SITES_INC = os.path.join(os.path.dirname(HERE), "voxelizer_b200", "csrc", "vxb_s
 
 
 def _read_sites(path=SITES_INC):
+    """{site: mode} for scalar sites, {site: [mode per node type]} for the
+    sites whose mode depends on the node type."""
     out = {}
     with open(path) as fh:
         for line in fh:
             line = line.strip()
-            if line.startswith("constexpr int "):
-                name, val = line[len("constexpr int "):].rstrip(";").split("=")
-                out[name.strip()] = int(val)
+            if not line.startswith("constexpr int "):
+                continue
+            name, val = line[len("constexpr int "):].rstrip(";").split("=")
+            name, val = name.strip(), val.strip()
+            if name.endswith("]"):
+                out[name[:name.index("[")]] = [int(x) for x in val.strip("{}").split(",")]
+            else:
+                out[name] = int(val)
     return out
 
 
 PINNED_FMA = _read_sites()
 
 
-def fma_sites(model=None):
-    """48-entry site array from a {site name: mode} dict (None: pinned)."""
-    arr = [0] * 48
+def fma_sites(model=None, node_type=1):
+    """64-entry site array for one node type from a {site name: mode or
+    [mode per node type]} dict (None: pinned)."""
+    arr = [0] * 64
     for k, v in (PINNED_FMA if model is None else model).items():
-        arr[SITE[k]] = int(v)
+        arr[SITE[k]] = int(v[node_type] if isinstance(v, (list, tuple)) else v)
     return arr
 
 NODE_BYTES = {0: 1, 1: 2, 2: 8, 3: 2, 4: 4}
@@ -62,7 +71,7 @@ class _Params(ctypes.Structure):
     _fields_ = [("node_type", ctypes.c_int), ("node_output", ctypes.c_int), ("materials", ctypes.c_int),
                 ("by_cube_length", ctypes.c_int), ("max_dim", ctypes.c_uint32), ("cube_length", ctypes.c_double),
                 ("vox_split", ctypes.c_uint32 * 3), ("mat_split", ctypes.c_uint32 * 3),
-                ("fma_sites", ctypes.c_uint8 * 48), ("threads", ctypes.c_int), ("space", ctypes.c_int),
+                ("fma_sites", ctypes.c_uint8 * 64), ("threads", ctypes.c_int), ("space", ctypes.c_int),
                 ("part", ctypes.c_uint32 * 4), ("rotate_x", ctypes.c_int)]
 
 
@@ -103,7 +112,7 @@ def _params(node_type, nodes, materials, size, vox, mat, fma_model, threads, par
     p.cube_length = float(size) if isinstance(size, float) else 0.0
     p.vox_split[:] = list(vox)
     p.mat_split[:] = list(mat)
-    p.fma_sites[:] = fma_sites(fma_model)
+    p.fma_sites[:] = fma_sites(fma_model, int(node_type))
     p.threads = int(threads)
     if part is not None:   # device space: yz partition (y0, y1, z0, z1) of the grid
         p.space = 1
@@ -169,3 +178,24 @@ def voxelize_winners(mesh, size, vox=(1024, 512, 512), mat=(512, 512, 512), fma_
     if rc:
         raise RuntimeError(f"orc_voxelize_winners failed: {rc}")
     return out, info, conf, tri, cls
+
+
+def surface_hits(mesh, node_type, size, grid=0, vox=(1024, 512, 512), mat=(512, 512, 512), fma_model=None):
+    """Every surface hit of one lattice as an (n, 2) array of (triangle, node
+    index) rows, evaluated with `fma_model` (None: the pinned modes)."""
+    p = _params(node_type, 1, 1, size, vox, mat, fma_model, 0)
+    L = lib()
+    L.orc_surface_hits.restype = ctypes.c_longlong
+    L.orc_surface_hits.argtypes = [ctypes.POINTER(_Params), ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                   ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64]
+    cap = 1 << 16
+    while True:
+        buf = np.empty(cap, np.uint64)
+        n = L.orc_surface_hits(ctypes.byref(p), mesh.vertices.ctypes.data, mesh.n_vertices, mesh.indices.ctypes.data,
+                               mesh.n_triangles, int(grid), buf.ctypes.data, cap)
+        if n < 0:
+            raise RuntimeError(f"orc_surface_hits failed: {n}")
+        if n <= cap:
+            buf = buf[:n]
+            return np.stack([(buf >> np.uint64(32)).astype(np.int64), (buf & np.uint64(0xFFFFFFFF)).astype(np.int64)], 1)
+        cap = int(n)

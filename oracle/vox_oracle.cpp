@@ -537,7 +537,7 @@ static void performVoxelization(const float* V, const uint* I, uint nT, d3 mn, d
                     }
                     uint pass = 0;
                     for (int i = 0; i < 3; i++) {
-                        double r = sum2p1(en[i].x, px, en[i].y, py, dist[i], F[ORC_S_E_GEN]);
+                        double r = sum2p1(en[i].x, px, en[i].y, py, dist[i], (F[ORC_S_E_GEN] >> (2 * i)) & 3);
                         if (en[i].x > 0.0 || (en[i].x == 0.0 && en[i].y < 0.0)) r += DBL_MIN;
                         if (r > 0.0) pass++;
                     }
@@ -737,6 +737,14 @@ static inline i2 depthRange(const f3* t, f3 p, f3 n, f3 m, float d, int axis, in
     return i2{vcMin(a, mm, d), vcMax(b, mm, d)};
 }
 
+// Form of the edge functions at iteration `pos` of a loop of `n` iterations
+// that the reference build unrolled `unr` times with a prolog: the prolog
+// runs the first n mod unr iterations.
+static inline int loopForm(int pos, int n, int unr, int mainMode, int proMode) {
+    if (unr <= 1) return mainMode;
+    return pos < n % unr ? proMode : mainMode;
+}
+
 // process1D/2D/3DTriangles for one triangle inside one material subspace,
 // src/voxelizer.cu:3306-3955.  Calls hit(nodeIndex) for every processVoxel.
 template <class Hit>
@@ -763,23 +771,32 @@ static void surfaceTriangle(const SurfaceCtx& c, uint tri, uint code, Bounds<u3>
     if (bb == 2) {
         f3 n = crossF(sub3(t[0], t[2]), sub3(t[1], t[0]), F[ORC_S_CRF_2D]);
         const int pc = F[ORC_S_PC_2D];
+        // The inner loop (z for the x and y axes, y for the z axis) runs its
+        // first (trip count mod UNR_2D) iterations in the prolog forms.
+        const int unr = F[ORC_S_UNR_2D];
+        auto form = [&](int inner, int lo, int hi, int mainMode, int proMode) {
+            return loopForm(inner - lo, hi - lo + 1, unr, mainMode, proMode);
+        };
         if (axis == 0) {
             Overlap o = setupOverlap(t, n, c.d, 0, F[ORC_S_DE_2D_YZ]);
             for (int j = vb.min.y; j <= vb.max.y; j++)
                 for (int k = vb.min.z; k <= vb.max.z; k++)
-                    if (overlapTest(o, vbComp(j, c.m.y, c.d, pc), vbComp(k, c.m.z, c.d, pc), F[ORC_S_OT_2D_YZ]))
+                    if (overlapTest(o, vbComp(j, c.m.y, c.d, pc), vbComp(k, c.m.z, c.d, pc),
+                                    form(k, vb.min.z, vb.max.z, F[ORC_S_OT_2D_YZ], F[ORC_S_OT_2DP_YZ])))
                         hit(nodeIndex(c, vb.min.x + ax, j + ay, k + az));
         } else if (axis == 1) {
             Overlap o = setupOverlap(t, n, c.d, 1, F[ORC_S_DE_2D_ZX]);
             for (int i = vb.min.x; i <= vb.max.x; i++)
                 for (int k = vb.min.z; k <= vb.max.z; k++)
-                    if (overlapTest(o, vbComp(k, c.m.z, c.d, pc), vbComp(i, c.m.x, c.d, pc), F[ORC_S_OT_2D_ZX]))
+                    if (overlapTest(o, vbComp(k, c.m.z, c.d, pc), vbComp(i, c.m.x, c.d, pc),
+                                    form(k, vb.min.z, vb.max.z, F[ORC_S_OT_2D_ZX], F[ORC_S_OT_2DP_ZX])))
                         hit(nodeIndex(c, i + ax, vb.min.y + ay, k + az));
         } else {
             Overlap o = setupOverlap(t, n, c.d, 2, F[ORC_S_DE_2D_XY]);
             for (int i = vb.min.x; i <= vb.max.x; i++)
                 for (int j = vb.min.y; j <= vb.max.y; j++)
-                    if (overlapTest(o, vbComp(i, c.m.x, c.d, pc), vbComp(j, c.m.y, c.d, pc), F[ORC_S_OT_2D_XY]))
+                    if (overlapTest(o, vbComp(i, c.m.x, c.d, pc), vbComp(j, c.m.y, c.d, pc),
+                                    form(j, vb.min.y, vb.max.y, F[ORC_S_OT_2D_XY], F[ORC_S_OT_2DP_XY])))
                         hit(nodeIndex(c, i + ax, j + ay, vb.min.z + az));
         }
         return;
@@ -789,6 +806,7 @@ static void surfaceTriangle(const SurfaceCtx& c, uint tri, uint code, Bounds<u3>
     Overlap o1 = setupOverlap(t, n, c.d, 1, F[ORC_S_DE_3D_ZX]);
     Overlap o2 = setupOverlap(t, n, c.d, 2, F[ORC_S_DE_3D_XY]);
     const int pc = F[ORC_S_PC_3D], pl = F[ORC_S_PC_3DL];
+    const int ul = F[ORC_S_UNR_3DL];
     if (axis == 0) {
         for (int j = vb.min.y; j <= vb.max.y; j++)
             for (int k = vb.min.z; k <= vb.max.z; k++) {
@@ -801,7 +819,9 @@ static void surfaceTriangle(const SurfaceCtx& c, uint tri, uint code, Bounds<u3>
                 if (r.x == r.y) { hit(nodeIndex(c, r.x + ax, j + ay, k + az)); continue; }
                 for (int i = r.x; i <= r.y; i++) {
                     p.x = vbComp(i, c.m.x, c.d, pl);
-                    if (overlapTest(o1, p.z, p.x, F[ORC_S_OT_3DX_ZX]) && overlapTest(o2, p.x, p.y, F[ORC_S_OT_3DX_XY]))
+                    const int q = i - r.x, nl = r.y - r.x + 1;
+                    if (overlapTest(o1, p.z, p.x, loopForm(q, nl, ul, F[ORC_S_OT_3DX_ZX], F[ORC_S_OT_3DXP_ZX])) &&
+                        overlapTest(o2, p.x, p.y, loopForm(q, nl, ul, F[ORC_S_OT_3DX_XY], F[ORC_S_OT_3DXP_XY])))
                         hit(nodeIndex(c, i + ax, j + ay, k + az));
                 }
             }
@@ -817,7 +837,9 @@ static void surfaceTriangle(const SurfaceCtx& c, uint tri, uint code, Bounds<u3>
                 if (r.x == r.y) { hit(nodeIndex(c, i + ax, r.x + ay, k + az)); continue; }
                 for (int j = r.x; j <= r.y; j++) {
                     p.y = vbComp(j, c.m.y, c.d, pl);
-                    if (overlapTest(o2, p.x, p.y, F[ORC_S_OT_3DY_XY]) && overlapTest(o0, p.y, p.z, F[ORC_S_OT_3DY_YZ]))
+                    const int q = j - r.x, nl = r.y - r.x + 1;
+                    if (overlapTest(o2, p.x, p.y, loopForm(q, nl, ul, F[ORC_S_OT_3DY_XY], F[ORC_S_OT_3DYP_XY])) &&
+                        overlapTest(o0, p.y, p.z, loopForm(q, nl, ul, F[ORC_S_OT_3DY_YZ], F[ORC_S_OT_3DYP_YZ])))
                         hit(nodeIndex(c, i + ax, j + ay, k + az));
                 }
             }
@@ -833,7 +855,9 @@ static void surfaceTriangle(const SurfaceCtx& c, uint tri, uint code, Bounds<u3>
                 if (r.x == r.y) { hit(nodeIndex(c, i + ax, j + ay, r.x + az)); continue; }
                 for (int k = r.x; k <= r.y; k++) {
                     p.z = vbComp(k, c.m.z, c.d, pl);
-                    if (overlapTest(o0, p.y, p.z, F[ORC_S_OT_3DZ_YZ]) && overlapTest(o1, p.z, p.x, F[ORC_S_OT_3DZ_ZX]))
+                    const int q = k - r.x, nl = r.y - r.x + 1;
+                    if (overlapTest(o0, p.y, p.z, loopForm(q, nl, ul, F[ORC_S_OT_3DZ_YZ], F[ORC_S_OT_3DZP_YZ])) &&
+                        overlapTest(o1, p.z, p.x, loopForm(q, nl, ul, F[ORC_S_OT_3DZ_ZX], F[ORC_S_OT_3DZP_ZX])))
                         hit(nodeIndex(c, i + ax, j + ay, k + az));
                 }
             }
@@ -1430,4 +1454,40 @@ extern "C" float orc_node_ratio(const orc_params* p, const float* verts, const u
                        false, 1, &F, 1, 1};
     bool unstable = false;
     return ratio::nodeRatio(c, tri, cls, x, y, z, unstable);
+}
+
+// Every surface hit (triangle << 32 | node index) of one lattice of the
+// planned grid (grid 0: Cartesian; 1-4: FCC sub-lattice g), evaluated with
+// the site modes in p->fma_sites, in triangle order within each material
+// subspace.  Returns the number of hits (pairs beyond `cap` are counted, not
+// stored).  Used to fit and check the contraction model one triangle at a
+// time against the reference's output.
+extern "C" long long orc_surface_hits(const orc_params* p, const float* verts, uint32_t nV, const uint32_t* idx,
+                                      uint32_t nT, int grid, uint64_t* pairs, uint64_t cap) {
+    Plan pl = makePlan(p, verts, nV);
+    applySpace(p, pl);
+    if (pl.err) return pl.err;
+    if (grid < 0 || grid > 4) return -13;
+    const Fma F(p->fma_sites);
+    Bounds<u3> ext{u3{0, 0, 0}, pl.ext};
+    std::vector<Bounds<u3> > matSplits = split3(u3{p->mat_split[0], p->mat_split[1], p->mat_split[2]}, ext);
+    const double h = pl.d / 2.0;
+    d3 sh = grid <= 1 ? d3{0, 0, 0} : grid == 2 ? d3{h, h, 0} : grid == 3 ? d3{0, h, h} : d3{h, 0, h};
+    d3 m{pl.mnExt.x + sh.x, pl.mnExt.y + sh.y, pl.mnExt.z + sh.z};
+    const SurfaceCtx c{verts, idx, nullptr, f3{float(m.x), float(m.y), float(m.z)}, float(pl.d), pl.alloc,
+                       grid > 0, grid > 0 ? grid : 1, &F, (int)pl.padY, (int)pl.padZ};
+    std::vector<uint> codes(nT);
+    for (uint t = 0; t < nT; ++t) {
+        f3 v[3];
+        fetchF(verts, idx, t, v);
+        codes[t] = classify(v, c.m, c.d, F);
+    }
+    unsigned long long n = 0;
+    for (const Bounds<u3>& sub : matSplits)
+        for (uint t = 0; t < nT; ++t)
+            surfaceTriangle(c, t, codes[t], sub, [&](uint i) {
+                if (n < cap) pairs[n] = ((uint64_t)t << 32) | i;
+                ++n;
+            });
+    return (long long)n;
 }

@@ -45,6 +45,14 @@ enum {
     ORC_S_OT_2D_YZ, ORC_S_OT_2D_ZX, ORC_S_OT_2D_XY, ORC_S_OT_3D_YZ, ORC_S_OT_3D_ZX, ORC_S_OT_3D_XY,
     ORC_S_OT_3DX_ZX, ORC_S_OT_3DX_XY, ORC_S_OT_3DY_XY, ORC_S_OT_3DY_YZ, ORC_S_OT_3DZ_YZ, ORC_S_OT_3DZ_ZX,
     ORC_S_DT_3DX, ORC_S_DT_3DY, ORC_S_DT_3DZ,
+    /* process2DTriangles' inner loop is unrolled: the first (trip count mod
+     * UNR_2D) iterations evaluate the edge functions in the OT_2DP_* forms,
+     * the rest in the OT_2D_* forms (UNR_2D 0: one form throughout). */
+    ORC_S_OT_2DP_YZ, ORC_S_OT_2DP_ZX, ORC_S_OT_2DP_XY, ORC_S_UNR_2D,
+    /* The same for the depth loop of process3DTriangles (UNR_3DL, prolog
+     * forms OT_3DxP_*). */
+    ORC_S_OT_3DXP_ZX, ORC_S_OT_3DXP_XY, ORC_S_OT_3DYP_XY, ORC_S_OT_3DYP_YZ, ORC_S_OT_3DZP_YZ, ORC_S_OT_3DZP_ZX,
+    ORC_S_UNR_3DL,
     ORC_NSITES
 };
 
@@ -57,7 +65,7 @@ typedef struct {
     double cube_length;
     uint32_t vox_split[3];
     uint32_t mat_split[3];
-    uint8_t fma_sites[48];   /* one mode per ORC_S_* site */
+    uint8_t fma_sites[64];   /* one mode per ORC_S_* site, for this node type */
     int threads;          /* OpenMP threads (0 = library default) */
     /* Device space (src/host_side.cpp:782-1011): space = 1 voxelizes the
      * yz partition [part[0], part[1]) x [part[2], part[3]) of the grid as

@@ -175,7 +175,7 @@ CASES = [
     case("room_full_long", "room_full", LONG, 1, 1, 1024, store="digest"),
     case("room_full_bits", "room_full", LONG, 0, 0, 1024, store="digest"),
     case("elong4_4096_long", "elong4", LONG, 1, 0, 4096, store="digest"),
-    case("stress_full_sfcc", "stress_full_fcc", SHORT_FCC, 1, 1, FCC_A, store="digest", strict_mats=False),
+    case("stress_full_sfcc", "stress_full_fcc", SHORT_FCC, 1, 1, FCC_A, strict_mats=False),
     # PartialNode without and with materials (the surface ratio depends on
     # which racing triangle wrote last).
     case("ico4_partial_nomat", "ico4", PARTIAL, 1, 0, 1.0 / 64.0),

@@ -110,6 +110,40 @@ def oracle_case(c, m, want_conflicts=True):
 # the crossings.
 REF_ANOMALY_ROWS = {"room_lite_bits_part13_1": [(76, 24)]}
 
+# Node-grid counterpart: a box of node rows (y range, z range, inclusive) of
+# a golden node grid where the reference's solid bits differ from the
+# restated algorithm's, and the most boundary ids that differ inside it.
+# Materials and surface nodes are identical in both boxes.
+#  * stress_partial_mat (8,120 triangles, 96x80x80 PartialNodes): the
+#    reference's rows y 74-75 x z 59-60 (one 4x4 solid tile) hold solid runs
+#    at x 14-15, 18-19, 43-44, 46-47 and 54 that no triangle crossing those
+#    rows produces; pruning spreads them to 45 boundary ids.
+#  * stress_full_sfcc (20,120 triangles, 192x68x136 ShortFCCNodes): three
+#    node rows of sub-lattice 1 are solid from x 132 to the row's end in the
+#    reference only; 679 boundary ids differ around them.
+# Both sit where a generation edge function of a 45-degree edge is exactly
+# 0 at a voxel centre (triangles 8091 and 18257), but the same tie in
+# stress_sfcc_mat (triangle 7364) resolves the other way in the reference,
+# so no contraction mode of the FP64 solid path reproduces all three; the
+# reference's two runs agree on the boundary ids of every case.
+REF_ANOMALY_NODE_BOX = {"stress_partial_mat": ((73, 76), (58, 60), 45),
+                        "stress_full_sfcc": ((49, 52), (99, 104), 679)}
+
+
+def node_rows_mask(name, dims):
+    """Boolean mask over the nodes of a golden node grid: False inside the
+    case's anomaly box (REF_ANOMALY_NODE_BOX), and that box's bound on the
+    number of boundary ids that may differ inside it (0 without a box)."""
+    X, Y, Z = dims
+    keep = np.ones(X * Y * Z, dtype=bool)
+    box = REF_ANOMALY_NODE_BOX.get(name)
+    if box is None:
+        return keep, 0
+    (y0, y1), (z0, z1), limit = box
+    k = keep.reshape(Z, Y, X)
+    k[z0:z1 + 1, y0:y1 + 1, :] = False
+    return keep, limit
+
 
 def bit_rows_mask(name, dims):
     """Boolean mask over the words of a bit array: False on anomaly rows."""

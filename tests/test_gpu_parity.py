@@ -20,7 +20,7 @@ import pytest
 import cases as C
 import oracle as O
 from helpers import (CONFLICT_MAT, CONFLICT_RATIO, PARTIAL, RATIO_REF_TOL, RATIO_TOL, RATIO_UNSTABLE, bid_of,
-                     bit_rows_mask, describe_diff, mat_of, masked, oracle_case, ratio_bad, ratio_of)
+                     bit_rows_mask, describe_diff, mat_of, masked, node_rows_mask, oracle_case, ratio_bad, ratio_of)
 from voxelizer_b200.api import LONG, SHORT, Voxelizer
 from voxelizer_b200.scenes import Mesh
 
@@ -30,12 +30,6 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLD = os.path.join(ROOT, "tests", "golden")
 INDEX = json.load(open(os.path.join(GOLD, "index.json")))
 
-# Cases whose oracle output is not yet pinned to the reference at exact FP32
-# ties of the surface tests (vertices snapped to voxel corners).  The CUDA
-# path must still equal the oracle exactly on them.
-UNPINNED = {"stress_short_mat", "stress_long_splits", "stress_sfcc_mat", "stress_lfcc_mat", "stress_full_sfcc",
-            "stress_lfcc_part31_1",
-            "stress_partial_mat"}
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -92,14 +86,14 @@ def test_small_cases(name):
     else:
         assert np.array_equal(got, want), "CUDA vs oracle: " + describe_diff(got, want, info.dims)
     gold = np.load(os.path.join(GOLD, name + ".npz"))["out"]
-    if name in UNPINNED:
-        return
     if not c["nodes"]:
         keep = bit_rows_mask(name, info.dims)
         assert np.array_equal(got[keep], gold[keep]), "CUDA vs reference: " + describe_diff(got[keep], gold[keep])
         return
-    assert np.array_equal(bid_of(nt, got), bid_of(nt, gold)), "ids vs reference: " + describe_diff(
-        bid_of(nt, got), bid_of(nt, gold), info.dims)
+    rows, limit = node_rows_mask(name, info.dims)
+    bg, bw = bid_of(nt, got), bid_of(nt, gold)
+    assert np.array_equal(bg[rows], bw[rows]), "ids vs reference: " + describe_diff(bg[rows], bw[rows])
+    assert np.count_nonzero(bg != bw) <= limit, "ids vs reference in the anomaly box"
     keep = (conf & CONFLICT_MAT) == 0
     gm, wm = mat_of(nt, got), mat_of(nt, gold)
     assert np.array_equal(gm[keep], wm[keep]), "materials vs reference: " + describe_diff(gm[keep], wm[keep])
@@ -107,13 +101,13 @@ def test_small_cases(name):
         # Against the reference's own ratio wherever a single triangle of the
         # winning class wrote the node (non-surface nodes hold exactly 0 or 1)
         # and no edge parameter sits at a branch point.
-        sole = np.nonzero((conf & (CONFLICT_RATIO | RATIO_UNSTABLE)) == 0)[0]
+        sole = np.nonzero(((conf & (CONFLICT_RATIO | RATIO_UNSTABLE)) == 0) & rows)[0]
         bad = sole[ratio_bad(got[sole], gold[sole], RATIO_REF_TOL)]
         exact = int(np.count_nonzero((got >> np.uint64(32))[sole] == (gold >> np.uint64(32))[sole]))
         assert bad.size == 0, f"ratios vs reference: {bad.size} of {sole.size} beyond {RATIO_REF_TOL} " \
                               f"({exact} bit-identical): {ratio_of(got[bad[:5]])} vs {ratio_of(gold[bad[:5]])}"
     elif INDEX[name]["deterministic"]:
-        assert np.array_equal(got[keep], gold[keep])
+        assert np.array_equal(got[keep & rows], gold[keep & rows])
 
 
 @pytest.mark.parametrize("name", DIGEST)
@@ -124,10 +118,9 @@ def test_full_size_digests(name):
     assert info.dims == tuple(e["dims"])
     if c["nodes"]:
         bid = bid_of(c["node_type"], got).astype(np.uint32)
-        if name not in UNPINNED:
-            assert hashlib.sha256(bid.tobytes()).hexdigest() == e["bid_sha256"]
-        assert int(np.count_nonzero(bid)) == e["n_solid"] or name in UNPINNED
-        if e["deterministic"] and name not in UNPINNED:
+        assert hashlib.sha256(bid.tobytes()).hexdigest() == e["bid_sha256"]
+        assert int(np.count_nonzero(bid)) == e["n_solid"]
+        if e["deterministic"]:
             assert hashlib.sha256(got.tobytes()).hexdigest() == e["sha256"]
     else:
         assert hashlib.sha256(got.tobytes()).hexdigest() == e["sha256"]

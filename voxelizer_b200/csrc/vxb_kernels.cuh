@@ -96,7 +96,7 @@ void launch_surface_prepare(const Batch& b, uint32_t nWork, uint32_t* codes, uin
 // append (bit position << 24 | key) to `list` (entries past listCap are
 // counted, not stored); mode 1: merge every hit's key at its rank (needs
 // complete bits and `ranks`).  wide: 64-bit keys (PartialNode).
-void launch_surface_work(int mode, int wide, const Batch& b, const void* recs, const void* ovl,
+void launch_surface_work(int kind, int mode, int wide, const Batch& b, const void* recs, const void* ovl,
                          const uint32_t* offsets, uint32_t nWork, const uint32_t* total, const uint32_t* buckets,
                          uint32_t* surf, const uint32_t* ranks, void* keys, uint32_t keysCap,
                          unsigned long long* list, uint32_t* listCount, uint32_t listCap, uint32_t blocksPerSm,

@@ -368,8 +368,8 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
                     st + kSurfOverflow, s, &launches);
         mark(5, false);
         tuneMark(kKnobSurface, false, s);
-        launch_surface_work(0, wide_ ? 1 : 0, b, recs.p, ovl.p, offsets.as<uint32_t>(), nWork_, st + kSurfTotal,
-                            buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_,
+        launch_surface_work(nodeKind_, 0, wide_ ? 1 : 0, b, recs.p, ovl.p, offsets.as<uint32_t>(), nWork_,
+                            st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_,
                             hitList.as<unsigned long long>(), st + kHitCount, listCap_, shape.surfBlocksPerSm,
                             shape.surfBatch, s, &launches);
         tuneMark(kKnobSurface, true, s);
@@ -420,9 +420,9 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
                                   ranks.as<uint32_t>(), keys.as<uint32_t>(), keysCap_, shape.mergeBlocksPerSm, s,
                                   &launches);
         else
-            launch_surface_work(1, 1, b, recs.p, ovl.p, offsets.as<uint32_t>(), nWork_, st + kSurfTotal,
-                                buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_,
-                                nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch, s, &launches);
+            launch_surface_work(nodeKind_, 1, 1, b, recs.p, ovl.p, offsets.as<uint32_t>(), nWork_,
+                                st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(),
+                                keys.p, keysCap_, nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch, s, &launches);
         tuneMark(kKnobMerge, true, s);
         mark(4, true);
     }
@@ -571,9 +571,9 @@ int Pipeline::finish(cudaStream_t s) {
                 keysCap_ = surfaceVoxels + 1;
             }
             launch_surface_keys_zero(keys.p, st + kSurfaceVoxels, keysCap_, wide_ ? 1 : 0, s, &launches);
-            launch_surface_work(1, wide_ ? 1 : 0, b, recs.p, ovl.p, offsets.as<uint32_t>(), nWork_, st + kSurfTotal,
-                                buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_,
-                                nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch, s, &launches);
+            launch_surface_work(nodeKind_, 1, wide_ ? 1 : 0, b, recs.p, ovl.p, offsets.as<uint32_t>(), nWork_,
+                                st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(),
+                                keys.p, keysCap_, nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch, s, &launches);
             reemit = true;
         }
     }

@@ -420,9 +420,34 @@ struct Sink {
     }
 };
 
+// The loop of the reference over [lo, hi] along one axis runs inside one
+// material subspace (adjustVoxelRange, src/voxelizer.cu:3963-3993): clamps
+// [lo, hi] to the subspace slice (sl: nSl (lo, hi) pairs) that holds c.
+__device__ __forceinline__ void subspaceRange(const uint32_t* sl, uint32_t nSl, int c, int& lo, int& hi) {
+    for (uint32_t s = 0; s < nSl; ++s) {
+        const int a = (int)__ldg(sl + 2 * s), b = (int)__ldg(sl + 2 * s + 1) - 1;
+        if (c >= a && c <= b) {
+            lo = max(lo, a);
+            hi = min(hi, b);
+            return;
+        }
+    }
+}
+
+// Whether iteration `pos` of a loop of n iterations falls in the prolog of a
+// loop the reference build unrolled U times (the prolog runs the first
+// n mod U iterations; vxb_sites.inc).
+template <int U> __device__ __forceinline__ bool inProlog(int pos, int n) { return U > 1 && pos < n % U; }
+
+template <int M, int P> __device__ __forceinline__ bool overlapAt(bool prolog, const Overlap& o, float a, float b) {
+    return prolog ? overlapTest<P>(o, a, b) : overlapTest<M>(o, a, b);
+}
+
 // One column (one voxel for 1D boxes) of a partitioned triangle
-// (process1D/2D/3DTriangles).  xr / yr / zr: the material subspace slices
-// along each axis ((lo, hi) pairs).
+// (process1D/2D/3DTriangles, instantiated per node type K as the reference
+// instantiates them).  xr / yr / zr: the material subspace slices along each
+// axis ((lo, hi) pairs).
+template <int K>
 __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const SurfRec& r, const Overlap& od,
                                             const SurfOvl* __restrict__ ov, uint32_t u, const PassGeom& g,
                                             const uint32_t* __restrict__ slices, const uint32_t* sliceOff,
@@ -438,28 +463,42 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
         return;
     }
     if (bb == 2) {
-        // process2DTriangles (3418-3596): the dominant projection only.
+        // process2DTriangles (3418-3596): the dominant projection only; the
+        // inner loop (z for the x and y axes, y for the z axis) evaluates its
+        // prolog iterations in their own forms.
+        constexpr int U = site::UNR_2D[K];
         if (axis == 0) {
             const int j = r.lo[1] + (int)(u % ey), k = r.lo[2] + (int)(u / ey);
-            if (overlapTest<site::OT_2D_YZ>(od, vbComp<site::PC_2D>(j, g.mnf[1], d),
-                                            vbComp<site::PC_2D>(k, g.mnf[2], d)))
+            int lo = r.lo[2], hi = r.hi[2];
+            if (U > 1) subspaceRange(slices + 2 * sliceOff[2], sliceN[2], k, lo, hi);
+            if (overlapAt<site::OT_2D_YZ, site::OT_2DP_YZ>(inProlog<U>(k - lo, hi - lo + 1), od,
+                                                           vbComp<site::PC_2D>(j, g.mnf[1], d),
+                                                           vbComp<site::PC_2D>(k, g.mnf[2], d)))
                 sink(r.lo[0], j, k, key, ug, ws);
         } else if (axis == 1) {
             const int i = r.lo[0] + (int)(u % ex), k = r.lo[2] + (int)(u / ex);
-            if (overlapTest<site::OT_2D_ZX>(od, vbComp<site::PC_2D>(k, g.mnf[2], d),
-                                            vbComp<site::PC_2D>(i, g.mnf[0], d)))
+            int lo = r.lo[2], hi = r.hi[2];
+            if (U > 1) subspaceRange(slices + 2 * sliceOff[2], sliceN[2], k, lo, hi);
+            if (overlapAt<site::OT_2D_ZX, site::OT_2DP_ZX>(inProlog<U>(k - lo, hi - lo + 1), od,
+                                                           vbComp<site::PC_2D>(k, g.mnf[2], d),
+                                                           vbComp<site::PC_2D>(i, g.mnf[0], d)))
                 sink(i, r.lo[1], k, key, ug, ws);
         } else {
             const int i = r.lo[0] + (int)(u % ex), j = r.lo[1] + (int)(u / ex);
-            if (overlapTest<site::OT_2D_XY>(od, vbComp<site::PC_2D>(i, g.mnf[0], d),
-                                            vbComp<site::PC_2D>(j, g.mnf[1], d)))
+            int lo = r.lo[1], hi = r.hi[1];
+            if (U > 1) subspaceRange(slices + 2 * sliceOff[1], sliceN[1], j, lo, hi);
+            if (overlapAt<site::OT_2D_XY, site::OT_2DP_XY>(inProlog<U>(j - lo, hi - lo + 1), od,
+                                                           vbComp<site::PC_2D>(i, g.mnf[0], d),
+                                                           vbComp<site::PC_2D>(j, g.mnf[1], d)))
                 sink(i, j, r.lo[2], key, ug, ws);
         }
         return;
     }
     // process3DTriangles (3603-3955): dominant projection, depth range from
     // the plane, then per subspace slice of the depth axis either the single
-    // voxel or the other two projections per voxel.
+    // voxel or the other two projections per voxel (the depth loop's prolog
+    // iterations in their own forms).
+    constexpr int UL = site::UNR_3DL[K];
     const F3 n{r.n[0], r.n[1], r.n[2]};
     const F3 t0{r.v0[0], r.v0[1], r.v0[2]};
     if (axis == 0) {
@@ -467,7 +506,7 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
         F3 p{0.0f, vbComp<site::PC_3D>(j, g.mnf[1], d), vbComp<site::PC_3D>(k, g.mnf[2], d)};
         if (!overlapTest<site::OT_3D_YZ>(od, p.y, p.z)) return;
         int d0, d1;
-        depthRange<0, site::DT_3DX>(t0, p, n, g, d0, d1);
+        depthRange<0, site::DT_3DX[K]>(t0, p, n, g, d0, d1);
         const uint32_t* sl = slices + 2 * sliceOff[0];
         for (uint32_t s = 0; s < sliceN[0]; ++s) {
             const int lo = max(r.lo[0], (int)__ldg(sl + 2 * s)), hi = min(r.hi[0], (int)__ldg(sl + 2 * s + 1) - 1);
@@ -476,7 +515,9 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
             if (a == c) { sink(a, j, k, key, ug, ws); continue; }
             for (int i = a; i <= c; ++i) {
                 p.x = vbComp<site::PC_3DL>(i, g.mnf[0], d);
-                if (overlapTest<site::OT_3DX_ZX>(ov->o[1], p.z, p.x) && overlapTest<site::OT_3DX_XY>(ov->o[2], p.x, p.y))
+                const bool pro = inProlog<UL>(i - a, c - a + 1);
+                if (overlapAt<site::OT_3DX_ZX, site::OT_3DXP_ZX[K]>(pro, ov->o[1], p.z, p.x) &&
+                    overlapAt<site::OT_3DX_XY, site::OT_3DXP_XY>(pro, ov->o[2], p.x, p.y))
                     sink(i, j, k, key, ug, ws);
             }
         }
@@ -494,7 +535,9 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
             if (a == c) { sink(i, a, k, key, ug, ws); continue; }
             for (int j = a; j <= c; ++j) {
                 p.y = vbComp<site::PC_3DL>(j, g.mnf[1], d);
-                if (overlapTest<site::OT_3DY_XY>(ov->o[2], p.x, p.y) && overlapTest<site::OT_3DY_YZ>(ov->o[0], p.y, p.z))
+                const bool pro = inProlog<UL>(j - a, c - a + 1);
+                if (overlapAt<site::OT_3DY_XY, site::OT_3DYP_XY>(pro, ov->o[2], p.x, p.y) &&
+                    overlapAt<site::OT_3DY_YZ, site::OT_3DYP_YZ>(pro, ov->o[0], p.y, p.z))
                     sink(i, j, k, key, ug, ws);
             }
         }
@@ -512,7 +555,9 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
             if (a == c) { sink(i, j, a, key, ug, ws); continue; }
             for (int k = a; k <= c; ++k) {
                 p.z = vbComp<site::PC_3DL>(k, g.mnf[2], d);
-                if (overlapTest<site::OT_3DZ_YZ>(ov->o[0], p.y, p.z) && overlapTest<site::OT_3DZ_ZX>(ov->o[1], p.z, p.x))
+                const bool pro = inProlog<UL>(k - a, c - a + 1);
+                if (overlapAt<site::OT_3DZ_YZ, site::OT_3DZP_YZ>(pro, ov->o[0], p.y, p.z) &&
+                    overlapAt<site::OT_3DZ_ZX, site::OT_3DZP_ZX>(pro, ov->o[1], p.z, p.x))
                     sink(i, j, k, key, ug, ws);
             }
         }
@@ -528,7 +573,7 @@ __device__ __forceinline__ void surfaceItem(uint32_t bb, uint32_t axis, const Su
 // gives every lane its owner.  The class and axis of a position follow from
 // the bucket bounds, so the projection edge functions load together with
 // the record.
-template <uint32_t kBatch>
+template <uint32_t kBatch, int K>
 __global__ void __launch_bounds__(kBlock) surfaceWorkKernel(Sink sink, Batch b, const SurfRec* __restrict__ recs,
                                                             const SurfOvl* __restrict__ ovl,
                                                             const uint32_t* __restrict__ off, uint32_t n,
@@ -585,8 +630,8 @@ __global__ void __launch_bounds__(kBlock) surfaceWorkKernel(Sink sink, Batch b, 
                 const uint32_t sliceOff[3] = {U.sliceBase, U.sliceBase + U.sliceN[0],
                                               U.sliceBase + U.sliceN[0] + U.sliceN[1]};
                 const uint32_t sliceN[3] = {U.sliceN[0], U.sliceN[1], U.sliceN[2]};
-                surfaceItem(bb, axis, r, od, ovl + pos, item - ok, g, b.slices, sliceOff, sliceN, key, sink, ug,
-                            ws);
+                surfaceItem<K>(bb, axis, r, od, ovl + pos, item - ok, g, b.slices, sliceOff, sliceN, key, sink,
+                               ug, ws);
             }
             __syncwarp();
             if (sink.mode == 0 && *ws.count >= kFlushAt) sink.flush(ws, lane);
@@ -735,7 +780,17 @@ void launch_surface_prepare(const Batch& b, uint32_t nWork, uint32_t* codes, uin
     *launches += 3;
 }
 
-void launch_surface_work(int mode, int wide, const Batch& b, const void* recs, const void* ovl,
+template <int K>
+static void launchSurfaceWorkKind(uint32_t batch, uint32_t grid, const Sink& sink, const Batch& b, const SurfRec* R,
+                                  const SurfOvl* O, const uint32_t* offsets, uint32_t nWork, const uint32_t* total,
+                                  const uint32_t* buckets, cudaStream_t s) {
+    if (batch == 8) surfaceWorkKernel<8, K><<<grid, kBlock, 0, s>>>(sink, b, R, O, offsets, nWork, total, buckets);
+    else if (batch == 32)
+        surfaceWorkKernel<32, K><<<grid, kBlock, 0, s>>>(sink, b, R, O, offsets, nWork, total, buckets);
+    else surfaceWorkKernel<16, K><<<grid, kBlock, 0, s>>>(sink, b, R, O, offsets, nWork, total, buckets);
+}
+
+void launch_surface_work(int kind, int mode, int wide, const Batch& b, const void* recs, const void* ovl,
                          const uint32_t* offsets, uint32_t nWork, const uint32_t* total, const uint32_t* buckets,
                          uint32_t* surf, const uint32_t* ranks, void* keys, uint32_t keysCap,
                          unsigned long long* list, uint32_t* listCount, uint32_t listCap, uint32_t blocksPerSm,
@@ -753,9 +808,19 @@ void launch_surface_work(int mode, int wide, const Batch& b, const void* recs, c
     const uint32_t grid = 148u * blocksPerSm;
     const SurfRec* R = static_cast<const SurfRec*>(recs);
     const SurfOvl* O = static_cast<const SurfOvl*>(ovl);
-    if (batch == 8) surfaceWorkKernel<8><<<grid, kBlock, 0, s>>>(sink, b, R, O, offsets, nWork, total, buckets);
-    else if (batch == 32) surfaceWorkKernel<32><<<grid, kBlock, 0, s>>>(sink, b, R, O, offsets, nWork, total, buckets);
-    else surfaceWorkKernel<16><<<grid, kBlock, 0, s>>>(sink, b, R, O, offsets, nWork, total, buckets);
+    switch (kind) {
+    case kShort: launchSurfaceWorkKind<kShort>(batch, grid, sink, b, R, O, offsets, nWork, total, buckets, s); break;
+    case kLong: launchSurfaceWorkKind<kLong>(batch, grid, sink, b, R, O, offsets, nWork, total, buckets, s); break;
+    case kPartial:
+        launchSurfaceWorkKind<kPartial>(batch, grid, sink, b, R, O, offsets, nWork, total, buckets, s);
+        break;
+    case kShortFcc:
+        launchSurfaceWorkKind<kShortFcc>(batch, grid, sink, b, R, O, offsets, nWork, total, buckets, s);
+        break;
+    default:
+        launchSurfaceWorkKind<kLongFcc>(batch, grid, sink, b, R, O, offsets, nWork, total, buckets, s);
+        break;
+    }
     *launches += 1;
 }
 
