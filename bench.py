@@ -42,6 +42,11 @@ sys.path.insert(0, ROOT)
 METRIC = "node-grid voxelization throughput (Gvoxels/s), bit-exact vs reference"
 UNIT = "Gvoxels/s"
 WORKLOAD = "room scene, 1,049,868 triangles, 17 materials, LongNode, maxDimension 1024 -> 1088x771x515 nodes"
+# The same config dict in both arms: the workload and how the L2 is kept out
+# of the timing (every step writes an 864 MB node grid).
+L2_NOTE = ("each step writes an 864 MB node grid (L2 126 MB); the device-resident timing also writes 256 MB "
+           "to flush the L2 before every timed step")
+CONFIG = {"workload": WORKLOAD, "l2": L2_NOTE}
 MAX_DIM = 1024
 CPU_SAMPLE_DIM = 384
 
@@ -71,50 +76,87 @@ def ncu_traffic(key):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling while the timed region runs."""
+    """SM clock and throttle-reason samples while the timed region runs:
+    NVML polled every 5 ms from a thread (reads only), else nvidia-smi at its
+    shortest period."""
 
-    def __init__(self, index):
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
+
+    def __init__(self, index, period_s=0.005):
         self.index = index
-        self.samples = []
+        self.period = period_s
+        self.samples = []   # (sm_mhz, max_mhz, reasons set)
         self._stop = threading.Event()
         self._proc = None
+        self._thread = None
+        self._nvml = None
 
     def __enter__(self):
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            self._nvml = pynvml
+
+            def poll():
+                while not self._stop.is_set():
+                    sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    bits = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((float(sm), float(mx),
+                                         {n for n, b in self.REASONS.items() if bits & b}))
+                    self._stop.wait(self.period)
+
+            self._thread = threading.Thread(target=poll, daemon=True)
+            self._thread.start()
+            return self
+        except Exception:
+            self._nvml = None
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
         try:
             self._proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                           "-i", str(self.index), "-lms", "100"], stdout=subprocess.PIPE,
+                                           "-i", str(self.index), "-lms", "20"], stdout=subprocess.PIPE,
                                           stderr=subprocess.DEVNULL, text=True)
-            threading.Thread(target=self._read, daemon=True).start()
+            self._thread = threading.Thread(target=self._read, daemon=True)
+            self._thread.start()
         except OSError:
             self._proc = None
         return self
 
     def _read(self):
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self._proc.stdout:
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 8:
-                self.samples.append(parts)
+            if len(parts) >= 8 and parts[1].replace(".", "").isdigit():
+                self.samples.append((float(parts[1]), float(parts[2]),
+                                     {names[i] for i in range(4) if parts[4 + i] == "Active"}))
 
     def __exit__(self, *a):
+        self._stop.set()
         if self._proc:
             self._proc.terminate()
             try:
                 self._proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self._proc.kill()
+        if self._thread:
+            self._thread.join(timeout=5)
+        if self._nvml:
+            try:
+                self._nvml.nvmlShutdown()
+            except Exception:
+                pass
 
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = sorted(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
-        mx = max(float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit())
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[4 + i] == "Active"})
-        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
-                "samples": len(self.samples)}
+        sm = sorted(s[0] for s in self.samples)
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(s[1] for s in self.samples),
+                "reasons": sorted(set().union(*(s[2] for s in self.samples))), "samples": len(self.samples),
+                "source": "nvml" if self._nvml else "nvidia-smi"}
 
 
 def dist_setup():
@@ -213,7 +255,7 @@ def run_reference_cuda(args, world, ref):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t / len(times), 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32+u32",
             "data": "synthetic (seeded room scene)", "device": "cuda:0",
-            "config": {"workload": WORKLOAD, "sample": sample},
+            "config": dict(CONFIG), "sample": sample,
             "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": 1, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -253,7 +295,7 @@ def run_reference(args, world, rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t / len(times), 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32+u32",
             "data": "synthetic (seeded room scene)",
-            "config": {"workload": WORKLOAD, "sample": sample},
+            "config": dict(CONFIG), "sample": sample,
             "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -316,6 +358,13 @@ BATCH_METRIC = "batched meshes/s (256-mesh mix, LongNode with materials), bit-ex
 def run_batched(args, world, rank, local):
     """The 256-mesh mix: one batch (graph replay) against a loop of plain
     per-mesh calls, same outputs.  Each rank runs its own copy (replicas)."""
+    line = batched_line(args, world, local, args.steps, args.warmup)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def batched_line(args, world, local, steps, warmup):
+    """The batched workload's result line (see run_batched)."""
     import torch
 
     from voxelizer_b200 import scenes
@@ -360,20 +409,20 @@ def run_batched(args, world, rank, local):
         stream.synchronize()
 
     tuned = autotune(args, tune_calls)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         loop()
         batch.run(stream=sh, graph=True)
     launches = batch.last_launch_count()
-    t_loop = timed(loop, max(1, args.steps // 2))
+    t_loop = timed(loop, max(1, steps // 2))
     with ClockSampler(local) as clk:
-        t_batch = timed(lambda: batch.run(stream=sh, graph=True), args.steps)
+        t_batch = timed(lambda: batch.run(stream=sh, graph=True), steps)
     same = all(torch.equal(a, b) for a, b in zip(outs_loop, outs_batch))
     batch.close()
     for v in vxs:
         v.close()
     value = args.batch_meshes * world / (t_batch * 1e-3)
     line = {"metric": BATCH_METRIC, "value": round(value, 2), "unit": "meshes/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_batch, 3), "higher_is_better": True,
+            "steps": steps, "warmup": warmup, "ms_per_step": round(t_batch, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32+u32",
             "data": f"synthetic (seeded {args.batch_meshes}-mesh mix: icospheres/tori, 500-500k triangles, "
                     "maxDimension 32-512, 1-16 materials)",
@@ -385,9 +434,8 @@ def run_batched(args, world, rank, local):
             "speedup_vs_loop": round(t_loop / t_batch, 3),
             "gvoxels_per_s": round(n_nodes * world / (t_batch * 1e-3) / 1e9, 3),
             "mtriangles_per_s": round(n_tris * world / (t_batch * 1e-3) / 1e6, 3),
-            "identical_to_loop": bool(same), "gpu_launches": int(launches * args.steps), "clocks": clk.summary()}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+            "identical_to_loop": bool(same), "gpu_launches": int(launches * steps), "clocks": clk.summary()}
+    return line
 
 
 SERVE_METRIC = "served voxelization (Poisson arrivals, 256-mesh mix shapes): sustained meshes/s and p50/p99 latency"
@@ -428,6 +476,21 @@ def run_served(args, world, rank, local):
     """Poisson request streams at several rates through the continuous-
     batching server, beside the plain path (one voxelization call per
     request, first come first served) under the same arrivals."""
+    rates = [50, 200, 1000, 2000]
+    rows = served_rows(args, local, rates, args.serve_seconds)
+    top = rows[-1]
+    line = {"metric": SERVE_METRIC, "value": top["served"]["meshes_per_s"], "unit": "meshes/s", "n_gpus": world,
+            "steps": len(rates), "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64+f32+u32", "data": "synthetic (seeded 256-mesh mix shapes, Poisson arrivals)",
+            "config": {"workload": "LongNode with materials; admission by a 160 GB device-memory budget; 2 lanes",
+                       "rates_req_s": rates, "seconds_per_rate": args.serve_seconds},
+            "p50_ms": top["served"]["p50_ms"], "p99_ms": top["served"]["p99_ms"], "rates": rows}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def served_rows(args, local, rates, seconds):
+    """Per rate: served and plain-path p50 / p99 latency and meshes/s."""
     import queue
 
     import torch
@@ -439,10 +502,9 @@ def run_served(args, world, rank, local):
     torch.cuda.set_device(local)
     pool = scenes.batch_mix(args.batch_meshes, seed=1)
     rng = np.random.default_rng(7)
-    rates = [50, 200, 1000, 2000]
     rows = []
     for rate in rates:
-        n = int(min(args.serve_max_requests, max(50, rate * args.serve_seconds)))
+        n = int(min(args.serve_max_requests, max(50, rate * seconds)))
         arrivals = _poisson(rate, n, rng)
         # Served.
         with VoxelServer(budget_bytes=160 << 30, lanes=2, device=local) as srv:
@@ -502,15 +564,7 @@ def run_served(args, world, rank, local):
                                 "p99_ms": pct(lat_s, 99), "batches": batches},
                      "plain": {"meshes_per_s": round(n / span_p, 1), "p50_ms": pct(lat_p, 50),
                                "p99_ms": pct(lat_p, 99)}})
-    top = rows[-1]
-    line = {"metric": SERVE_METRIC, "value": top["served"]["meshes_per_s"], "unit": "meshes/s", "n_gpus": world,
-            "steps": len(rates), "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64+f32+u32", "data": "synthetic (seeded 256-mesh mix shapes, Poisson arrivals)",
-            "config": {"workload": "LongNode with materials; admission by a 160 GB device-memory budget; 2 lanes",
-                       "rates_req_s": rates, "seconds_per_rate": args.serve_seconds},
-            "p50_ms": top["served"]["p50_ms"], "p99_ms": top["served"]["p99_ms"], "rates": rows}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return rows
 
 
 def autotune(args, call, rounds=8):
@@ -534,6 +588,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the short batched and served runs of the room line")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--workload", default="room", choices=["room", "batched", "served"],
                     help="room: the single-mesh headline; batched: the 256-mesh mix as one batch vs a per-mesh "
@@ -583,15 +638,14 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
-    vx.set_profiling(True)
     tuned = autotune(args, lambda: (vx.voxelize_device(1, MAX_DIM, out, stream=sh), stream.synchronize()))
     for _ in range(args.warmup):
         vx.voxelize_device(1, MAX_DIM, out, stream=sh)
     stream.synchronize()
     launches = vx.last_launch_count()
 
+    # Timed: profiling off (no stage events inside the timed calls).
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    stage_acc = {}
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -602,9 +656,6 @@ def main():
             evs[i][0].record(stream)
             vx.voxelize_device(1, MAX_DIM, out, stream=sh)
             evs[i][1].record(stream)
-            st = vx.stage_times()
-            for k, v in st.items():
-                stage_acc.setdefault(k, []).append(v)
         stream.synchronize()
     torch.cuda.synchronize()
     total_ms = sum(a.elapsed_time(b) for a, b in evs)
@@ -614,8 +665,19 @@ def main():
     ms = total_ms / args.steps
     value = replica_throughput(n_nodes, world, ms) / 1e9
 
-    # e2e through the reference-facing entry with host buffers.
+    # Stage times from a separate untimed pass with per-stage CUDA events.
+    stage_acc = {}
+    vx.set_profiling(True)
+    for _ in range(5):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        vx.voxelize_device(1, MAX_DIM, out, stream=sh)
+        for k, v in vx.stage_times().items():
+            stage_acc.setdefault(k, []).append(v)
     vx.set_profiling(False)
+    stream.synchronize()
+
+    # e2e through the reference-facing entry with host buffers.
     pin_v = torch.from_numpy(mesh.vertices.reshape(-1)).pin_memory().numpy()
     pin_i = torch.from_numpy(mesh.indices.reshape(-1).view(np.int32)).pin_memory().numpy().view(np.uint32)
     pin_m = torch.from_numpy(mesh.materials).pin_memory().numpy()
@@ -663,8 +725,8 @@ def main():
     line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64+f32+u32", "data": "synthetic (seeded room scene)",
-            "config": {"workload": WORKLOAD, "l2": "256 MB flush before every timed step",
-                       "parallelism": f"replicas x{world}", "autotune": tuned if tuned is not None else "off"},
+            "config": dict(CONFIG), "parallelism": f"replicas x{world}",
+            "autotune": tuned if tuned is not None else "off",
             "roofline": roofs[0],
             "roofline_next_kernel": roofs[1],
             "work": stats,
@@ -679,6 +741,23 @@ def main():
             "clocks": clk.summary()}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(mesh)
+    if rank == 0 and world == 1 and not args.no_extras:
+        # The batched and served forms of the target, in short runs: the
+        # 256-mesh mix as one graph-replayed batch against the per-mesh loop,
+        # and one Poisson rate through the server against the plain path.
+        vx.close()
+        del out, flush
+        torch.cuda.empty_cache()
+        bl = batched_line(args, 1, local, steps=10, warmup=3)
+        line["batched"] = {k: bl[k] for k in ("value", "unit", "ms_per_step", "per_mesh_loop", "speedup_vs_loop",
+                                               "identical_to_loop", "gvoxels_per_s", "mtriangles_per_s",
+                                               "gpu_launches", "clocks")}
+        line["batched"]["workload"] = bl["config"]["workload"]
+        row = served_rows(args, local, [1000], 1.0)[0]
+        line["served"] = {"rate_req_s": row["rate_req_s"], "requests": row["requests"], "unit": "meshes/s",
+                          "served": row["served"], "plain": row["plain"],
+                          "workload": "Poisson arrivals of the 256-mesh mix shapes, LongNode with materials, "
+                                      "160 GB admission budget, 2 lanes"}
     if dist:
         dist.barrier()
         dist.destroy_process_group()

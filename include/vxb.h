@@ -104,6 +104,10 @@ vxb_status vxb_set_materials(vxb_voxelizer* v, const uint8_t* materials, uint32_
 vxb_status vxb_set_material_output(vxb_voxelizer* v, int enable);
 /* verboseOutput(bool), include/voxelizer.h:866. */
 vxb_status vxb_verbose_output(vxb_voxelizer* v, int enable);
+/* The mesh's bounding box as the constructor computed it
+ * (calculateBoundingBox, src/host_side.cpp:2462-2488: the float vertices'
+ * component-wise min / max widened to double). */
+vxb_status vxb_bounding_box(const vxb_voxelizer* v, double min_vertex[3], double max_vertex[3]);
 
 /* Dimensions, voxel length and bounds a request produces, without running
  * it (getArrayDimensions, include/voxelizer.h:868-875, plus the getters
@@ -250,21 +254,33 @@ vxb_status vxb_batch_last_launch_count(vxb_batch* b, uint32_t* launches);
  * memory: solvers that reserve the whole GPU for their own pool, or that
  * cannot let cudaFree / cudaMalloc synchronize the device mid-step.  It
  * allocates nothing: the mesh (dev_vertices: 3 floats per vertex,
- * dev_indices: 3 indices < n_vertices per triangle) and dev_out are the
- * caller's device buffers, and its work lists live in a fixed device array
- * of 16,797,440 bytes inside the library, which every GPU that loads the
- * library holds until exit.  min_vertex / max_vertex: the mesh's bounding
- * box, the component-wise min / max of the vertices (vxb_plan reports it).
- * Limits: at most 2,097,152 triangles and 1024 yz subspaces (vox_split_res
- * parts in y times z); larger requests return VXB_EINVAL.  Runs on the
- * current device, stream-ordered on `stream`.  The first call on a device
- * looks up the array's address (one-time set-up); make it before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race
- * and must be serialized by the caller. */
+ * dev_indices: 3 indices per triangle) and dev_out are the caller's device
+ * buffers, and its work lists live in a fixed device array of 20,990,720
+ * bytes inside the library, which every GPU that loads the library holds
+ * until exit.  min_vertex / max_vertex: the mesh's bounding box, the
+ * component-wise min / max of the vertices (vxb_plan reports it).
+ * Limits: at most 1,048,576 triangles, 1024 yz subspaces (vox_split_res
+ * parts in y times z) and fewer than 2^32 (triangle, yz subspace, 4x4 tile)
+ * candidates, bounded by n_triangles * (ceil(Y / 4) + parts in y) *
+ * (ceil(Z / 4) + parts in z) over the grid's resolution Y x Z; larger
+ * requests return VXB_EINVAL.  Runs on the current device, stream-ordered on
+ * `stream`; it neither waits for the GPU nor copies from host memory.  The
+ * first call on a device looks up the array's address (one-time set-up);
+ * make it before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race and must be serialized by the caller. */
 vxb_status vxb_voxelize_bits_noalloc(const float* dev_vertices, const uint32_t* dev_indices, uint32_t n_vertices,
                                      uint32_t n_triangles, const double min_vertex[3], const double max_vertex[3],
                                      const vxb_request* req, void* dev_out, uint64_t dev_bytes, void* stream,
                                      vxb_grid_info* info);
+
+/* No counterpart in the reference.  The errors of the last
+ * vxb_voxelize_bits_noalloc call on the current device that only the GPU
+ * sees: VXB_EINVAL if an index was >= n_vertices (such indices read vertex
+ * 0, so no kernel reads past the vertex buffer, but the bit array is
+ * undefined), VXB_EOVERFLOW if the candidate count overflowed, else VXB_OK.
+ * Call it once that call's stream has finished; it copies 12 bytes from the
+ * device and allocates nothing. */
+vxb_status vxb_noalloc_status(void);
 
 #ifdef __cplusplus
 }

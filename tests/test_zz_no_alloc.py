@@ -6,8 +6,9 @@ voxelize, or that cannot afford the device-wide synchronization of
 cudaMalloc / cudaFree in the middle of a time step.  Its work lists live in a
 fixed array inside the library that every call reuses, so the GPU check runs
 two different requests back to back on that array and compares each result
-bit for bit with the allocating entry point's.  This file is named to be
-collected last.
+bit for bit with the allocating entry point's.  Errors that only the GPU sees (an
+index past the vertex buffer) are read back with vxb_noalloc_status once
+the call's stream has finished.  This file is named to be collected last.
 """
 
 import ctypes
@@ -18,7 +19,7 @@ import pytest
 from voxelizer_b200 import _lib, scenes
 from voxelizer_b200.api import LONG, Voxelizer
 
-MAX_TRIANGLES = 1 << 21
+MAX_TRIANGLES = 1 << 20
 
 
 class _FakeBuffer:
@@ -50,11 +51,78 @@ def test_noalloc_rejects_oversized_requests():
     box = ((0.0, 0.0, 0.0), (1.0, 1.0, 1.0))
     st, _ = _noalloc(lib, 256, 256, 3, MAX_TRIANGLES + 1, *box, _lib.make_request(64), _FakeBuffer())
     assert st == -1
-    assert b"2097152" in lib.vxb_last_error()
+    assert b"1048576" in lib.vxb_last_error()
     # One yz subspace per voxel row and column: 200 x 200 subspaces.
     st, _ = _noalloc(lib, 256, 256, 3, 1, *box, _lib.make_request(200, vox_split=(1024, 1, 1)), _FakeBuffer())
     assert st == -1
     assert b"1024" in lib.vxb_last_error() and b"subspaces" in lib.vxb_last_error()
+    # The candidate bound: 1M triangles over a 4096 x 4096 yz plane in 8 x 8
+    # subspaces could list more than 2^32 (triangle, tile) candidates.
+    slab = ((0.0, 0.0, 0.0), (0.01, 1.0, 1.0))
+    st, _ = _noalloc(lib, 256, 256, 3, MAX_TRIANGLES, *slab, _lib.make_request(4096, vox_split=(1024, 512, 512)),
+                     _FakeBuffer())
+    assert st == -1
+    assert b"2^32" in lib.vxb_last_error()
+    # A voxel length so small that the resolution would wrap 32 bits.
+    st, _ = _noalloc(lib, 256, 256, 3, 1, *box, _lib.make_request(1e-12), _FakeBuffer())
+    assert st == -1
+
+
+def _sphere_on_device(torch):
+    v, i = scenes.icosphere(3, radius=1.0, center=(0.1, -0.2, 0.05))
+    v = v.astype(np.float32)
+    i = i.astype(np.uint32)
+    return v, i, torch.from_numpy(v.reshape(-1)).cuda(), torch.from_numpy(i.reshape(-1).view(np.int32)).cuda()
+
+
+@pytest.mark.gpu
+def test_noalloc_reports_index_out_of_range():
+    """An index >= n_vertices is caught on the device: the call reads vertex
+    0 in its place (nothing past the vertex buffer), and the status call
+    reports VXB_EINVAL once the stream has finished; the next valid call
+    clears it."""
+    torch = pytest.importorskip("torch")
+    lib = _lib.lib()
+    v, i, dv, di = _sphere_on_device(torch)
+    with Voxelizer(v, i, node_type=LONG) as vx:
+        info = vx.plan(0, 64)
+    out = torch.zeros(int(info.count), dtype=torch.int32, device="cuda")
+    bad = di.clone()
+    bad[7] = v.shape[0] + 5
+    st, _ = _noalloc(lib, dv.data_ptr(), bad.data_ptr(), v.shape[0], i.shape[0], info.min_vertex, info.max_vertex,
+                     _lib.make_request(64), out)
+    assert st == 0, lib.vxb_last_error()
+    torch.cuda.synchronize()
+    assert lib.vxb_noalloc_status() == -1
+    assert b"index" in lib.vxb_last_error()
+    st, _ = _noalloc(lib, dv.data_ptr(), di.data_ptr(), v.shape[0], i.shape[0], info.min_vertex, info.max_vertex,
+                     _lib.make_request(64), out)
+    assert st == 0
+    torch.cuda.synchronize()
+    assert lib.vxb_noalloc_status() == 0
+
+
+@pytest.mark.gpu
+def test_noalloc_on_a_non_default_stream():
+    """Stream-ordered on the caller's stream: the result equals the
+    allocating entry point's, and the status reads back clean."""
+    torch = pytest.importorskip("torch")
+    lib = _lib.lib()
+    v, i, dv, di = _sphere_on_device(torch)
+    with Voxelizer(v, i, node_type=LONG) as vx:
+        info = vx.plan(0, 96)
+        ref = torch.empty(int(info.count), dtype=torch.int32, device="cuda")
+        vx.voxelize_device(0, 96, ref)
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream()
+    out = torch.full((int(info.count),), -1, dtype=torch.int32, device="cuda")
+    with torch.cuda.stream(s):
+        st, _ = _noalloc(lib, dv.data_ptr(), di.data_ptr(), v.shape[0], i.shape[0], info.min_vertex,
+                         info.max_vertex, _lib.make_request(96), out, stream=s.cuda_stream)
+    assert st == 0, lib.vxb_last_error()
+    s.synchronize()
+    assert lib.vxb_noalloc_status() == 0
+    assert torch.equal(out, ref)
 
 
 @pytest.mark.gpu
@@ -90,3 +158,4 @@ def test_noalloc_matches_device_entry_on_two_calls():
             assert int(ref.ne(0).sum()) > 0
             assert torch.equal(out[: ref.numel()], ref), f"bit array differs for request {size!r}"
             assert bool((out[ref.numel():] == -1).all()), "wrote past the result"
+            assert lib.vxb_noalloc_status() == 0

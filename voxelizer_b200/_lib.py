@@ -28,7 +28,7 @@ EXPORTS = ["vxb_last_error", "vxb_version", "vxb_create", "vxb_destroy", "vxb_se
            "vxb_batch_destroy", "vxb_batch_add", "vxb_batch_clear", "vxb_batch_run", "vxb_batch_last_launch_count",
            "vxb_last_stats", "vxb_plan_parts", "vxb_voxelize_parts_to_device", "vxb_voxelize_parts_to_host",
            "vxb_plan_slice", "vxb_voxelize_slice_to_device", "vxb_voxelize_slice_to_host", "vxb_set_autotune",
-           "vxb_autotune_state"]
+           "vxb_autotune_state", "vxb_noalloc_status", "vxb_bounding_box"]
 
 BATCH_GRAPH = 1
 
@@ -125,6 +125,8 @@ def lib():
         "vxb_voxelize_bits_noalloc": (ctypes.c_int, [vp, vp, ctypes.c_uint32, ctypes.c_uint32, P(ctypes.c_double),
                                                      P(ctypes.c_double), P(Request), vp, ctypes.c_uint64, vp,
                                                      P(GridInfo)]),
+        "vxb_noalloc_status": (ctypes.c_int, []),
+        "vxb_bounding_box": (ctypes.c_int, [vp, P(ctypes.c_double), P(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

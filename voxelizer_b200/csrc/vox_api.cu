@@ -32,19 +32,12 @@ Voxelizer<Node>::Voxelizer(float const* _vertices, uint const* _indices, uint _n
     check(vxb_create(&handle, Node::kind, _vertices, _indices, _nrOfVertices, _nrOfTriangles, 0));
     vertices.assign(_vertices, _vertices + 3 * (size_t)_nrOfVertices);
     indices.assign(_indices, _indices + 3 * (size_t)_nrOfTriangles);
-    // calculateBoundingBox, src/host_side.cpp:2462-2488
-    minVertex = make_double3(0, 0, 0);
-    maxVertex = make_double3(0, 0, 0);
-    if (_nrOfVertices > 0) {
-        double mn[3] = {_vertices[0], _vertices[1], _vertices[2]}, mx[3] = {mn[0], mn[1], mn[2]};
-        for (uint i = 1; i < _nrOfVertices; ++i)
-            for (int a = 0; a < 3; ++a) {
-                if (_vertices[3 * i + a] > mx[a]) mx[a] = _vertices[3 * i + a];
-                if (_vertices[3 * i + a] < mn[a]) mn[a] = _vertices[3 * i + a];
-            }
-        minVertex = make_double3(mn[0], mn[1], mn[2]);
-        maxVertex = make_double3(mx[0], mx[1], mx[2]);
-    }
+    // calculateBoundingBox (src/host_side.cpp:2462-2488) ran in vxb_create,
+    // on the device when there is one.
+    double mn[3], mx[3];
+    check(vxb_bounding_box(handle, mn, mx));
+    minVertex = make_double3(mn[0], mn[1], mn[2]);
+    maxVertex = make_double3(mx[0], mx[1], mx[2]);
     resolution = make_uint3(256, 0, 0);
 }
 

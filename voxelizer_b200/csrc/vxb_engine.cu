@@ -554,6 +554,15 @@ vxb_status vxb_create(vxb_voxelizer** out, int node_type, const float* vertices,
     return VXB_OK;
 }
 
+vxb_status vxb_bounding_box(const vxb_voxelizer* v, double min_vertex[3], double max_vertex[3]) {
+    if (!v || !min_vertex || !max_vertex) return failf(VXB_EINVAL, "NULL argument");
+    for (int a = 0; a < 3; ++a) {
+        min_vertex[a] = v->mn[a];
+        max_vertex[a] = v->mx[a];
+    }
+    return VXB_OK;
+}
+
 vxb_status vxb_destroy(vxb_voxelizer* v) {
     if (!v) return VXB_OK;
     // The instance's buffers go back to the block cache: after a failed

@@ -6,25 +6,32 @@
 // times cudaMalloc) synchronizes the whole device, which a caller that keeps
 // several streams busy cannot afford in the middle of a time step.  The
 // caller passes the mesh and the output already in device memory; the work
-// lists this path needs (per-triangle candidate counts, their scan and the
-// yz subspace table) live in a fixed, statically sized array in device
-// memory instead of buffers allocated per call.  The call itself allocates
-// nothing, on the device or on the host (its subspace table is built on the
-// stack); the array is placed by the CUDA driver when it loads this
-// library's device code.
+// lists this path needs (a range-checked copy of the indices, per-triangle
+// candidate counts, their scan, the yz subspace table and the unit table)
+// live in a fixed, statically sized array in device memory instead of
+// buffers allocated per call.  The call itself allocates nothing, on the
+// device or on the host; its tables are passed to a set-up kernel by value,
+// so it copies nothing from host memory either.  The array is placed by the
+// CUDA driver when it loads this library's device code.
 //
 // Limits: at most kMaxTriangles triangles and kMaxSubspaces yz subspaces
-// per call; larger requests are rejected with VXB_EINVAL.
+// per call, and fewer than 2^32 (triangle, subspace, tile) candidates by the
+// bound checked below; larger requests are rejected with VXB_EINVAL.
+//
+// Errors found on the device (an index >= n_vertices, a candidate count
+// that overflows) cannot be returned by the call, which does not wait for
+// the GPU; vxb_noalloc_status() reports them for the last call on the
+// current device once its stream has finished.
 //
 // The first call on a device looks up the array's device address (a
 // one-time set-up per device, made with that device current); make that
 // first call before any stream capture.
 //
 // The array is shared by every call on a device and keeps the previous
-// call's contents; each call overwrites everything it reads before reading
-// it, so nothing has to be cleared.  Calls whose work overlaps on the GPU
-// (two host threads, or two streams without ordering between them) race on
-// the array and give undefined results: serialize them.
+// call's contents; each call clears its status words and overwrites
+// everything else it reads before reading it.  Calls whose work overlaps on
+// the GPU (two host threads, or two streams without ordering between them)
+// race on the array and give undefined results: serialize them.
 
 #include "vxb.h"
 #include "vxb_kernels.cuh"
@@ -44,7 +51,7 @@ int recordError(int code, const char* msg);  // vxb_host.cu
 
 namespace {
 
-constexpr uint32_t kMaxTriangles = 1u << 21;  // 2,097,152
+constexpr uint32_t kMaxTriangles = 1u << 20;  // 1,048,576
 constexpr uint32_t kMaxSubspaces = 1024;
 constexpr uint32_t kScanTile = 4096;          // items per tile of launch_scan
 constexpr int kMaxDevices = 64;
@@ -61,19 +68,20 @@ struct UnitTables {
 };
 
 // Layout of the scratch array (byte offsets).
-constexpr size_t kStatusOff = 0;  // [0] candidate total, [1] overflow flag
+constexpr size_t kStatusOff = 0;  // [0] candidate total, [1] overflow flag, [2] index out of range
 constexpr size_t kTablesOff = kStatusOff + 256;
 constexpr size_t kSubspaceOff = kTablesOff + 768;
 static_assert(sizeof(UnitTables) <= 768, "tables region");
 constexpr size_t kTileOff = kSubspaceOff + roundUp(kMaxSubspaces * sizeof(vxb::SplitYZ));
 constexpr size_t kCountOff = kTileOff + roundUp(4 * (kMaxTriangles / kScanTile + 2));
 constexpr size_t kOffsetOff = kCountOff + roundUp(4 * ((size_t)kMaxTriangles + 1));
-constexpr size_t kScratchBytes = kOffsetOff + roundUp(4 * ((size_t)kMaxTriangles + 2));
-static_assert(kScratchBytes == 16797440, "scratch layout changed: update the stated size");
+constexpr size_t kIndexOff = kOffsetOff + roundUp(4 * ((size_t)kMaxTriangles + 2));
+constexpr size_t kScratchBytes = kIndexOff + roundUp(12 * (size_t)kMaxTriangles);
+static_assert(kScratchBytes == 20990720, "scratch layout changed: update the stated size");
 
 }  // namespace
 
-// 16,797,440 bytes (about 16.0 MiB) of device memory, held by every GPU that
+// 20,990,720 bytes (about 20.0 MiB) of device memory, held by every GPU that
 // loads this library until the process exits.
 static __device__ __align__(256) unsigned char g_noallocScratch[kScratchBytes];
 
@@ -111,67 +119,34 @@ int scratchAddress(int device, unsigned char** out) {
     return 0;
 }
 
-// The grid arithmetic of vxb::makePlan (determineDimensions and the x
-// rounding of src/host_side.cpp:2497-2634) without its split vectors.
-struct BitGrid {
-    double d;
-    uint32_t res[3], alloc[3], xSplits;
-};
-
-int sizeGrid(const double* mn, const double* mx, const vxb_request* r, BitGrid& g) {
-    const double dx = mx[0] - mn[0], dy = mx[1] - mn[1], dz = mx[2] - mn[2];
-    uint32_t res[3];
-    double d;
-    if (r->by_cube_length) {
-        if (!(r->cube_length > 0.0)) return -1;
-        d = r->cube_length;
-        res[0] = vxb::toUint(std::ceil(dx / d)) + 1;
-        res[1] = vxb::toUint(std::ceil(dy / d)) + 1;
-        res[2] = vxb::toUint(std::ceil(dz / d)) + 1;
-    } else {
-        if (r->max_dimension < 2) return -1;
-        const uint32_t m = r->max_dimension;
-        if (dx > dy && dx > dz) {
-            d = dx / double(m - 1);
-            res[0] = m; res[1] = vxb::toUint(std::ceil(dy / d)) + 1; res[2] = vxb::toUint(std::ceil(dz / d)) + 1;
-        } else if (dx > dy) {
-            d = dz / double(m - 1);
-            res[2] = m; res[0] = vxb::toUint(std::ceil(dx / d)) + 1; res[1] = vxb::toUint(std::ceil(dy / d)) + 1;
-        } else if (dy > dz) {
-            d = dy / double(m - 1);
-            res[1] = m; res[0] = vxb::toUint(std::ceil(dx / d)) + 1; res[2] = vxb::toUint(std::ceil(dz / d)) + 1;
-        } else {
-            d = dz / double(m - 1);
-            res[2] = m; res[0] = vxb::toUint(std::ceil(dx / d)) + 1; res[1] = vxb::toUint(std::ceil(dy / d)) + 1;
-        }
-        if (!(d > 0.0)) return -1;
+// Set-up of one call: the unit table (by value), the yz subspaces of the
+// solid pass in the reference's order (z outer; splitResolutionByNrOfParts
+// per axis) and cleared status words.
+__global__ void noallocSetupKernel(UnitTables tab, uint32_t resY, uint32_t resZ, uint32_t splitY, uint32_t splitZ,
+                                   UnitTables* dtab, vxb::SplitYZ* dsub, uint32_t* status) {
+    if (threadIdx.x == 0) {
+        *dtab = tab;
+        status[0] = status[1] = status[2] = 0u;
     }
-    res[0] += 2;
-    const uint32_t vs[3] = {r->vox_split_res.x, r->vox_split_res.y, r->vox_split_res.z};
-    for (int a = 0; a < 3; ++a)
-        if (vs[a] == 0) return -1;
-    g.d = d;
-    g.xSplits = (res[0] + vs[0] - 1) / vs[0];
-    const uint32_t xMod = 32u * g.xSplits;
-    if (res[0] % xMod != 0) res[0] += xMod - res[0] % xMod;
-    if (res[0] / g.xSplits > 1024) return -1;
-    for (int a = 0; a < 3; ++a) g.res[a] = res[a];
-    g.alloc[0] = res[0];
-    g.alloc[1] = res[1] + 2;
-    g.alloc[2] = res[2] + 2;
-    return 0;
+    const uint32_t ny = (resY + splitY - 1) / splitY, nz = (resZ + splitZ - 1) / splitZ;
+    for (uint32_t k = threadIdx.x; k < ny * nz; k += blockDim.x) {
+        const vxb::Range ry = vxb::splitPart(resY, splitY, k % ny), rz = vxb::splitPart(resZ, splitZ, k / ny);
+        dsub[k] = vxb::SplitYZ{ry.lo, ry.hi, rz.lo, rz.hi};
+    }
 }
 
-// Parts of splitResolutionByNrOfParts (vxb::splitLength) into `out`.
-uint32_t splitInto(uint32_t len, uint32_t maxPart, vxb::Range* out) {
-    const uint32_t n = (len + maxPart - 1) / maxPart;
-    uint32_t prev = len;
-    for (uint32_t i = n; i > 0; --i) {
-        out[i - 1].hi = prev;
-        out[i - 1].lo = prev - prev / i;
-        prev = out[i - 1].lo;
+// The caller's indices, range-checked: an index >= nV reads vertex 0
+// instead and sets status[2], so no kernel reads past the vertex buffer.
+__global__ void noallocIndexKernel(const uint32_t* __restrict__ idx, uint32_t n, uint32_t nV, uint32_t* __restrict__ out,
+                                   uint32_t* status) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t v = idx[i];
+        if (v >= nV) {
+            v = 0u;
+            status[2] = 1u;
+        }
+        out[i] = v;
     }
-    return n;
 }
 
 }  // namespace
@@ -189,8 +164,9 @@ extern "C" vxb_status vxb_voxelize_bits_noalloc(const float* dev_vertices, const
                      "%u triangles exceed the %u that the allocation-free path's fixed scratch array holds; "
                      "use vxb_voxelize_to_device",
                      n_triangles, kMaxTriangles);
-    BitGrid bg;
-    if (sizeGrid(min_vertex, max_vertex, req, bg))
+    vxb::GridSize bg;
+    const uint32_t vs[3] = {req->vox_split_res.x, req->vox_split_res.y, req->vox_split_res.z};
+    if (vxb::sizeGrid(min_vertex, max_vertex, req->by_cube_length, req->max_dimension, req->cube_length, vs, bg))
         return failf(VXB_EINVAL, "invalid request (maxDimension >= 2 or cubeLength > 0, split sizes > 0 and an x "
                                  "pass of at most 1024 voxels are required)");
     const uint64_t voxels = (uint64_t)bg.alloc[0] * bg.alloc[1] * bg.alloc[2];
@@ -202,6 +178,15 @@ extern "C" vxb_status vxb_voxelize_bits_noalloc(const float* dev_vertices, const
                      "%llu yz subspaces exceed the %u that the allocation-free path's fixed scratch array holds; "
                      "use larger split sizes",
                      (unsigned long long)ny * nz, kMaxSubspaces);
+    // A triangle is a candidate at most once per (subspace, 4x4 tile) pair
+    // it overlaps, and a subspace cut adds at most one partial tile per
+    // axis: keep the scan of candidate counts below 2^32.
+    const double bound = (double)n_triangles * (double)((bg.res[1] + 3) / 4 + ny) * (double)((bg.res[2] + 3) / 4 + nz);
+    if (bound >= 4294967295.0)
+        return failf(VXB_EINVAL,
+                     "up to %.0f (triangle, tile) candidates: the allocation-free path takes fewer than 2^32; use "
+                     "vxb_voxelize_to_device",
+                     bound);
     vxb_grid_info gi;
     memset(&gi, 0, sizeof(gi));
     gi.dim.x = bg.alloc[0];
@@ -230,15 +215,7 @@ extern "C" vxb_status vxb_voxelize_bits_noalloc(const float* dev_vertices, const
     unsigned char* scratch = nullptr;
     if (int rc = scratchAddress(device, &scratch)) return rc;
 
-    // yz subspaces of the solid pass in the reference's order (z outer).
-    vxb::Range ys[kMaxSubspaces], zs[kMaxSubspaces];
-    vxb::SplitYZ sub[kMaxSubspaces];
-    splitInto(bg.res[1], req->vox_split_res.y, ys);
-    splitInto(bg.res[2], req->vox_split_res.z, zs);
-    uint32_t nSub = 0;
-    for (uint32_t z = 0; z < nz; ++z)
-        for (uint32_t y = 0; y < ny; ++y) sub[nSub++] = vxb::SplitYZ{ys[y].lo, ys[y].hi, zs[z].lo, zs[z].hi};
-
+    const uint32_t nSub = ny * nz;
     UnitTables tab;
     memset(&tab, 0, sizeof(tab));
     vxb::PassGeom& g = tab.unit.g;
@@ -257,8 +234,9 @@ extern "C" vxb_status vxb_voxelize_bits_noalloc(const float* dev_vertices, const
     g.padY = 1;
     g.padZ = 1;
     g.border = 0;
+    uint32_t* checkedIdx = reinterpret_cast<uint32_t*>(scratch + kIndexOff);
     tab.unit.V = dev_vertices;
-    tab.unit.I = dev_indices;
+    tab.unit.I = checkedIdx;
     tab.unit.nT = n_triangles;
     tab.unit.nSplits = nSub;
     tab.unit.out = dev_out;
@@ -284,17 +262,39 @@ extern "C" vxb_status vxb_voxelize_bits_noalloc(const float* dev_vertices, const
     b.splits = dsub;
     uint32_t launches = 0;
     e = cudaMemsetAsync(grid, 0, gi.bytes, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dtab, &tab, sizeof(tab), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dsub, sub, nSub * sizeof(vxb::SplitYZ), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return failf(VXB_ECUDA, "%s", cudaGetErrorString(e));
     }
+    noallocSetupKernel<<<1, 256, 0, s>>>(tab, bg.res[1], bg.res[2], req->vox_split_res.y, req->vox_split_res.z, dtab,
+                                         dsub, status);
+    const uint32_t nIdx = 3u * n_triangles;
+    noallocIndexKernel<<<(nIdx + 255) / 256 < 148u * 8u ? (nIdx + 255) / 256 : 148u * 8u, 256, 0, s>>>(
+        dev_indices, nIdx, n_vertices, checkedIdx, status);
+    launches += 2;
     vxb::launch_solid_count(b, n_triangles, counts, s, &launches);
     vxb::launch_scan(counts, offsets, n_triangles, tiles, status, status + 1, s, &launches);
     vxb::launch_solid_toggle(b, n_triangles, offsets, status, grid, 3, s, &launches);
     vxb::launch_row_fill(b, tab.rowBase[1], grid, s, &launches);
     e = cudaGetLastError();
     if (e != cudaSuccess) return failf(VXB_ECUDA, "%s", cudaGetErrorString(e));
+    return VXB_OK;
+}
+
+extern "C" vxb_status vxb_noalloc_status(void) {
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return failf(VXB_ECUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+    if (device < 0 || device >= kMaxDevices) return failf(VXB_EINVAL, "device %d is not supported", device);
+    unsigned char* scratch = nullptr;
+    if (int rc = scratchAddress(device, &scratch)) return rc;
+    uint32_t st[3] = {0, 0, 0};
+    e = cudaMemcpy(st, scratch + kStatusOff, sizeof(st), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return failf(VXB_ECUDA, "reading the status words: %s", cudaGetErrorString(e));
+    }
+    if (st[2]) return failf(VXB_EINVAL, "the last call's mesh has an index >= n_vertices; its bit array is undefined");
+    if (st[1]) return failf(VXB_EOVERFLOW, "the last call's candidate count overflowed; its bit array is undefined");
     return VXB_OK;
 }

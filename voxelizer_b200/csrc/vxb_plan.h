@@ -11,6 +11,12 @@
 #include <cstdint>
 #include <vector>
 
+#ifdef __CUDACC__
+#define VXB_HD __host__ __device__
+#else
+#define VXB_HD
+#endif
+
 namespace vxb {
 
 struct Range { uint32_t lo, hi; };
@@ -45,18 +51,34 @@ inline uint32_t toUint(double v) {
 }
 
 // splitResolutionByNrOfParts: floor division, the remainder goes to the
-// first part (src/host_side.cpp:3025-3105).
-inline std::vector<Range> splitLength(uint32_t len, uint32_t maxPart) {
+// first part (src/host_side.cpp:3025-3105).  Writes the parts of [0, len)
+// into out (room for ceil(len / maxPart) ranges) and returns their number.
+inline uint32_t splitInto(uint32_t len, uint32_t maxPart, Range* out) {
     const uint32_t n = (len + maxPart - 1) / maxPart;
-    std::vector<Range> out(n);
     uint32_t prev = len;
     for (uint32_t i = n; i > 0; --i) {
-        Range r;
-        r.hi = prev;
-        r.lo = r.hi - r.hi / i;
-        prev = r.lo;
-        out[i - 1] = r;
+        out[i - 1].hi = prev;
+        out[i - 1].lo = prev - prev / i;
+        prev = out[i - 1].lo;
     }
+    return n;
+}
+
+// Part i alone of the same split (for device code that has no room for the
+// whole list).
+VXB_HD inline Range splitPart(uint32_t len, uint32_t maxPart, uint32_t i) {
+    const uint32_t n = (len + maxPart - 1) / maxPart;
+    uint32_t prev = len;
+    for (uint32_t k = n; k > i + 1; --k) prev -= prev / k;
+    Range r;
+    r.hi = prev;
+    r.lo = prev - prev / (i + 1);
+    return r;
+}
+
+inline std::vector<Range> splitLength(uint32_t len, uint32_t maxPart) {
+    std::vector<Range> out((len + maxPart - 1) / maxPart);
+    splitInto(len, maxPart, out.data());
     return out;
 }
 
@@ -69,52 +91,87 @@ inline void boundingBox(const float* v, uint32_t nV, double* mn, double* mx) {
         }
 }
 
-// Returns 0, or a negative vxb status for arguments the path cannot honour.
-inline int makePlan(const double* mn, const double* mx, int byCube, uint32_t maxDim, double cube,
-                    const uint32_t* voxSplit, const uint32_t* matSplit, Plan& p) {
-    for (int a = 0; a < 3; ++a) { p.mn[a] = mn[a]; p.mx[a] = mx[a]; p.mnHost[a] = mn[a]; }
+// The grid of determineDimensions and adjustResolution without the split
+// lists.
+struct GridSize {
+    double d;              // voxel length
+    uint32_t res[3];       // resolution.max: x padded (+2) and rounded to 32 * xSplits
+    uint32_t xSplits, xRes;
+    uint32_t alloc[3];     // res + (0, 2, 2)
+};
+
+// uint(ceil(extent / d)) + 1 of determineDimensions; false where the count
+// leaves no room for the padding rows in 32 bits (the reference would wrap
+// to an empty grid there).
+inline bool axisRes(double extent, double d, uint32_t& r) {
+    const double c = std::ceil(extent / d);
+    if (c >= 4294967290.0) return false;
+    r = toUint(c) + 1;
+    return true;
+}
+
+// Returns 0, or -1 for arguments the path cannot honour.
+inline int sizeGrid(const double* mn, const double* mx, int byCube, uint32_t maxDim, double cube,
+                    const uint32_t* voxSplit, GridSize& g) {
     const double dx = mx[0] - mn[0], dy = mx[1] - mn[1], dz = mx[2] - mn[2];
     uint32_t r[3];
     double d;
+    bool ok = true;
     if (byCube) {
         if (!(cube > 0.0)) return -1;
         d = cube;
-        r[0] = toUint(std::ceil(dx / d)) + 1;
-        r[1] = toUint(std::ceil(dy / d)) + 1;
-        r[2] = toUint(std::ceil(dz / d)) + 1;
+        ok = axisRes(dx, d, r[0]) && axisRes(dy, d, r[1]) && axisRes(dz, d, r[2]);
     } else {
         if (maxDim < 2) return -1;
         const uint32_t m = maxDim;
         if (dx > dy && dx > dz) {
             d = dx / double(m - 1);
-            r[0] = m; r[1] = toUint(std::ceil(dy / d)) + 1; r[2] = toUint(std::ceil(dz / d)) + 1;
+            r[0] = m; ok = axisRes(dy, d, r[1]) && axisRes(dz, d, r[2]);
         } else if (dx > dy) {
             d = dz / double(m - 1);
-            r[2] = m; r[0] = toUint(std::ceil(dx / d)) + 1; r[1] = toUint(std::ceil(dy / d)) + 1;
+            r[2] = m; ok = axisRes(dx, d, r[0]) && axisRes(dy, d, r[1]);
         } else if (dy > dz) {
             d = dy / double(m - 1);
-            r[1] = m; r[0] = toUint(std::ceil(dx / d)) + 1; r[2] = toUint(std::ceil(dz / d)) + 1;
+            r[1] = m; ok = axisRes(dx, d, r[0]) && axisRes(dz, d, r[2]);
         } else {
             d = dz / double(m - 1);
-            r[2] = m; r[0] = toUint(std::ceil(dx / d)) + 1; r[1] = toUint(std::ceil(dy / d)) + 1;
+            r[2] = m; ok = axisRes(dx, d, r[0]) && axisRes(dy, d, r[1]);
         }
         if (!(d > 0.0)) return -1;
     }
+    if (!ok || r[0] > 0xFFFFFFFFu - 2u || r[1] > 0xFFFFFFFFu - 2u || r[2] > 0xFFFFFFFFu - 2u) return -1;
     r[0] += 2;
     for (int a = 0; a < 3; ++a)
         if (voxSplit[a] == 0) return -1;
-    p.d = d;
-    p.xSplits = (r[0] + voxSplit[0] - 1) / voxSplit[0];
-    const uint32_t xMod = 32u * p.xSplits;
+    g.d = d;
+    g.xSplits = (r[0] + voxSplit[0] - 1) / voxSplit[0];
+    const uint32_t xMod = 32u * g.xSplits;
     if (r[0] % xMod != 0) r[0] += xMod - r[0] % xMod;
-    p.xRes = r[0] / p.xSplits;
+    g.xRes = r[0] / g.xSplits;
     // The reference's per-split word mask (src/voxelizer.cu:1579-1616) holds
     // 32 words, so an x pass longer than 1024 voxels is undefined there.
-    if (p.xRes > 1024) return -1;
-    for (int a = 0; a < 3; ++a) p.res[a] = r[a];
-    p.alloc[0] = r[0];
-    p.alloc[1] = r[1] + 2;
-    p.alloc[2] = r[2] + 2;
+    if (g.xRes > 1024) return -1;
+    for (int a = 0; a < 3; ++a) g.res[a] = r[a];
+    g.alloc[0] = r[0];
+    g.alloc[1] = r[1] + 2;
+    g.alloc[2] = r[2] + 2;
+    return 0;
+}
+
+// Returns 0, or a negative vxb status for arguments the path cannot honour.
+inline int makePlan(const double* mn, const double* mx, int byCube, uint32_t maxDim, double cube,
+                    const uint32_t* voxSplit, const uint32_t* matSplit, Plan& p) {
+    for (int a = 0; a < 3; ++a) { p.mn[a] = mn[a]; p.mx[a] = mx[a]; p.mnHost[a] = mn[a]; }
+    GridSize g;
+    if (sizeGrid(mn, mx, byCube, maxDim, cube, voxSplit, g)) return -1;
+    const uint32_t* r = g.res;
+    p.d = g.d;
+    p.xSplits = g.xSplits;
+    p.xRes = g.xRes;
+    for (int a = 0; a < 3; ++a) {
+        p.res[a] = g.res[a];
+        p.alloc[a] = g.alloc[a];
+    }
     p.ySplitsExt = splitLength(r[1], voxSplit[1]);
     p.zSplitsExt = splitLength(r[2], voxSplit[2]);
     p.ySplitsAlloc = splitLength(p.alloc[1], voxSplit[1]);

@@ -17,7 +17,9 @@ constexpr uint32_t kScanTile = kScanThreads * kScanItems;
 
 // ---------------------------------------------------------------------------
 // Exclusive scan of per-triangle counts (three kernels: tile scan, scan of
-// tile sums, tile offsets).  Totals above 2^32 set *overflow.
+// tile sums, tile offsets).  Totals of 2^32 - 1 or more set *overflow: a
+// tile whose own sum wraps 32 bits reports the saturated sum 2^32 - 1, so
+// the 64-bit carry over the tile sums sees it.
 
 __device__ __forceinline__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* warpSums, uint32_t& blockTotal) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -53,36 +55,42 @@ __global__ void scanTileKernel(const uint32_t* __restrict__ in, uint32_t* __rest
     __shared__ uint32_t warpSums[33];
     const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
-    uint32_t sum = 0;
+    unsigned long long sum64 = 0;
 #pragma unroll
     for (int i = 0; i < kScanItems; ++i) {
         v[i] = (base + i < n) ? in[base + i] : 0u;
-        sum += v[i];
+        sum64 += v[i];
     }
+    const uint32_t sum = (uint32_t)sum64;
     uint32_t total;
     uint32_t ex = blockExclusiveScan(sum, warpSums, total);
+    // A 32-bit prefix that passes 2^32 wraps at the thread whose items cross
+    // it, so the tile's sum is exact unless some thread saw a wrap.
+    const int wrapped = __syncthreads_or(sum64 > 0xFFFFFFFFull || ex + sum < ex);
 #pragma unroll
     for (int i = 0; i < kScanItems; ++i) {
         if (base + i < n) out[base + i] = ex;
         ex += v[i];
     }
-    if (threadIdx.x == 0) tileSums[blockIdx.x] = total;
+    if (threadIdx.x == 0) tileSums[blockIdx.x] = wrapped ? 0xFFFFFFFFu : total;
 }
 
 __global__ void scanSumsKernel(uint32_t* tileSums, uint32_t nTiles, uint32_t* total, uint32_t* overflow) {
     __shared__ uint32_t warpSums[33];
     unsigned long long carry = 0;
+    int wrapped = 0;
     for (uint32_t start = 0; start < nTiles; start += blockDim.x) {
         uint32_t i = start + threadIdx.x;
         uint32_t v = i < nTiles ? tileSums[i] : 0u;
         uint32_t chunk;
         uint32_t ex = blockExclusiveScan(v, warpSums, chunk);
+        wrapped |= __syncthreads_or(ex + v < ex);
         if (i < nTiles) tileSums[i] = (uint32_t)(carry + ex);
         carry += chunk;
     }
     if (threadIdx.x == 0) {
         *total = (uint32_t)carry;
-        *overflow = carry > 0xFFFFFFFFull ? 1u : 0u;
+        *overflow = (wrapped || carry >= 0xFFFFFFFFull) ? 1u : 0u;
     }
 }
 
