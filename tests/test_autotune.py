@@ -23,16 +23,21 @@ def test_modes_and_cache_file(tmp_path):
     path = tmp_path / "shapes.json"
     path.write_text('{\n'
                     '  "t12-w17-k1-m1": {"surf_blocks_per_sm": 16, "surf_batch": 8, "merge_blocks_per_sm": 32, '
-                    '"emit_blocks_per_sm": 8, "toggle_blocks_per_sm": 6},\n'
+                    '"emit_blocks_per_sm": 8, "toggle_blocks_per_sm": 6, "surf_queue": 1, "toggle_queue": 1},\n'
                     '  "t13-w17-k1-m1": {"surf_blocks_per_sm": 7, "surf_batch": 8, "merge_blocks_per_sm": 32, '
+                    '"emit_blocks_per_sm": 8, "toggle_blocks_per_sm": 6, "surf_queue": 0, "toggle_queue": 0},\n'
+                    '  "t14-w17-k1-m1": {"surf_blocks_per_sm": 16, "surf_batch": 8, "merge_blocks_per_sm": 32, '
                     '"emit_blocks_per_sm": 8, "toggle_blocks_per_sm": 6}\n'
                     '}\n')
     _lib.set_autotune(2, str(path))
     n, text = _lib.autotune_state()
-    assert n == 1   # the second entry names a shape that is not a candidate
+    # The second entry names a shape that is not a candidate; the third
+    # lacks the work-distribution fields.
+    assert n == 1
     shapes = json.loads(text)
     assert shapes == {"t12-w17-k1-m1": {"surf_blocks_per_sm": 16, "surf_batch": 8, "merge_blocks_per_sm": 32,
-                                        "emit_blocks_per_sm": 8, "toggle_blocks_per_sm": 6}}
+                                        "emit_blocks_per_sm": 8, "toggle_blocks_per_sm": 6, "surf_queue": 1,
+                                        "toggle_queue": 1}}
     with pytest.raises(_lib.VxbError, match="EINVAL"):
         _lib.set_autotune(3)
     _lib.set_autotune(0)

@@ -71,9 +71,11 @@ void launch_scan(const uint32_t* in, uint32_t* offsets, uint32_t n, uint32_t* bl
 // the `fill` arena, then the row prefix XOR over all rows of the batch.
 void launch_solid_count(const Batch& b, uint32_t nWork, uint32_t* counts, cudaStream_t s, uint32_t* launches);
 // blocksPerSm: launch shape (the autotuner's choice; results do not depend
-// on it), here and in the launchers below that take one.
+// on it), here and in the launchers below that take one.  queue: NULL for
+// a fixed grid-stride order, else a device word the launcher zeroes and the
+// kernel's persistent blocks take batches of work from.
 void launch_solid_toggle(const Batch& b, uint32_t nWork, const uint32_t* offsets, const uint32_t* total,
-                         uint32_t* fill, uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches);
+                         uint32_t* fill, uint32_t blocksPerSm, uint32_t* queue, cudaStream_t s, uint32_t* launches);
 void launch_row_fill(const Batch& b, uint64_t nRows, uint32_t* fill, cudaStream_t s, uint32_t* launches);
 
 // ---- Surface voxelization: src/voxelizer.cu:2358-2989, 3040-4201 ----
@@ -95,12 +97,14 @@ void launch_surface_prepare(const Batch& b, uint32_t nWork, uint32_t* codes, uin
 // entries), one thread per column.  mode 0: set bits in the `surf` arena and
 // append (bit position << 24 | key) to `list` (entries past listCap are
 // counted, not stored); mode 1: merge every hit's key at its rank (needs
-// complete bits and `ranks`).  wide: 64-bit keys (PartialNode).
+// complete bits and `ranks`).  wide: 64-bit keys (PartialNode).  kind: the
+// node type, whose instantiation of the class kernels the arithmetic
+// follows.  queue: as for launch_solid_toggle, per warp.
 void launch_surface_work(int kind, int mode, int wide, const Batch& b, const void* recs, const void* ovl,
                          const uint32_t* offsets, uint32_t nWork, const uint32_t* total, const uint32_t* buckets,
                          uint32_t* surf, const uint32_t* ranks, void* keys, uint32_t keysCap,
                          unsigned long long* list, uint32_t* listCount, uint32_t listCap, uint32_t blocksPerSm,
-                         uint32_t batch, cudaStream_t s, uint32_t* launches);
+                         uint32_t batch, uint32_t* queue, cudaStream_t s, uint32_t* launches);
 // Exclusive popcount prefix over `words` surface words; *total = surface voxels.
 void launch_surface_rank(const uint32_t* bits, uint64_t words, uint32_t* ranks, uint32_t* tileSums, uint32_t* total,
                          cudaStream_t s, uint32_t* launches);

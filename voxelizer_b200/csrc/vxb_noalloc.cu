@@ -274,7 +274,7 @@ extern "C" vxb_status vxb_voxelize_bits_noalloc(const float* dev_vertices, const
     launches += 2;
     vxb::launch_solid_count(b, n_triangles, counts, s, &launches);
     vxb::launch_scan(counts, offsets, n_triangles, tiles, status, status + 1, s, &launches);
-    vxb::launch_solid_toggle(b, n_triangles, offsets, status, grid, 3, s, &launches);
+    vxb::launch_solid_toggle(b, n_triangles, offsets, status, grid, 3, nullptr, s, &launches);
     vxb::launch_row_fill(b, tab.rowBase[1], grid, s, &launches);
     e = cudaGetLastError();
     if (e != cudaSuccess) return failf(VXB_ECUDA, "%s", cudaGetErrorString(e));

@@ -19,7 +19,7 @@ namespace {
 
 // Slots of the status buffer; pruning flags follow at kFlags.
 enum : int { kSolidTotal = 0, kSolidOverflow = 1, kSurfTotal = 2, kSurfOverflow = 3, kHitCount = 4,
-             kSurfaceVoxels = 5, kFlags = 8 };
+             kSurfaceVoxels = 5, kSurfQueue = 6, kToggleQueue = 7, kFlags = 8 };
 
 const uint32_t kNodeBytes[5] = {1, 2, 8, 2, 4};
 
@@ -342,8 +342,8 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
     launch_scan(counts.as<uint32_t>(), offsets.as<uint32_t>(), nWork_, tileSums.as<uint32_t>(), st + kSolidTotal,
                 st + kSolidOverflow, s, &launches);
     tuneMark(kKnobToggle, false, s);
-    launch_solid_toggle(b, nWork_, offsets.as<uint32_t>(), st + kSolidTotal, fillP, shape.toggleBlocksPerSm, s,
-                        &launches);
+    launch_solid_toggle(b, nWork_, offsets.as<uint32_t>(), st + kSolidTotal, fillP, shape.toggleBlocksPerSm,
+                        shape.toggleQueue ? st + kToggleQueue : nullptr, s, &launches);
     tuneMark(kKnobToggle, true, s);
     launch_row_fill(b, totalRows_, fillP, s, &launches);
     mark(0, true);
@@ -369,9 +369,10 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
         mark(5, false);
         tuneMark(kKnobSurface, false, s);
         launch_surface_work(nodeKind_, 0, wide_ ? 1 : 0, b, recs.p, ovl.p, offsets.as<uint32_t>(), nWork_,
-                            st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_,
-                            hitList.as<unsigned long long>(), st + kHitCount, listCap_, shape.surfBlocksPerSm,
-                            shape.surfBatch, s, &launches);
+                            st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(),
+                            keys.p, keysCap_, hitList.as<unsigned long long>(), st + kHitCount, listCap_,
+                            shape.surfBlocksPerSm, shape.surfBatch, shape.surfQueue ? st + kSurfQueue : nullptr, s,
+                            &launches);
         tuneMark(kKnobSurface, true, s);
         mark(5, true);
         launch_surface_rank(surf.as<uint32_t>(), totalWords_, ranks.as<uint32_t>(), rankTiles.as<uint32_t>(),
@@ -422,7 +423,8 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
         else
             launch_surface_work(nodeKind_, 1, 1, b, recs.p, ovl.p, offsets.as<uint32_t>(), nWork_,
                                 st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(),
-                                keys.p, keysCap_, nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch, s, &launches);
+                                keys.p, keysCap_, nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch,
+                                shape.surfQueue ? st + kSurfQueue : nullptr, s, &launches);
         tuneMark(kKnobMerge, true, s);
         mark(4, true);
     }
@@ -573,7 +575,8 @@ int Pipeline::finish(cudaStream_t s) {
             launch_surface_keys_zero(keys.p, st + kSurfaceVoxels, keysCap_, wide_ ? 1 : 0, s, &launches);
             launch_surface_work(nodeKind_, 1, wide_ ? 1 : 0, b, recs.p, ovl.p, offsets.as<uint32_t>(), nWork_,
                                 st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(),
-                                keys.p, keysCap_, nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch, s, &launches);
+                                keys.p, keysCap_, nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch,
+                                shape.surfQueue ? st + kSurfQueue : nullptr, s, &launches);
             reemit = true;
         }
     }

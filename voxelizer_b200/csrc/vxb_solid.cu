@@ -215,12 +215,20 @@ __device__ __forceinline__ void solidCandidate(const SolidStage& st, const Batch
 __global__ void __launch_bounds__(kBlock, 3) solidToggleKernel(Batch b, uint32_t nWork,
                                                                const uint32_t* __restrict__ offsets,
                                                                const uint32_t* __restrict__ totalPtr,
-                                                               uint32_t* __restrict__ fill) {
+                                                               uint32_t* __restrict__ fill, uint32_t* queue) {
     __shared__ SolidStage stage[kSlots];
     __shared__ uint32_t stOff[kSlots + 1];
-    __shared__ uint32_t tFirst, nStage;
+    __shared__ uint32_t tFirst, nStage, nextBase;
     const uint32_t total = *totalPtr;
-    for (uint32_t base = blockIdx.x * kBlock; base < total; base += gridDim.x * kBlock) {
+    // Batches of kBlock candidates in a fixed grid-stride order, or
+    // (queue != NULL) taken from a device work queue, one atomic per batch.
+    uint32_t base = blockIdx.x * kBlock;
+    if (queue) {
+        if (threadIdx.x == 0) nextBase = atomicAdd(queue, kBlock);
+        __syncthreads();
+        base = nextBase;
+    }
+    while (base < total) {
         const uint32_t last = min(base + kBlock, total) - 1;
         if (threadIdx.x == 0) {
             const uint32_t t0 = findOwner(offsets, nWork, base);
@@ -253,7 +261,9 @@ __global__ void __launch_bounds__(kBlock, 3) solidToggleKernel(Batch b, uint32_t
                 solidCandidate(st, b, item - __ldg(offsets + wt), fill);
             }
         }
+        if (queue && threadIdx.x == 0) nextBase = atomicAdd(queue, kBlock);
         __syncthreads();
+        base = queue ? nextBase : base + gridDim.x * kBlock;
     }
 }
 
@@ -288,8 +298,9 @@ void launch_solid_count(const Batch& b, uint32_t nWork, uint32_t* counts, cudaSt
 }
 
 void launch_solid_toggle(const Batch& b, uint32_t nWork, const uint32_t* offsets, const uint32_t* total,
-                         uint32_t* fill, uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches) {
-    solidToggleKernel<<<148u * blocksPerSm, kBlock, 0, s>>>(b, nWork, offsets, total, fill);
+                         uint32_t* fill, uint32_t blocksPerSm, uint32_t* queue, cudaStream_t s, uint32_t* launches) {
+    if (queue) cudaMemsetAsync(queue, 0, sizeof(uint32_t), s);
+    solidToggleKernel<<<148u * blocksPerSm, kBlock, 0, s>>>(b, nWork, offsets, total, fill, queue);
     *launches += 1;
 }
 

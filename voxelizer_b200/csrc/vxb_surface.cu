@@ -578,7 +578,8 @@ __global__ void __launch_bounds__(kBlock) surfaceWorkKernel(Sink sink, Batch b, 
                                                             const SurfOvl* __restrict__ ovl,
                                                             const uint32_t* __restrict__ off, uint32_t n,
                                                             const uint32_t* __restrict__ totalPtr,
-                                                            const uint32_t* __restrict__ bucketCount) {
+                                                            const uint32_t* __restrict__ bucketCount,
+                                                            uint32_t* queue) {
     __shared__ unsigned long long stageBuf[kBlock / 32][kStageHits];
     __shared__ uint32_t stageCount[kBlock / 32];
     __shared__ uint32_t bucketEnd[kSurfaceBuckets];
@@ -599,7 +600,16 @@ __global__ void __launch_bounds__(kBlock) surfaceWorkKernel(Sink sink, Batch b, 
     const uint32_t batches = (chunks + kBatch - 1) / kBatch;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nWarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t bt = warp; bt < batches; bt += nWarps) {
+    // Batches in a fixed grid-stride order, or (queue != NULL) taken from a
+    // device work queue, one atomic per batch, so that warps that drew cheap
+    // batches keep working while others finish expensive ones.
+    auto nextBatch = [&](uint32_t cur) {
+        if (!queue) return cur + nWarps;
+        uint32_t v = 0;
+        if (lane == 0) v = atomicAdd(queue, 1u);
+        return __shfl_sync(kFull, v, 0);
+    };
+    for (uint32_t bt = queue ? nextBatch(0) : warp; bt < batches; bt = nextBatch(bt)) {
         const uint32_t c1 = min((bt + 1) * kBatch, chunks);
         uint32_t t0 = warpFindOwner(off, n, bt * kBatch * 32u, lane);
         for (uint32_t c = bt * kBatch; c < c1; ++c) {
@@ -783,18 +793,20 @@ void launch_surface_prepare(const Batch& b, uint32_t nWork, uint32_t* codes, uin
 template <int K>
 static void launchSurfaceWorkKind(uint32_t batch, uint32_t grid, const Sink& sink, const Batch& b, const SurfRec* R,
                                   const SurfOvl* O, const uint32_t* offsets, uint32_t nWork, const uint32_t* total,
-                                  const uint32_t* buckets, cudaStream_t s) {
-    if (batch == 8) surfaceWorkKernel<8, K><<<grid, kBlock, 0, s>>>(sink, b, R, O, offsets, nWork, total, buckets);
+                                  const uint32_t* buckets, uint32_t* queue, cudaStream_t s) {
+    if (batch == 8)
+        surfaceWorkKernel<8, K><<<grid, kBlock, 0, s>>>(sink, b, R, O, offsets, nWork, total, buckets, queue);
     else if (batch == 32)
-        surfaceWorkKernel<32, K><<<grid, kBlock, 0, s>>>(sink, b, R, O, offsets, nWork, total, buckets);
-    else surfaceWorkKernel<16, K><<<grid, kBlock, 0, s>>>(sink, b, R, O, offsets, nWork, total, buckets);
+        surfaceWorkKernel<32, K><<<grid, kBlock, 0, s>>>(sink, b, R, O, offsets, nWork, total, buckets, queue);
+    else surfaceWorkKernel<16, K><<<grid, kBlock, 0, s>>>(sink, b, R, O, offsets, nWork, total, buckets, queue);
 }
 
 void launch_surface_work(int kind, int mode, int wide, const Batch& b, const void* recs, const void* ovl,
                          const uint32_t* offsets, uint32_t nWork, const uint32_t* total, const uint32_t* buckets,
                          uint32_t* surf, const uint32_t* ranks, void* keys, uint32_t keysCap,
                          unsigned long long* list, uint32_t* listCount, uint32_t listCap, uint32_t blocksPerSm,
-                         uint32_t batch, cudaStream_t s, uint32_t* launches) {
+                         uint32_t batch, uint32_t* queue, cudaStream_t s, uint32_t* launches) {
+    if (queue) cudaMemsetAsync(queue, 0, sizeof(uint32_t), s);
     Sink sink;
     sink.bits = surf;
     sink.wordRank = ranks;
@@ -809,16 +821,16 @@ void launch_surface_work(int kind, int mode, int wide, const Batch& b, const voi
     const SurfRec* R = static_cast<const SurfRec*>(recs);
     const SurfOvl* O = static_cast<const SurfOvl*>(ovl);
     switch (kind) {
-    case kShort: launchSurfaceWorkKind<kShort>(batch, grid, sink, b, R, O, offsets, nWork, total, buckets, s); break;
-    case kLong: launchSurfaceWorkKind<kLong>(batch, grid, sink, b, R, O, offsets, nWork, total, buckets, s); break;
+    case kShort: launchSurfaceWorkKind<kShort>(batch, grid, sink, b, R, O, offsets, nWork, total, buckets, queue, s); break;
+    case kLong: launchSurfaceWorkKind<kLong>(batch, grid, sink, b, R, O, offsets, nWork, total, buckets, queue, s); break;
     case kPartial:
-        launchSurfaceWorkKind<kPartial>(batch, grid, sink, b, R, O, offsets, nWork, total, buckets, s);
+        launchSurfaceWorkKind<kPartial>(batch, grid, sink, b, R, O, offsets, nWork, total, buckets, queue, s);
         break;
     case kShortFcc:
-        launchSurfaceWorkKind<kShortFcc>(batch, grid, sink, b, R, O, offsets, nWork, total, buckets, s);
+        launchSurfaceWorkKind<kShortFcc>(batch, grid, sink, b, R, O, offsets, nWork, total, buckets, queue, s);
         break;
     default:
-        launchSurfaceWorkKind<kLongFcc>(batch, grid, sink, b, R, O, offsets, nWork, total, buckets, s);
+        launchSurfaceWorkKind<kLongFcc>(batch, grid, sink, b, R, O, offsets, nWork, total, buckets, queue, s);
         break;
     }
     *launches += 1;

@@ -16,11 +16,13 @@ namespace vxb {
 namespace {
 
 // Candidate k of every knob; candidate 0 is the untuned shape.
-const uint32_t kSurfBlocks[kTuneCandidates] = {16, 8, 4};
-const uint32_t kSurfBatch[kTuneCandidates] = {8, 16, 32};
+const uint32_t kSurfBlocks[kTuneCandidates] = {16, 16, 8};
+const uint32_t kSurfBatch[kTuneCandidates] = {8, 8, 16};
+const uint32_t kSurfQueue[kTuneCandidates] = {0, 1, 1};
 const uint32_t kMerge[kTuneCandidates] = {8, 16, 32};
 const uint32_t kEmit[kTuneCandidates] = {16, 8, 32};
-const uint32_t kToggle[kTuneCandidates] = {3, 6, 2};
+const uint32_t kToggle[kTuneCandidates] = {3, 3, 6};
+const uint32_t kToggleQueue[kTuneCandidates] = {0, 1, 1};
 
 LaunchShape candidate(int k) {
     LaunchShape s;
@@ -29,6 +31,8 @@ LaunchShape candidate(int k) {
     s.mergeBlocksPerSm = kMerge[k];
     s.emitBlocksPerSm = kEmit[k];
     s.toggleBlocksPerSm = kToggle[k];
+    s.surfQueue = kSurfQueue[k];
+    s.toggleQueue = kToggleQueue[k];
     return s;
 }
 
@@ -52,12 +56,14 @@ State& state() {
     return *s;
 }
 
-const char* const kFields[5] = {"surf_blocks_per_sm", "surf_batch", "merge_blocks_per_sm", "emit_blocks_per_sm",
-                                "toggle_blocks_per_sm"};
+constexpr int kFieldCount = 7;
+const char* const kFields[kFieldCount] = {"surf_blocks_per_sm", "surf_batch", "merge_blocks_per_sm",
+                                          "emit_blocks_per_sm", "toggle_blocks_per_sm", "surf_queue",
+                                          "toggle_queue"};
 
 uint32_t* field(LaunchShape& s, int i) {
-    uint32_t* f[5] = {&s.surfBlocksPerSm, &s.surfBatch, &s.mergeBlocksPerSm, &s.emitBlocksPerSm,
-                      &s.toggleBlocksPerSm};
+    uint32_t* f[kFieldCount] = {&s.surfBlocksPerSm, &s.surfBatch,   &s.mergeBlocksPerSm, &s.emitBlocksPerSm,
+                                &s.toggleBlocksPerSm, &s.surfQueue, &s.toggleQueue};
     return f[i];
 }
 
@@ -68,7 +74,8 @@ bool validShape(const LaunchShape& s) {
         return false;
     };
     return in(s.surfBlocksPerSm, kSurfBlocks) && in(s.surfBatch, kSurfBatch) && in(s.mergeBlocksPerSm, kMerge) &&
-           in(s.emitBlocksPerSm, kEmit) && in(s.toggleBlocksPerSm, kToggle);
+           in(s.emitBlocksPerSm, kEmit) && in(s.toggleBlocksPerSm, kToggle) && in(s.surfQueue, kSurfQueue) &&
+           in(s.toggleQueue, kToggleQueue);
 }
 
 std::string jsonLocked(const State& st) {
@@ -77,11 +84,14 @@ std::string jsonLocked(const State& st) {
     for (const auto& kv : st.buckets) {
         if (!kv.second.settled) continue;
         LaunchShape s = kv.second.best;
-        char line[512];
-        snprintf(line, sizeof(line), "%s  \"%s\": {\"%s\": %u, \"%s\": %u, \"%s\": %u, \"%s\": %u, \"%s\": %u}",
-                 first ? "" : ",\n", kv.first.c_str(), kFields[0], *field(s, 0), kFields[1], *field(s, 1), kFields[2],
-                 *field(s, 2), kFields[3], *field(s, 3), kFields[4], *field(s, 4));
-        out += line;
+        out += first ? "  \"" : ",\n  \"";
+        out += kv.first + "\": {";
+        for (int i = 0; i < kFieldCount; ++i) {
+            char item[96];
+            snprintf(item, sizeof(item), "%s\"%s\": %u", i ? ", " : "", kFields[i], *field(s, i));
+            out += item;
+        }
+        out += "}";
         first = false;
     }
     out += "\n}\n";
@@ -112,7 +122,7 @@ void loadLocked(State& st) {
         const std::string key(q0 + 1, q1);
         LaunchShape s;
         bool ok = true;
-        for (int i = 0; i < 5 && ok; ++i) {
+        for (int i = 0; i < kFieldCount && ok; ++i) {
             const std::string name = std::string("\"") + kFields[i] + "\":";
             const char* p = strstr(q1, name.c_str());
             unsigned v = 0;
@@ -187,10 +197,14 @@ void tuneReport(const std::string& bucket, int trial, const float* ms) {
         case kKnobSurface:
             best.surfBlocksPerSm = c.surfBlocksPerSm;
             best.surfBatch = c.surfBatch;
+            best.surfQueue = c.surfQueue;
             break;
         case kKnobMerge: best.mergeBlocksPerSm = c.mergeBlocksPerSm; break;
         case kKnobEmit: best.emitBlocksPerSm = c.emitBlocksPerSm; break;
-        default: best.toggleBlocksPerSm = c.toggleBlocksPerSm; break;
+        default:
+            best.toggleBlocksPerSm = c.toggleBlocksPerSm;
+            best.toggleQueue = c.toggleQueue;
+            break;
         }
     }
     e.best = best;

@@ -20,6 +20,11 @@ struct LaunchShape {
     uint32_t mergeBlocksPerSm = 8;   // mergeKeysKernel
     uint32_t emitBlocksPerSm = 16;   // emitNarrowKernel
     uint32_t toggleBlocksPerSm = 3;  // solidToggleKernel
+    // Work distribution of surfaceWorkKernel / solidToggleKernel: 0 a fixed
+    // grid-stride order, 1 a device work queue (persistent warps / blocks
+    // take the next batch of items with one atomic each).
+    uint32_t surfQueue = 0;
+    uint32_t toggleQueue = 0;
 };
 
 // The tuned kernels, in the order of their timing events.
