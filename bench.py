@@ -14,11 +14,12 @@ value: Gvoxels/s of node grid, device resident (mesh already on the GPU,
 e2e: the same metric through the reference-facing C ABI with host buffers:
   each step constructs the voxelizer from pinned host arrays, uploads the
   mesh, voxelizes and copies the node grid back into pinned host memory.
---impl reference: the reference's own implementation of the path.  It has
-  no CPU code: its kernels are CUDA (src/voxelizer.cu), built from its
-  sources into oracle/_ref/ and run on cuda:0 with host arrays in and out,
-  on the full workload.  Where that library or a GPU is missing, the CPU
-  restatement (oracle/) runs on all host cores on a bounded sample.
+--impl reference: the reference's own implementation of the path through
+  its public API (Voxelizer<LongNode>::voxelizeToNodesToRAM, src/host_side.cpp
+  with its CUDA kernels src/voxelizer.cu), built from its sources into
+  oracle/_ref/ and run on cuda:0 with host arrays in and out, on the full
+  workload.  It has no CPU code; where that library or a GPU is missing, the
+  CPU restatement (oracle/) runs on all host cores on a bounded sample.
 Multi-GPU: replicas only (the path does not shard); under torchrun every
 rank voxelizes its own copy and value sums the voxels of all ranks over the
 slowest rank's time.
@@ -262,10 +263,52 @@ def run_reference_cuda(args, world, ref):
     print(json.dumps(line), flush=True)
 
 
+def run_reference_api(args, world):
+    """Full workload through the reference's own public API on cuda:0:
+    vox::Voxelizer<LongNode>::voxelizeToNodesToRAM(1024) of its
+    src/host_side.cpp and src/voxelizer.cu, built from its sources
+    (oracle/_ref/libvoxhost.so).  Host arrays in, node grid back in host
+    memory, wall clock per call (the call allocates, uploads, computes and
+    copies back)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_host as RH
+    from voxelizer_b200 import scenes
+
+    mesh = scenes.room_scene()
+    out, dims, _ = RH.voxelize(mesh, 1, 1, MAX_DIM)
+    n_nodes = dims[0] * dims[1] * dims[2]
+    times = []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        RH.voxelize(mesh, 1, 1, MAX_DIM, out=out)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            times.append(dt)
+    t = sum(times)
+    value = n_nodes * len(times) / t / 1e9
+    sample = (f"full workload, {dims[0]}x{dims[1]}x{dims[2]} nodes per step: the reference's own public API "
+              f"(Voxelizer<LongNode>::voxelizeToNodesToRAM of src/host_side.cpp with src/voxelizer.cu, built from "
+              f"its sources for sm_100a) on cuda:0, host arrays in and out, wall clock per call")
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t / len(times), 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32+u32",
+            "data": "synthetic (seeded room scene)", "device": "cuda:0",
+            "config": dict(CONFIG), "sample": sample,
+            "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": 1, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, world, rank):
-    """The reference's implementation of the path: its CUDA build where it
-    was compiled, else its CPU restatement (oracle/) on all host cores."""
+    """The reference's implementation of the path: its own public API where
+    it was built from its sources, else its kernels behind the restated
+    host flow of oracle/ref_driver.cu, else its CPU restatement (oracle/) on
+    all host cores."""
     if rank != 0:
+        return
+    if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libvoxhost.so")) and _reference_cuda() is not None:
+        run_reference_api(args, world)
         return
     ref = _reference_cuda()
     if ref is not None:

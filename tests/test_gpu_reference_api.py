@@ -1,0 +1,59 @@
+"""The CUDA path against the reference's own public API run on the same GPU.
+
+oracle/_ref/libvoxhost.so is the reference's src/host_side.cpp and
+src/voxelizer.cu compiled from its sources (oracle/Makefile, target
+refhost); ref_host.py calls its vox::Voxelizer<Node>::voxelizeToNodesToRAM
+and voxelizeToRAM unchanged, so these comparisons need no restatement of its
+host flow.  Rules as in test_gpu_parity.py: bit arrays and boundary ids
+identical; materials identical wherever the reference's surface stores do
+not race (the oracle flags those nodes).
+"""
+
+import numpy as np
+import pytest
+
+import cases as C
+import oracle as O
+import ref_host as RH
+from helpers import CONFLICT_MAT, PARTIAL, bid_of, describe_diff, mat_of, masked
+from voxelizer_b200.api import Voxelizer
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not RH.available(), reason="oracle/_ref/libvoxhost.so not built")]
+
+CASES = [
+    # (mesh, node type, node grid?, size, vox split, mat split)
+    ("ico4", 1, 1, 96, (1024, 512, 512), (512, 512, 512)),
+    ("torus", 0, 1, 1.0 / 100.0, (1024, 40, 48), (512, 512, 512)),
+    ("ico3_mixed", 2, 1, 64, (1024, 512, 512), (512, 512, 512)),
+    ("ico4", 3, 1, C.FCC_A, (1024, 512, 512), (512, 512, 512)),
+    ("stress", 1, 1, 1.0 / 128.0, (96, 40, 40), (40, 40, 40)),
+    ("room_lite", 1, 0, 160, (1024, 512, 512), (512, 512, 512)),
+]
+
+
+@pytest.mark.parametrize("mesh_name,nt,nodes,size,vox,mat", CASES)
+def test_cuda_matches_reference_public_api(mesh_name, nt, nodes, size, vox, mat):
+    import torch
+
+    assert torch.cuda.is_available()
+    m = C.mesh(mesh_name)
+    want, dims, _ = RH.voxelize(m, nt, nodes, size, vox, mat, materials=bool(nodes))
+    with Voxelizer(m.vertices, m.indices, node_type=nt) as v:
+        if nodes:
+            v.setMaterials(m.materials, m.n_materials)
+            got, info = v.voxelizeToNodesToRAM(size, vox, mat)
+        else:
+            got, info = v.voxelizeToRAM(size, vox)
+    assert tuple(info.dims) == dims
+    if not nodes:
+        assert np.array_equal(got, want), describe_diff(got, want)
+        return
+    got, want = masked(nt, 1, got), masked(nt, 1, want)
+    assert np.array_equal(bid_of(nt, got), bid_of(nt, want)), describe_diff(bid_of(nt, got), bid_of(nt, want), dims)
+    _, _, conf = O.voxelize(m, nt, 1, 1, size, vox, mat, want_conflicts=True)
+    keep = (conf & CONFLICT_MAT) == 0
+    assert np.array_equal(mat_of(nt, got)[keep], mat_of(nt, want)[keep])
+    if nt == PARTIAL:
+        low = np.uint64(0xFFFFFFFF)
+        assert np.array_equal((got & low)[keep], (want & low)[keep])

@@ -1,7 +1,9 @@
 """CPU-only checks of the host side: the C ABI library loads and exports
 every symbol include/vxb.h declares, planning (dimensions, padding, x
-rounding) matches the oracle and the reference's golden dims, and argument
-errors surface as the reference's errors.  Nothing here touches a GPU."""
+rounding) matches the oracle, the reference's golden dims and the
+reference's own sizing code (built from its sources into oracle/_ref and
+run here on the CPU), and argument errors surface as the reference's errors.
+Nothing here touches a GPU."""
 
 import json
 import os
@@ -12,8 +14,10 @@ import pytest
 
 import cases as C
 import oracle as O
+import ref_host as RH
 from voxelizer_b200 import _lib
 from voxelizer_b200.api import Voxelizer
+from voxelizer_b200.scenes import Mesh
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 INDEX = json.load(open(os.path.join(ROOT, "tests", "golden", "index.json")))
@@ -109,5 +113,53 @@ def test_array_dimensions_match_plan():
             # FCC lattices with x and z doubled (src/host_side.cpp:3333-3371)
             f = 2 if nt >= 3 else 1
             for size in (1.0 / 100.0, 90):
+                if f == 2 and not isinstance(size, float):
+                    continue   # FCC by maxDimension: the reference's own quirk, checked against its code below
                 t = O.plan(m, 0, 1, size, rotate_x=True).dims
                 assert v.getArrayDimensions(size, 1024, True) == (f * t[1], t[0], f * t[2])
+
+
+@pytest.mark.skipif(not RH.available(), reason="oracle/_ref/libvoxhost.so not built (needs the reference's sources)")
+@pytest.mark.parametrize("seed", range(4))
+def test_sizing_matches_the_reference_code(seed):
+    """getArrayDimensions of this library against the reference's own
+    getArrayDimensions (src/host_side.cpp:3329-3475, compiled from its
+    sources into oracle/_ref and run on the CPU) over random boxes, sizes by
+    maxDimension and by cube length, x pass lengths, all node types and both
+    slice orientations."""
+    rng = np.random.default_rng(100 + seed)
+    checked = 0
+    for _ in range(30):
+        ext = rng.uniform(0.05, 3.0, size=3) * rng.choice([1.0, 1.0, 0.01], size=3)
+        lo = rng.uniform(-2.0, 2.0, size=3)
+        v = (lo + rng.uniform(0.0, 1.0, size=(12, 3)) * ext).astype(np.float32)
+        v[0], v[1] = lo, lo + ext          # the box corners themselves
+        f = rng.integers(0, 12, size=(8, 3)).astype(np.uint32)
+        m = Mesh(v, f, None, 0)
+        nt = int(rng.integers(0, 5))
+        size = float(rng.uniform(0.004, 0.05)) * float(ext.max()) if rng.random() < 0.5 else int(
+            rng.integers(8, 900))
+        max_x = int(rng.choice([64, 256, 1024]))
+        for slice_x in (False, True):
+            try:
+                want = RH.array_dimensions(m, nt, size, max_x, slice_x)
+            except RuntimeError:
+                continue
+            with Voxelizer(m.vertices, m.indices, node_type=nt) as vx:
+                try:
+                    got = vx.getArrayDimensions(size, max_x, slice_x)
+                except _lib.VxbError:
+                    continue   # refused here (x pass above 1024 voxels, FCC by maxDimension, ...)
+            assert got == want, (nt, size, max_x, slice_x)
+            checked += 1
+    assert checked > 20
+
+
+@pytest.mark.skipif(not RH.available(), reason="oracle/_ref/libvoxhost.so not built (needs the reference's sources)")
+@pytest.mark.parametrize("name", sorted(n for n in RAN if not C.BY_NAME[n].get("space")))
+def test_golden_dims_are_the_reference_codes(name):
+    """Every golden case's array dimensions equal what the reference's own
+    getArrayDimensions gives for its mesh and size."""
+    c = C.BY_NAME[name]
+    m = C.mesh(c["mesh"])
+    assert RH.array_dimensions(m, c["node_type"], c["size"], c["vox"][0]) == tuple(INDEX[name]["dims"])

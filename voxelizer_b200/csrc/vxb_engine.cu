@@ -632,6 +632,26 @@ vxb_status vxb_get_array_dimensions(vxb_voxelizer* v, int by_cube_length, uint32
         dims->x = f * p.alloc[1];
         dims->y = p.alloc[0];
         dims->z = f * p.alloc[2];
+        if (f == 2 && !by_cube_length) {
+            // The maxDimension overload (src/host_side.cpp:3329-3369) turns
+            // the corners of the undoubled grid back with unRotateCoords'
+            // FCC branch (3293-3309) and doubles x and z afterwards.
+            const uint32_t X = p.alloc[0], Y = p.alloc[1], Z = p.alloc[2];
+            auto unrot = [&](uint32_t x, uint32_t y, uint32_t z, uint32_t out[3]) {
+                out[0] = 2 * y + (x + z + 1) % 2;
+                out[1] = X / 2 - 1 - x / 2;
+                out[2] = z;
+            };
+            uint32_t a[3], b[3];
+            unrot(0, 0, 0, a);
+            unrot(X - 1, Y - 1, Z - 1, b);
+            const uint32_t ext[3] = {std::max(a[0], b[0]) - std::min(a[0], b[0]) + 1,
+                                     std::max(a[1], b[1]) - std::min(a[1], b[1]) + 1,
+                                     std::max(a[2], b[2]) - std::min(a[2], b[2]) + 1};
+            dims->x = 2 * ext[0];
+            dims->y = ext[1];
+            dims->z = 2 * ext[2];
+        }
         return VXB_OK;
     }
     vxb_request r;
