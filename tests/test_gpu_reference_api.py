@@ -46,6 +46,7 @@ def test_cuda_matches_reference_public_api(mesh_name, nt, nodes, mats, size, vox
     with Voxelizer(m.vertices, m.indices, node_type=nt) as v:
         if mats:
             v.setMaterials(m.materials, m.n_materials)
+        if nodes:
             got, info = v.voxelizeToNodesToRAM(size, vox, mat)
         else:
             got, info = v.voxelizeToRAM(size, vox)

@@ -292,6 +292,15 @@ int Pipeline::prepare(const std::vector<MeshJob>& jobs, cudaStream_t s) {
     listCap_ = 0;
     keysCap_ = 0;
     if (anyMaterials_) {
+        if (!side_) {
+            VXB_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+            VXB_CUDA(cudaEventCreateWithFlags(&evFork_, cudaEventDisableTiming));
+            VXB_CUDA(cudaEventCreateWithFlags(&evSurfBits_, cudaEventDisableTiming));
+            VXB_CUDA(cudaEventCreateWithFlags(&evSurfDone_, cudaEventDisableTiming));
+        }
+        if ((rc = sCounts.ensure(4 * ((size_t)nWork_ + 2)))) return rc;
+        if ((rc = sOffsets.ensure(4 * ((size_t)nWork_ + 2)))) return rc;
+        if ((rc = sTileSums.ensure(4 * ((size_t)nWork_ / 4096 + 2)))) return rc;
         if ((rc = surf.ensure(wordBytes))) return rc;
         if ((rc = ranks.ensure(wordBytes))) return rc;
         if ((rc = rankTiles.ensure(4 * ((size_t)totalWords_ / 2048 + 2)))) return rc;
@@ -335,6 +344,52 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
     bucket_ = tuneBucket(nWork_, totalWords_, nodeKind_, anyMaterials_);
     shape = tunePick(bucket_, &trial_, cap == cudaStreamCaptureStatusNone);
     for (bool& u : tuneUsed_) u = false;
+    // Surface voxelization, hit list and surface ranks on the side stream,
+    // beside the solid pass (they share no buffer).
+    cudaStream_t ss = s;
+    if (anyMaterials_) {
+        ss = side_;
+        VXB_CUDA(cudaEventRecord(evFork_, s));
+        VXB_CUDA(cudaStreamWaitEvent(ss, evFork_, 0));
+        if (timer) timer->mark(1, false, ss);
+        VXB_CUDA(cudaMemsetAsync(surf.p, 0, 4 * (size_t)totalWords_, ss));
+        VXB_CUDA(cudaMemsetAsync(buckets.p, 0, 4 * 2 * kSurfaceBuckets, ss));
+        VXB_CUDA(cudaMemsetAsync(sCounts.p, 0, 4 * ((size_t)nWork_ + 1), ss));
+        VXB_CUDA(cudaMemsetAsync(st + kHitCount, 0, 4, ss));
+        launch_surface_prepare(b, nWork_, codes.as<uint32_t>(), unitCounts.as<uint32_t>(), buckets.as<uint32_t>(),
+                               perm.as<uint32_t>(), sCounts.as<uint32_t>(), recs.p, ovl.p, ss, &launches);
+        launch_scan(sCounts.as<uint32_t>(), sOffsets.as<uint32_t>(), nWork_, sTileSums.as<uint32_t>(),
+                    st + kSurfTotal, st + kSurfOverflow, ss, &launches);
+        if (timer) timer->mark(5, false, ss);
+        tuneMark(kKnobSurface, false, ss);
+        launch_surface_work(nodeKind_, 0, wide_ ? 1 : 0, b, recs.p, ovl.p, sOffsets.as<uint32_t>(), nWork_,
+                            st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(),
+                            keys.p, keysCap_, hitList.as<unsigned long long>(), st + kHitCount, listCap_,
+                            shape.surfBlocksPerSm, shape.surfBatch, shape.surfQueue ? st + kSurfQueue : nullptr, ss,
+                            &launches);
+        tuneMark(kKnobSurface, true, ss);
+        if (timer) timer->mark(5, true, ss);
+        VXB_CUDA(cudaEventRecord(evSurfBits_, ss));
+        launch_surface_rank(surf.as<uint32_t>(), totalWords_, ranks.as<uint32_t>(), rankTiles.as<uint32_t>(),
+                            st + kSurfaceVoxels, ss, &launches);
+        if (timer) timer->mark(1, true, ss);
+        // Material keys by surface rank (independent of pruning).
+        if (timer) timer->mark(4, false, ss);
+        launch_surface_keys_zero(keys.p, st + kSurfaceVoxels, keysCap_, wide_ ? 1 : 0, ss, &launches);
+        tuneMark(kKnobMerge, false, ss);
+        if (!wide_)
+            launch_surface_merge(hitList.as<unsigned long long>(), st + kHitCount, listCap_, surf.as<uint32_t>(),
+                                  ranks.as<uint32_t>(), keys.as<uint32_t>(), keysCap_, shape.mergeBlocksPerSm, ss,
+                                  &launches);
+        else
+            launch_surface_work(nodeKind_, 1, 1, b, recs.p, ovl.p, sOffsets.as<uint32_t>(), nWork_,
+                                st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(),
+                                keys.p, keysCap_, nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch,
+                                shape.surfQueue ? st + kSurfQueue : nullptr, ss, &launches);
+        tuneMark(kKnobMerge, true, ss);
+        if (timer) timer->mark(4, true, ss);
+        VXB_CUDA(cudaEventRecord(evSurfDone_, ss));
+    }
     // Solid voxelization.
     mark(0, false);
     VXB_CUDA(cudaMemsetAsync(fillP, 0, wordBytes, s));
@@ -355,32 +410,9 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
         VXB_CUDA(cudaGetLastError());
         return 0;
     }
-    // Surface voxelization, hit list and surface ranks.
-    if (anyMaterials_) {
-        mark(1, false);
-        VXB_CUDA(cudaMemsetAsync(surf.p, 0, 4 * (size_t)totalWords_, s));
-        VXB_CUDA(cudaMemsetAsync(buckets.p, 0, 4 * 2 * kSurfaceBuckets, s));
-        VXB_CUDA(cudaMemsetAsync(counts.p, 0, 4 * ((size_t)nWork_ + 1), s));
-        VXB_CUDA(cudaMemsetAsync(st + kHitCount, 0, 4, s));
-        launch_surface_prepare(b, nWork_, codes.as<uint32_t>(), unitCounts.as<uint32_t>(), buckets.as<uint32_t>(),
-                               perm.as<uint32_t>(), counts.as<uint32_t>(), recs.p, ovl.p, s, &launches);
-        launch_scan(counts.as<uint32_t>(), offsets.as<uint32_t>(), nWork_, tileSums.as<uint32_t>(), st + kSurfTotal,
-                    st + kSurfOverflow, s, &launches);
-        mark(5, false);
-        tuneMark(kKnobSurface, false, s);
-        launch_surface_work(nodeKind_, 0, wide_ ? 1 : 0, b, recs.p, ovl.p, offsets.as<uint32_t>(), nWork_,
-                            st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(),
-                            keys.p, keysCap_, hitList.as<unsigned long long>(), st + kHitCount, listCap_,
-                            shape.surfBlocksPerSm, shape.surfBatch, shape.surfQueue ? st + kSurfQueue : nullptr, s,
-                            &launches);
-        tuneMark(kKnobSurface, true, s);
-        mark(5, true);
-        launch_surface_rank(surf.as<uint32_t>(), totalWords_, ranks.as<uint32_t>(), rankTiles.as<uint32_t>(),
-                            st + kSurfaceVoxels, s, &launches);
-        mark(1, true);
-    }
     // Split-ordered pruning (src/host_side.cpp:1183-1206).
     if (anyCartesian_ && !raw_) {
+        if (anyMaterials_) VXB_CUDA(cudaStreamWaitEvent(s, evSurfBits_, 0));
         mark(2, false);
         if (anyMaterials_)
             launch_combine(fillP, surf.as<uint32_t>(), fin.as<uint32_t>(), totalWords_, s, &launches);
@@ -411,23 +443,8 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
         }
         mark(2, true);
     }
-    // Material keys by surface rank.
-    if (anyMaterials_) {
-        mark(4, false);
-        launch_surface_keys_zero(keys.p, st + kSurfaceVoxels, keysCap_, wide_ ? 1 : 0, s, &launches);
-        tuneMark(kKnobMerge, false, s);
-        if (!wide_)
-            launch_surface_merge(hitList.as<unsigned long long>(), st + kHitCount, listCap_, surf.as<uint32_t>(),
-                                  ranks.as<uint32_t>(), keys.as<uint32_t>(), keysCap_, shape.mergeBlocksPerSm, s,
-                                  &launches);
-        else
-            launch_surface_work(nodeKind_, 1, 1, b, recs.p, ovl.p, offsets.as<uint32_t>(), nWork_,
-                                st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(),
-                                keys.p, keysCap_, nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch,
-                                shape.surfQueue ? st + kSurfQueue : nullptr, s, &launches);
-        tuneMark(kKnobMerge, true, s);
-        mark(4, true);
-    }
+    // Join: emission reads the merged keys.
+    if (anyMaterials_) VXB_CUDA(cudaStreamWaitEvent(s, evSurfDone_, 0));
     // Node emission.
     mark(3, false);
     if (raw_ && anyCartesian_)
@@ -498,6 +515,9 @@ int Pipeline::pruneGroupUntilStable(const Group& gr, cudaStream_t s) {
 }
 
 Pipeline::~Pipeline() {
+    for (cudaEvent_t e : {evFork_, evSurfBits_, evSurfDone_})
+        if (e) cudaEventDestroy(e);
+    if (side_) cudaStreamDestroy(side_);
     for (cudaEvent_t& e : tuneEv_)
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t& e : outEv_)
@@ -573,7 +593,7 @@ int Pipeline::finish(cudaStream_t s) {
                 keysCap_ = surfaceVoxels + 1;
             }
             launch_surface_keys_zero(keys.p, st + kSurfaceVoxels, keysCap_, wide_ ? 1 : 0, s, &launches);
-            launch_surface_work(nodeKind_, 1, wide_ ? 1 : 0, b, recs.p, ovl.p, offsets.as<uint32_t>(), nWork_,
+            launch_surface_work(nodeKind_, 1, wide_ ? 1 : 0, b, recs.p, ovl.p, sOffsets.as<uint32_t>(), nWork_,
                                 st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(),
                                 keys.p, keysCap_, nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch,
                                 shape.surfQueue ? st + kSurfQueue : nullptr, s, &launches);

@@ -134,6 +134,12 @@ private:
     DevBuf tables, status, counts, offsets, tileSums;
     DevBuf fill, surf, fin, ranks, rankTiles, pruneScratch, pruneLists;
     DevBuf codes, unitCounts, perm, buckets, recs, ovl, hitList, keys;
+    // The surface pass runs on a second stream beside the solid pass (its
+    // own work-list scan buffers), joined before pruning (surface bits) and
+    // before emission (merged keys).
+    DevBuf sCounts, sOffsets, sTileSums;
+    cudaStream_t side_ = nullptr;
+    cudaEvent_t evFork_ = nullptr, evSurfBits_ = nullptr, evSurfDone_ = nullptr;
 };
 
 }  // namespace vxb
