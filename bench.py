@@ -610,10 +610,11 @@ def served_rows(args, local, rates, seconds):
     return rows
 
 
-def autotune(args, call, rounds=8):
+def autotune(args, call, rounds=12):
     """With --autotune on: switch the launch-shape tuner on and make
-    `rounds` untimed calls (3 candidate shapes x 2 samples settle a size
-    bucket); returns the settled shapes (None when off)."""
+    `rounds` untimed calls (3 candidate shapes x 2 samples, then 2
+    material-key strategies x 2 samples settle a size bucket); returns the
+    settled shapes (None when off)."""
     if args.autotune != "on":
         return None
     from voxelizer_b200 import _lib

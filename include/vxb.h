@@ -210,7 +210,7 @@ typedef struct {
     uint32_t work_triangles;        /* triangles x lattices */
     uint32_t solid_candidates;      /* (triangle, subspace, 4x4 tile) candidates of the solid pass */
     uint32_t surface_columns;       /* work items of the surface pass */
-    uint32_t surface_hits;          /* surface voxel hits (with repeats) */
+    uint32_t surface_hits;          /* surface voxel hits (with repeats); 0 when no hit list was kept */
     uint32_t surface_voxels;        /* distinct surface voxels */
     uint32_t surface_triangles[3];  /* triangles with surface work by class: 1D, 2D, 3D boxes */
     uint64_t grid_words;            /* 32-bit words of one bit grid */

@@ -21,23 +21,20 @@ def _tuner_off():
 
 def test_modes_and_cache_file(tmp_path):
     path = tmp_path / "shapes.json"
-    path.write_text('{\n'
-                    '  "t12-w17-k1-m1": {"surf_blocks_per_sm": 16, "surf_batch": 8, "merge_blocks_per_sm": 32, '
-                    '"emit_blocks_per_sm": 8, "toggle_blocks_per_sm": 6, "surf_queue": 1, "toggle_queue": 1},\n'
-                    '  "t13-w17-k1-m1": {"surf_blocks_per_sm": 7, "surf_batch": 8, "merge_blocks_per_sm": 32, '
-                    '"emit_blocks_per_sm": 8, "toggle_blocks_per_sm": 6, "surf_queue": 0, "toggle_queue": 0},\n'
-                    '  "t14-w17-k1-m1": {"surf_blocks_per_sm": 16, "surf_batch": 8, "merge_blocks_per_sm": 32, '
-                    '"emit_blocks_per_sm": 8, "toggle_blocks_per_sm": 6}\n'
-                    '}\n')
+    good = {"surf_blocks_per_sm": 16, "surf_batch": 8, "merge_blocks_per_sm": 32, "emit_blocks_per_sm": 8,
+            "toggle_blocks_per_sm": 6, "surf_queue": 1, "toggle_queue": 1, "surf_merge": 1}
+    bad_shape = dict(good, surf_blocks_per_sm=7)
+    bad_merge = dict(good, surf_merge=2)
+    old_format = {k: v for k, v in good.items() if k != "surf_merge"}
+    path.write_text("{\n" + ",\n".join(f'  "{k}": {json.dumps(v)}' for k, v in (
+        ("t12-w17-k1-m1", good), ("t13-w17-k1-m1", bad_shape), ("t14-w17-k1-m1", bad_merge),
+        ("t15-w17-k1-m1", old_format))) + "\n}\n")
     _lib.set_autotune(2, str(path))
     n, text = _lib.autotune_state()
-    # The second entry names a shape that is not a candidate; the third
-    # lacks the work-distribution fields.
+    # Entries naming a value that is not a candidate, or lacking a field of
+    # the current format, are skipped.
     assert n == 1
-    shapes = json.loads(text)
-    assert shapes == {"t12-w17-k1-m1": {"surf_blocks_per_sm": 16, "surf_batch": 8, "merge_blocks_per_sm": 32,
-                                        "emit_blocks_per_sm": 8, "toggle_blocks_per_sm": 6, "surf_queue": 1,
-                                        "toggle_queue": 1}}
+    assert json.loads(text) == {"t12-w17-k1-m1": good}
     with pytest.raises(_lib.VxbError, match="EINVAL"):
         _lib.set_autotune(3)
     _lib.set_autotune(0)
@@ -53,7 +50,9 @@ def test_tuning_keeps_results_and_settles(tmp_path):
         want, _ = vx.voxelizeToNodesToRAM(160)
         wbits, _ = vx.voxelizeToRAM(160)
         _lib.set_autotune(1, str(path))
-        for _ in range(8):   # 3 candidates x 2 samples settle the bucket
+        # 3 shape candidates x 2 samples, then (node grids with materials)
+        # 2 material-key strategies x 2 samples settle a bucket.
+        for _ in range(12):
             got, _ = vx.voxelizeToNodesToRAM(160)
             assert np.array_equal(got, want)
             bits, _ = vx.voxelizeToRAM(160)
@@ -66,3 +65,13 @@ def test_tuning_keeps_results_and_settles(tmp_path):
         assert _lib.autotune_state()[0] == n
         got, _ = vx.voxelizeToNodesToRAM(160)
         assert np.array_equal(got, want)
+        # Both material-key strategies, forced through the cache, give the
+        # same node grid.
+        shapes = json.loads(text)
+        for merge in (0, 1):
+            path.write_text("{\n" + ",\n".join(f'  "{k}": {json.dumps(dict(s, surf_merge=merge))}'
+                                                for k, s in shapes.items()) + "\n}\n")
+            _lib.set_autotune(2, str(path))
+            for nodes in (True, False):
+                got, _ = vx.voxelizeToNodesToRAM(160) if nodes else vx.voxelizeToRAM(160)
+                assert np.array_equal(got, want if nodes else wbits), merge

@@ -360,9 +360,14 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
                                perm.as<uint32_t>(), sCounts.as<uint32_t>(), recs.p, ovl.p, ss, &launches);
         launch_scan(sCounts.as<uint32_t>(), sOffsets.as<uint32_t>(), nWork_, sTileSums.as<uint32_t>(),
                     st + kSurfTotal, st + kSurfOverflow, ss, &launches);
+        // Without a hit list (PartialNode keys, or the tuned strategy) the
+        // first traversal sets surface bits only and a second one merges
+        // every hit at its rank.
+        const bool retraverse = wide_ || shape.surfMerge != 0;
         if (timer) timer->mark(5, false, ss);
+        tuneMark(kKnobSurfaceSpan, false, ss);
         tuneMark(kKnobSurface, false, ss);
-        launch_surface_work(nodeKind_, 0, wide_ ? 1 : 0, b, recs.p, ovl.p, sOffsets.as<uint32_t>(), nWork_,
+        launch_surface_work(nodeKind_, retraverse ? 2 : 0, wide_ ? 1 : 0, b, recs.p, ovl.p, sOffsets.as<uint32_t>(), nWork_,
                             st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(),
                             keys.p, keysCap_, hitList.as<unsigned long long>(), st + kHitCount, listCap_,
                             shape.surfBlocksPerSm, shape.surfBatch, shape.surfQueue ? st + kSurfQueue : nullptr, ss,
@@ -377,16 +382,17 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
         if (timer) timer->mark(4, false, ss);
         launch_surface_keys_zero(keys.p, st + kSurfaceVoxels, keysCap_, wide_ ? 1 : 0, ss, &launches);
         tuneMark(kKnobMerge, false, ss);
-        if (!wide_)
+        if (!retraverse)
             launch_surface_merge(hitList.as<unsigned long long>(), st + kHitCount, listCap_, surf.as<uint32_t>(),
                                   ranks.as<uint32_t>(), keys.as<uint32_t>(), keysCap_, shape.mergeBlocksPerSm, ss,
                                   &launches);
         else
-            launch_surface_work(nodeKind_, 1, 1, b, recs.p, ovl.p, sOffsets.as<uint32_t>(), nWork_,
+            launch_surface_work(nodeKind_, 1, wide_ ? 1 : 0, b, recs.p, ovl.p, sOffsets.as<uint32_t>(), nWork_,
                                 st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(),
                                 keys.p, keysCap_, nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch,
                                 shape.surfQueue ? st + kSurfQueue : nullptr, ss, &launches);
         tuneMark(kKnobMerge, true, ss);
+        tuneMark(kKnobSurfaceSpan, true, ss);
         if (timer) timer->mark(4, true, ss);
         VXB_CUDA(cudaEventRecord(evSurfDone_, ss));
     }

@@ -25,7 +25,9 @@
 // materials from there.  The key orders triangles by class, then material
 // (NodeT in vxb_device.cuh), so the merged key names the winning material.
 // If the list overflows, a second traversal (mode 1) merges every hit
-// directly.
+// directly.  The same second traversal is the whole merge where no list is
+// kept (64-bit PartialNode keys, or when the launch-shape tuner measured it
+// faster): the first traversal then sets surface bits only (mode 2).
 
 #include "vxb_common.cuh"
 #include "vxb_device.cuh"
@@ -368,7 +370,8 @@ struct UnitGrid {
 
 // processVoxel of the surface pass.
 // mode 0: set the bit and append (bit position << 24 | key) to the hit list;
-// mode 1: merge the key at the voxel's rank (surface bits are complete).
+// mode 1: merge the key at the voxel's rank (surface bits are complete);
+// mode 2: set the bit only (a mode-1 traversal merges the keys).
 struct Sink {
     uint32_t* bits;            // surface arena
     const uint32_t* wordRank;  // exclusive popcount prefix per word (mode 1)
@@ -387,7 +390,9 @@ struct Sink {
         const uint64_t w = ug.wordBase + ((uint64_t)z * ug.AY + y) * ug.ipx + (x >> 5);
         const uint32_t b = x & 31u;
         const uint32_t bit = 0x80000000u >> b;
-        if (mode == 0) {
+        if (mode == 2) {
+            atomicOr(bits + w, bit);
+        } else if (mode == 0) {
             atomicOr(bits + w, bit);
             const unsigned long long e = ((unsigned long long)(w * 32 + b) << 24) | (key & 0xFFFFFFull);
             const uint32_t at = atomicAdd(ws.count, 1u);

@@ -42,6 +42,11 @@ struct Entry {
     uint32_t issued = 0;
     double sum[kKnobs][kTuneCandidates] = {};
     uint32_t n[kKnobs][kTuneCandidates] = {};
+    // Second phase: the settled shapes with each material-key strategy.
+    bool mergePhase = false;
+    uint32_t issuedMerge = 0;
+    double span[kMergeCandidates] = {};
+    uint32_t nSpan[kMergeCandidates] = {};
 };
 
 struct State {
@@ -56,14 +61,14 @@ State& state() {
     return *s;
 }
 
-constexpr int kFieldCount = 7;
+constexpr int kFieldCount = 8;
 const char* const kFields[kFieldCount] = {"surf_blocks_per_sm", "surf_batch", "merge_blocks_per_sm",
                                           "emit_blocks_per_sm", "toggle_blocks_per_sm", "surf_queue",
-                                          "toggle_queue"};
+                                          "toggle_queue", "surf_merge"};
 
 uint32_t* field(LaunchShape& s, int i) {
-    uint32_t* f[kFieldCount] = {&s.surfBlocksPerSm, &s.surfBatch,   &s.mergeBlocksPerSm, &s.emitBlocksPerSm,
-                                &s.toggleBlocksPerSm, &s.surfQueue, &s.toggleQueue};
+    uint32_t* f[kFieldCount] = {&s.surfBlocksPerSm,   &s.surfBatch, &s.mergeBlocksPerSm, &s.emitBlocksPerSm,
+                                &s.toggleBlocksPerSm, &s.surfQueue, &s.toggleQueue,      &s.surfMerge};
     return f[i];
 }
 
@@ -75,7 +80,7 @@ bool validShape(const LaunchShape& s) {
     };
     return in(s.surfBlocksPerSm, kSurfBlocks) && in(s.surfBatch, kSurfBatch) && in(s.mergeBlocksPerSm, kMerge) &&
            in(s.emitBlocksPerSm, kEmit) && in(s.toggleBlocksPerSm, kToggle) && in(s.surfQueue, kSurfQueue) &&
-           in(s.toggleQueue, kToggleQueue);
+           in(s.toggleQueue, kToggleQueue) && s.surfMerge < (uint32_t)kMergeCandidates;
 }
 
 std::string jsonLocked(const State& st) {
@@ -156,18 +161,40 @@ LaunchShape tunePick(const std::string& bucket, int* trial, bool allowTrial) {
     Entry& e = st.buckets[bucket];
     if (e.settled) return e.best;
     if (!allowTrial) return LaunchShape();
+    if (e.mergePhase) {
+        const int m = (int)(e.issuedMerge++ % kMergeCandidates);
+        *trial = kTuneCandidates + m;
+        LaunchShape s = e.best;
+        s.surfMerge = (uint32_t)m;
+        return s;
+    }
     const int k = (int)(e.issued++ % kTuneCandidates);
     *trial = k;
     return candidate(k);
 }
 
 void tuneReport(const std::string& bucket, int trial, const float* ms) {
-    if (trial < 0 || trial >= kTuneCandidates) return;
+    if (trial < 0 || trial >= kTuneCandidates + kMergeCandidates) return;
     State& st = state();
     std::lock_guard<std::mutex> lock(st.mu);
     if (st.mode != kTuneOn) return;
     Entry& e = st.buckets[bucket];
     if (e.settled) return;
+    if (trial >= kTuneCandidates) {
+        if (!e.mergePhase) return;
+        const int m = trial - kTuneCandidates;
+        if (ms[kKnobSurfaceSpan] >= 0.0f) {
+            e.span[m] += ms[kKnobSurfaceSpan];
+            e.nSpan[m] += 1;
+        }
+        for (int k = 0; k < kMergeCandidates; ++k)
+            if (e.nSpan[k] < (uint32_t)kTuneSamples) return;
+        e.best.surfMerge = e.span[1] / e.nSpan[1] < e.span[0] / e.nSpan[0] ? 1u : 0u;
+        e.settled = true;
+        saveLocked(st);
+        return;
+    }
+    if (e.mergePhase) return;
     for (int kn = 0; kn < kKnobs; ++kn)
         if (ms[kn] >= 0.0f) {
             e.sum[kn][trial] += ms[kn];
@@ -181,7 +208,7 @@ void tuneReport(const std::string& bucket, int trial, const float* ms) {
         if (most < (uint32_t)kTuneSamples) return;
     }
     LaunchShape best;
-    for (int kn = 0; kn < kKnobs; ++kn) {
+    for (int kn = 0; kn < kKnobSurfaceSpan; ++kn) {
         int arg = 0;
         double bestMs = HUGE_VAL;
         for (int k = 0; k < kTuneCandidates; ++k) {
@@ -208,6 +235,13 @@ void tuneReport(const std::string& bucket, int trial, const float* ms) {
         }
     }
     e.best = best;
+    // Buckets with a surface pass go on to the material-key strategies.
+    bool surface = false;
+    for (int k = 0; k < kTuneCandidates; ++k) surface |= e.n[kKnobSurfaceSpan][k] > 0;
+    if (surface) {
+        e.mergePhase = true;
+        return;
+    }
     e.settled = true;
     saveLocked(st);
 }

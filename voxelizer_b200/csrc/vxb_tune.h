@@ -25,11 +25,18 @@ struct LaunchShape {
     // take the next batch of items with one atomic each).
     uint32_t surfQueue = 0;
     uint32_t toggleQueue = 0;
+    // Material keys of the surface pass: 0 a hit list that mergeKeysKernel
+    // merges at the surface ranks, 1 no hit list and a second traversal that
+    // merges every hit at its rank.  Tuned after the shapes above are
+    // settled, on the time from the first traversal to the merged keys.
+    uint32_t surfMerge = 0;
 };
 
-// The tuned kernels, in the order of their timing events.
-enum TuneKnob { kKnobSurface = 0, kKnobMerge = 1, kKnobEmit = 2, kKnobToggle = 3, kKnobs = 4 };
+// The tuned kernels, in the order of their timing events; kKnobSurfaceSpan
+// times the surface pass from its first traversal to its merged keys.
+enum TuneKnob { kKnobSurface = 0, kKnobMerge = 1, kKnobEmit = 2, kKnobToggle = 3, kKnobSurfaceSpan = 4, kKnobs = 5 };
 constexpr int kTuneCandidates = 3;
+constexpr int kMergeCandidates = 2;
 constexpr int kTuneSamples = 2;
 
 enum TuneMode { kTuneOff = 0, kTuneOn = 1, kTuneFrozen = 2 };
@@ -38,7 +45,9 @@ enum TuneMode { kTuneOff = 0, kTuneOn = 1, kTuneFrozen = 2 };
 std::string tuneBucket(uint32_t workTriangles, uint64_t gridWords, int nodeKind, bool materials);
 
 // The shape for the next run of `bucket`.  *trial >= 0 when the run is a
-// tuning trial (its kernel times go to tuneReport); -1 otherwise.
+// tuning trial (its kernel times go to tuneReport); -1 otherwise.  Trials
+// 0 .. kTuneCandidates-1 try the launch shapes, the later ones the
+// material-key strategies on the settled shapes.
 LaunchShape tunePick(const std::string& bucket, int* trial, bool allowTrial = true);
 // Kernel times (ms, < 0 for a kernel that did not run) of trial `trial`.
 void tuneReport(const std::string& bucket, int trial, const float* ms);
