@@ -5,9 +5,11 @@
 // row): it forms the six neighbour masks of its word with shifts of the word
 // and of the words around it, so a whole word of boundary ids costs a few
 // bitwise operations when the word is uniform (all empty, or all solid with
-// all six neighbours solid: id 27) and a per-node table lookup only where
-// solid meets empty.  A warp's 32 words are staged in shared memory and
-// stored as contiguous 512-byte rows with 16-byte vector stores.
+// all six neighbours solid: id 27).  For 1- and 2-byte nodes the ids of a
+// mixed word are computed bit-sliced (five planes, one per id bit) and
+// transposed to bytes; PartialNodes and FCC nodes take a per-node table
+// lookup where solid meets empty.  A warp's 32 words are staged in shared
+// memory and stored as contiguous 512-byte rows with 16-byte vector stores.
 //
 // Grids of one unit hold fewer than 2^32 voxels, so word indices inside a
 // unit fit 32 bits; arena offsets (unit word bases) are 64-bit.
@@ -330,17 +332,70 @@ __device__ __forceinline__ WordNbrs loadNbrs(const UnitWords& u, uint32_t w) {
     return n;
 }
 
+// Boundary ids of the nodes `cm` of a word as five bit planes: plane k holds
+// bit k of every node's id.  Along each axis a node has a solid neighbour
+// below only (1), above only (2) or on both sides (3); the id is
+// kOrientTable[x | y << 2 | z << 4] for those three codes (0 when an axis has
+// none), and each plane is the union of the code combinations whose id has
+// that bit set, evaluated on whole words at once.
+__device__ __forceinline__ void idPlanes(const WordNbrs& n, uint32_t cm, uint32_t P[5]) {
+    const uint32_t L = n.L, R = n.R;
+    const uint32_t X1 = L & ~R, X3 = L & R, Xo = L ^ R, Xa = L | R, X2 = R & ~L;
+    const uint32_t Y1 = n.In & ~n.Out, Y2 = n.Out & ~n.In, Y3 = n.In & n.Out, Ya = n.In | n.Out;
+    const uint32_t Z1 = n.Dn & ~n.Up, Z2 = n.Up & ~n.Dn, Z3 = n.Dn & n.Up, Za = n.Dn | n.Up, Zo = n.Dn ^ n.Up;
+    P[0] = ((Za & ((Y1 & L) | (Y2 & X1))) | (Y3 & ((n.Dn & L) | (Z2 & X1)))) & cm;
+    P[1] = ((Y1 & ((Zo & X2) | (Z3 & R))) | (Za & Y2 & L) | (Y3 & ((Z1 & X1) | (Z2 & L) | (Z3 & X3)))) & cm;
+    P[2] = ((Z1 & ((Y2 & X2) | (Y3 & R))) | (Z2 & ((Y1 & Xa) | (Y2 & L) | (Y3 & X1))) | (Z3 & ((Y1 & X3) | (Y2 & R)))) &
+           cm;
+    P[3] = ((Z1 & (((Y1 | Y2) & X3) | (Y3 & Xo))) | (Z2 & ((Y1 & X3) | (Y2 & R) | (Y3 & L))) | (Z3 & Y3 & Xa)) & cm;
+    P[4] = ((Y3 & ((Z1 & X3) | (Z2 & R))) | (Z3 & Ya & Xa)) & cm;
+}
+
+// The planes as bytes in node order: N[m] holds the ids of nodes 4m .. 4m+3
+// (node t of a word is bit 31 - t), one per byte.  An 8x8 bit transpose in
+// each byte lane of the bit-reversed planes leaves the id of node 8b + i in
+// byte b of row i; 4x4 byte transposes put the nodes in order.
+__device__ __forceinline__ void idBytes(const uint32_t P[5], uint32_t N[8]) {
+    uint32_t r[8];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) r[k] = __brev(P[k]);
+    r[5] = r[6] = r[7] = 0u;
+#pragma unroll
+    for (int s = 4; s >= 1; s >>= 1) {
+        const uint32_t m = s == 4 ? 0x0F0F0F0Fu : s == 2 ? 0x33333333u : 0x55555555u;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if ((k / s) % 2 == 0) {
+                const uint32_t t = ((r[k] >> s) ^ r[k + s]) & m;
+                r[k + s] ^= t;
+                r[k] ^= t << s;
+            }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const uint32_t t0 = __byte_perm(r[4 * h], r[4 * h + 1], 0x5140), t1 = __byte_perm(r[4 * h], r[4 * h + 1], 0x7362);
+        const uint32_t t2 = __byte_perm(r[4 * h + 2], r[4 * h + 3], 0x5140),
+                       t3 = __byte_perm(r[4 * h + 2], r[4 * h + 3], 0x7362);
+        N[h] = __byte_perm(t0, t2, 0x5410);
+        N[2 + h] = __byte_perm(t0, t2, 0x7632);
+        N[4 + h] = __byte_perm(t1, t3, 0x5410);
+        N[6 + h] = __byte_perm(t1, t3, 0x7632);
+    }
+}
+
 __device__ __forceinline__ uint32_t permOf(const WordNbrs& n, uint32_t q) {
     return ((n.L >> q) & 1u) | (((n.R >> q) & 1u) << 1) | (((n.In >> q) & 1u) << 2) | (((n.Out >> q) & 1u) << 3) |
            (((n.Dn >> q) & 1u) << 4) | (((n.Up >> q) & 1u) << 5);
 }
 
 // 1- and 2-byte nodes.  Each lane owns one word and builds its 32 nodes in
-// its own shared-memory row: nodes whose six neighbours are all solid and
-// that carry no material (id 27) come from a bit expansion, and only the
-// remaining set bits (solid next to empty, surface nodes) are visited one by
-// one.  The warp's 32 rows are then stored as one contiguous span.  Unit
-// word bases are multiples of 32, so a warp's words belong to one unit.
+// its own shared-memory row: the ids of all 32 come from the bit planes of
+// idPlanes (or a constant for empty and all-interior words), the materials
+// of surface nodes from the merged keys, which are consecutive by rank (a
+// word whose 32 nodes are all surface nodes loads its 32 keys without a
+// per-node loop).  The warp's 32 rows are then stored as one contiguous
+// span.  Unit word bases are multiples of 32, so a warp's words belong to
+// one unit.
 template <int K>
 __global__ void __launch_bounds__(256, 6) emitNarrowKernel(EmitArgs a, uint64_t wordBegin, uint64_t totalWords) {
     typedef NodeT<K> NT;
@@ -350,9 +405,6 @@ __global__ void __launch_bounds__(256, 6) emitNarrowKernel(EmitArgs a, uint64_t 
     constexpr int CH = WB / 16;                  // 16-byte chunks per word
     constexpr int PITCH = (CH + 1) * 16;         // padded smem row (conflict-free)
     __shared__ __align__(16) uint8_t stage[8][32 * PITCH];
-    __shared__ uint8_t lut[64];
-    if (threadIdx.x < 64) lut[threadIdx.x] = kOrientTable[threadIdx.x];
-    __syncthreads();
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     uint8_t* my = stage[warp] + lane * PITCH;
     const uint32_t v27 = (uint32_t)NT::pack(27u, 0u, 0.0f);
@@ -381,47 +433,54 @@ __global__ void __launch_bounds__(256, 6) emitNarrowKernel(EmitArgs a, uint64_t 
             n = loadNbrs<K>(uw, w);
             zero = borderMask(uw, w);
         }
-        const uint32_t interior = n.c & n.L & n.R & n.In & n.Out & n.Dn & n.Up & ~n.s0 & ~zero;
-        uint32_t rest = ((n.c & ~interior) | n.s0) & ~zero;
-        uint32_t v[CH * 4];
-        if (interior == 0u) {
+        // Ids: none, all 27 (every node solid with six solid neighbours), or
+        // the bit-sliced planes.  Materials of surface nodes follow by rank.
+        const uint32_t cm = n.c & ~zero, sm = n.s0 & ~zero;
+        if (cm == 0u || (cm & n.L & n.R & n.In & n.Out & n.Dn & n.Up) == 0xFFFFFFFFu) {
+            const uint32_t rep = cm == 0u ? 0u : NB == 1 ? v27 * 0x01010101u : v27 * 0x00010001u;
 #pragma unroll
-            for (int i = 0; i < CH * 4; ++i) v[i] = 0u;
-        } else if (interior == 0xFFFFFFFFu) {
-            const uint32_t rep = NB == 1 ? v27 * 0x01010101u : v27 * 0x00010001u;
-#pragma unroll
-            for (int i = 0; i < CH * 4; ++i) v[i] = rep;
+            for (int i = 0; i < CH; ++i) *reinterpret_cast<uint4*>(my + 16 * i) = make_uint4(rep, rep, rep, rep);
         } else {
+            uint32_t N[8];
+            {
+                uint32_t P[5];
+                idPlanes(n, cm, P);
+                idBytes(P, N);
+            }
 #pragma unroll
-            for (int i = 0; i < CH * 4; ++i) {
-                uint32_t x = 0u;
-#pragma unroll
-                for (int j = 0; j < 4 / NB; ++j) {
-                    const uint32_t bt = (uint32_t)(i * (4 / NB) + j);
-                    x |= ((interior >> (31u - bt)) & 1u) * (v27 << (8 * NB * j));
+            for (int i = 0; i < CH; ++i) {
+                uint4 q;
+                if (NB == 1) {
+                    q = make_uint4(N[4 * i], N[4 * i + 1], N[4 * i + 2], N[4 * i + 3]);
+                } else {
+                    q = make_uint4(__byte_perm(N[2 * i], 0u, 0x4140), __byte_perm(N[2 * i], 0u, 0x4342),
+                                   __byte_perm(N[2 * i + 1], 0u, 0x4140), __byte_perm(N[2 * i + 1], 0u, 0x4342));
                 }
-                v[i] = x;
+                *reinterpret_cast<uint4*>(my + 16 * i) = q;
             }
         }
-#pragma unroll
-        for (int i = 0; i < CH; ++i)
-            *reinterpret_cast<uint4*>(my + 16 * i) = make_uint4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
-        if (rest) {
-            const uint32_t rank0 = n.s0 ? __ldg(a.ranks + uBase + w) : 0u;
-            do {
-                const uint32_t bt = __clz(rest);       // node index in the word
-                const uint32_t q = 31u - bt;          // its bit
-                uint32_t bid = 0u, mat = 0u;
-                if ((n.c >> q) & 1u) bid = lut[permOf(n, q)];
-                if ((n.s0 >> q) & 1u) {
-                    const uint32_t r = rank0 + (bt ? __popc(n.s0 >> (32u - bt)) : 0u);
-                    mat = r < a.keysCap ? NT::keyMat(reinterpret_cast<const uint32_t*>(a.keys)[r]) : 0u;
+        if (sm) {
+            const uint32_t* keys = reinterpret_cast<const uint32_t*>(a.keys);
+            const uint32_t rank0 = __ldg(a.ranks + uBase + w);
+            if (sm == 0xFFFFFFFFu && (uint64_t)rank0 + 32u <= a.keysCap) {
+                // 32 surface nodes: their keys are the 32 from rank0 on.
+#pragma unroll 8
+                for (uint32_t j = 0; j < 32u; ++j) {
+                    const uint32_t mat = NT::keyMat(__ldg(keys + rank0 + j));
+                    if (NB == 1) my[j] |= (uint8_t)(mat << 5);
+                    else my[2 * j + 1] = (uint8_t)mat;
                 }
-                const uint32_t nv = (uint32_t)NT::pack(bid, mat, 0.0f);
-                if (NB == 1) my[bt] = (uint8_t)nv;
-                else reinterpret_cast<uint16_t*>(my)[bt] = (uint16_t)nv;
-                rest &= ~(0x80000000u >> bt);
-            } while (rest);
+            } else {
+                uint32_t rest = sm;
+                do {
+                    const uint32_t bt = __clz(rest);       // node index in the word
+                    const uint32_t r = rank0 + (bt ? __popc(n.s0 >> (32u - bt)) : 0u);
+                    const uint32_t mat = r < a.keysCap ? NT::keyMat(__ldg(keys + r)) : 0u;
+                    if (NB == 1) my[bt] |= (uint8_t)(mat << 5);
+                    else my[2 * bt + 1] = (uint8_t)mat;
+                    rest &= ~(0x80000000u >> bt);
+                } while (rest);
+            }
         }
         __syncwarp();
         const uint32_t wend = wbase + 32u <= nWords ? 32u : nWords - wbase;
