@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(kBlock, 3) solidToggleKernel(Batch b, uint32_t
                                                                uint32_t* __restrict__ fill, uint32_t* queue) {
     __shared__ SolidStage stage[kSlots];
     __shared__ uint32_t stOff[kSlots + 1];
-    __shared__ uint32_t tFirst, nStage, nextBase;
+    __shared__ uint32_t tFirst, tLast, nextBase;
     const uint32_t total = *totalPtr;
     // Batches of kBlock candidates in a fixed grid-stride order, or
     // (queue != NULL) taken from a device work queue, one atomic per batch.
@@ -230,17 +230,20 @@ __global__ void __launch_bounds__(kBlock, 3) solidToggleKernel(Batch b, uint32_t
     }
     while (base < total) {
         const uint32_t last = min(base + kBlock, total) - 1;
-        if (threadIdx.x == 0) {
-            const uint32_t t0 = findOwner(offsets, nWork, base);
-            const uint32_t t1 = findOwner(offsets, nWork, last);
-            tFirst = t0;
-            nStage = min(t1 - t0 + 1, kSlots);
+        // Owners of the batch's first and last items, one warp each.
+        if (threadIdx.x < 64) {
+            const uint32_t t = warpFindOwner(offsets, nWork, threadIdx.x < 32 ? base : last, threadIdx.x & 31u);
+            if (threadIdx.x == 0) tFirst = t;
+            if (threadIdx.x == 32) tLast = t;
         }
         __syncthreads();
-        const uint32_t t0 = tFirst, ns = nStage;
+        const uint32_t t0 = tFirst, ns = min(tLast - t0 + 1, kSlots);
+        // Triangles without candidates between them are never selected
+        // (their offset equals the next one) and are not staged.
         if (threadIdx.x < ns) {
-            stageSolid(stage[threadIdx.x], b, t0 + threadIdx.x);
-            stOff[threadIdx.x] = __ldg(offsets + t0 + threadIdx.x);
+            const uint32_t o = __ldg(offsets + t0 + threadIdx.x);
+            stOff[threadIdx.x] = o;
+            if (__ldg(offsets + t0 + threadIdx.x + 1) > o) stageSolid(stage[threadIdx.x], b, t0 + threadIdx.x);
         }
         if (threadIdx.x == 0) stOff[ns] = __ldg(offsets + t0 + ns);
         __syncthreads();
@@ -267,25 +270,54 @@ __global__ void __launch_bounds__(kBlock, 3) solidToggleKernel(Batch b, uint32_t
     }
 }
 
-// Toggle bits -> solid runs: bit x = XOR of the toggles at or before x.
-// One thread per row walks its row's words with a running parity; a row is
-// at most 32 words per x pass and the words stay in L1 between the load and
-// the store.
+// Toggle bits -> solid runs: bit x of a row = XOR of the row's toggles at or
+// before x.  A warp takes kFillRows whole rows (consecutive words) and walks
+// them as 32-word chunks, one word per lane, so loads and stores are
+// coalesced: a lane turns its word into the prefix XOR of its bits and
+// inverts it when the words before it in its row hold an odd number of
+// toggles.  That parity is a segmented XOR scan over the lanes (a ballot of
+// word parities, cut at the lanes that start a row) plus the parity carried
+// from the previous chunk for the row that continues into this one.
+constexpr uint32_t kFillRows = 16;
+
 __global__ void rowFillKernel(Batch b, uint64_t nRows, uint32_t* __restrict__ fill) {
-    for (uint64_t row = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; row < nRows;
-         row += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t u = b.nUnits > 1 ? unitOf(b.rowBase, b.nUnits, row) : 0u;
-        const Unit& U = b.units[u];
-        const uint32_t ipx = U.g.ipx;
-        uint32_t* r = fill + U.wordBase + (row - __ldg(b.rowBase + u)) * ipx;
-        uint32_t carry = 0u;
-        for (uint32_t k = 0; k < ipx; ++k) {
-            const uint32_t w = r[k];
-            if (!(w | carry)) continue;
-            uint32_t p = w;
-            p ^= p >> 1; p ^= p >> 2; p ^= p >> 4; p ^= p >> 8; p ^= p >> 16;
-            r[k] = carry ? ~p : p;
-            carry ^= __popc(w) & 1u;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t nWarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g * kFillRows < nRows; g += nWarps) {
+        uint64_t row = g * kFillRows;
+        const uint64_t rowEnd = min(row + kFillRows, nRows);
+        while (row < rowEnd) {
+            // The rows of [row, rowEnd) in one unit.
+            const uint32_t u = b.nUnits > 1 ? unitOf(b.rowBase, b.nUnits, row) : 0u;
+            const uint64_t uRow0 = __ldg(b.rowBase + u), uRow1 = __ldg(b.rowBase + u + 1);
+            const uint64_t r1 = min(rowEnd, uRow1);
+            const Unit& U = b.units[u];
+            const uint32_t ipx = U.g.ipx;
+            uint32_t* words = fill + U.wordBase;
+            const uint32_t w0 = (uint32_t)(row - uRow0) * ipx, w1 = (uint32_t)(r1 - uRow0) * ipx;
+            uint32_t carry = 0u;
+            for (uint32_t cb = w0; cb < w1; cb += 32u) {
+                const uint32_t w = cb + lane;
+                const bool valid = w < w1;
+                const uint32_t x = valid ? words[w] : 0u;
+                const uint32_t starts = __ballot_sync(0xffffffffu, valid && (w - w0) % ipx == 0u);
+                const uint32_t odd = __ballot_sync(0xffffffffu, __popc(x) & 1u);
+                const uint32_t upTo = starts & ((2u << lane) - 1u);   // row starts at lanes <= lane
+                uint32_t below = (1u << lane) - 1u;                  // lanes < lane
+                uint32_t pre;
+                if (upTo) {
+                    below &= ~((1u << (31u - __clz(upTo))) - 1u);
+                    pre = __popc(odd & below) & 1u;
+                } else {
+                    pre = (__popc(odd & below) & 1u) ^ carry;
+                }
+                uint32_t p = x;
+                p ^= p >> 1; p ^= p >> 2; p ^= p >> 4; p ^= p >> 8; p ^= p >> 16;
+                if (pre) p = ~p;
+                if (valid && p != x) words[w] = p;
+                carry = __shfl_sync(0xffffffffu, pre ^ (__popc(x) & 1u), 31);
+            }
+            row = r1;
         }
     }
 }
@@ -305,7 +337,7 @@ void launch_solid_toggle(const Batch& b, uint32_t nWork, const uint32_t* offsets
 }
 
 void launch_row_fill(const Batch& b, uint64_t nRows, uint32_t* fill, cudaStream_t s, uint32_t* launches) {
-    rowFillKernel<<<gridFor(nRows, 256), 256, 0, s>>>(b, nRows, fill);
+    rowFillKernel<<<gridFor((nRows + kFillRows - 1) / kFillRows * 32u, 256), 256, 0, s>>>(b, nRows, fill);
     *launches += 1;
 }
 

@@ -660,17 +660,30 @@ __global__ void __launch_bounds__(kBlock) surfaceWorkKernel(Sink sink, Batch b, 
 constexpr int kRankItems = 8;
 constexpr uint32_t kRankTile = kBlock * kRankItems;
 
+// Two passes over the surface words, the second after the tile sums are
+// scanned: kApply false writes each tile's popcount sum, kApply true writes
+// the ranks (tile offset plus the block's exclusive scan).  The words were
+// just written by the surface pass and are read from L2 where they stay.
+template <bool kApply>
 __global__ void rankTileKernel(const uint32_t* __restrict__ words, uint64_t n, uint32_t* __restrict__ ranks,
                                uint32_t* __restrict__ tileSums) {
     __shared__ uint32_t warpSums[33];
     const uint64_t base = (uint64_t)blockIdx.x * kRankTile + (uint64_t)threadIdx.x * kRankItems;
+    const bool whole = base + kRankItems <= n;   // 32-byte aligned: kRankItems words per thread
     uint32_t c[kRankItems];
+    if (whole) {
+        const uint4 a = __ldg(reinterpret_cast<const uint4*>(words + base));
+        const uint4 b = __ldg(reinterpret_cast<const uint4*>(words + base) + 1);
+        const uint32_t x[kRankItems] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int i = 0; i < kRankItems; ++i) c[i] = (uint32_t)__popc(x[i]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < kRankItems; ++i) c[i] = base + i < n ? (uint32_t)__popc(__ldg(words + base + i)) : 0u;
+    }
     uint32_t sum = 0;
 #pragma unroll
-    for (int i = 0; i < kRankItems; ++i) {
-        c[i] = base + i < n ? (uint32_t)__popc(__ldg(words + base + i)) : 0u;
-        sum += c[i];
-    }
+    for (int i = 0; i < kRankItems; ++i) sum += c[i];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t incl = sum;
 #pragma unroll
@@ -692,13 +705,25 @@ __global__ void rankTileKernel(const uint32_t* __restrict__ words, uint64_t n, u
         if (lane == 31) warpSums[32] = si;
     }
     __syncthreads();
-    uint32_t ex = warpSums[warp] + incl - sum;
+    if (!kApply) {
+        if (threadIdx.x == 0) tileSums[blockIdx.x] = warpSums[32];
+        return;
+    }
+    uint32_t r[kRankItems];
+    uint32_t ex = __ldg(tileSums + blockIdx.x) + warpSums[warp] + incl - sum;
 #pragma unroll
     for (int i = 0; i < kRankItems; ++i) {
-        if (base + i < n) ranks[base + i] = ex;
+        r[i] = ex;
         ex += c[i];
     }
-    if (threadIdx.x == 0) tileSums[blockIdx.x] = warpSums[32];
+    if (whole) {
+        reinterpret_cast<uint4*>(ranks + base)[0] = make_uint4(r[0], r[1], r[2], r[3]);
+        reinterpret_cast<uint4*>(ranks + base)[1] = make_uint4(r[4], r[5], r[6], r[7]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < kRankItems; ++i)
+            if (base + i < n) ranks[base + i] = r[i];
+    }
 }
 
 __global__ void rankSumsKernel(uint32_t* tileSums, uint32_t nTiles, uint32_t* total) {
@@ -733,11 +758,6 @@ __global__ void rankSumsKernel(uint32_t* tileSums, uint32_t nTiles, uint32_t* to
         __syncthreads();
     }
     if (threadIdx.x == 0) *total = carry;
-}
-
-__global__ void rankAddKernel(uint32_t* ranks, uint64_t n, const uint32_t* __restrict__ tileSums) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        ranks[i] += tileSums[i / kRankTile];
 }
 
 __global__ void zeroKeysKernel(void* keys, const uint32_t* __restrict__ countPtr, uint32_t cap, int wide) {
@@ -844,9 +864,9 @@ void launch_surface_work(int kind, int mode, int wide, const Batch& b, const voi
 void launch_surface_rank(const uint32_t* bits, uint64_t words, uint32_t* ranks, uint32_t* tileSums, uint32_t* total,
                          cudaStream_t s, uint32_t* launches) {
     const uint32_t tiles = (uint32_t)((words + kRankTile - 1) / kRankTile);
-    rankTileKernel<<<tiles ? tiles : 1, kBlock, 0, s>>>(bits, words, ranks, tileSums);
+    rankTileKernel<false><<<tiles ? tiles : 1, kBlock, 0, s>>>(bits, words, ranks, tileSums);
     rankSumsKernel<<<1, 1024, 0, s>>>(tileSums, tiles, total);
-    rankAddKernel<<<gridFor(words, 256, 148u * 32u), 256, 0, s>>>(ranks, words, tileSums);
+    rankTileKernel<true><<<tiles ? tiles : 1, kBlock, 0, s>>>(bits, words, ranks, tileSums);
     *launches += 3;
 }
 
