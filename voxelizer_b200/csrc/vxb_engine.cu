@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -837,6 +838,23 @@ vxb_status vxb_stage_times(vxb_voxelizer* v, float* ms, uint32_t n) {
         if (e != cudaSuccess) return failf(VXB_ECUDA, "%s", cudaGetErrorString(e));
         float t = 0.0f;
         if (cudaEventElapsedTime(&t, v->timer.ev[2 * k], v->timer.ev[2 * k + 1]) == cudaSuccess) ms[k] = t;
+    }
+    return VXB_OK;
+}
+
+vxb_status vxb_stage_timeline(vxb_voxelizer* v, float* start_end, uint32_t n) {
+    if (!v || !start_end) return failf(VXB_EINVAL, "NULL argument");
+    const vxb::StageTimer& T = v->timer;
+    for (uint32_t k = 0; k < 2 * n; ++k) start_end[k] = NAN;
+    if (!T.enabled || !T.used[0]) return VXB_OK;
+    for (uint32_t k = 0; k < n && k < (uint32_t)vxb::StageTimer::kStages; ++k) {
+        if (!T.used[k]) continue;
+        cudaError_t e = cudaEventSynchronize(T.ev[2 * k + 1]);
+        if (e != cudaSuccess) return failf(VXB_ECUDA, "%s", cudaGetErrorString(e));
+        for (int j = 0; j < 2; ++j) {
+            float t = 0.0f;
+            if (cudaEventElapsedTime(&t, T.ev[0], T.ev[2 * k + j]) == cudaSuccess) start_end[2 * k + j] = t;
+        }
     }
     return VXB_OK;
 }

@@ -51,6 +51,13 @@ struct Unit {
 
 // Device tables of a batch.  Bases have nUnits + 1 entries (the last one is
 // the total), so that the unit of an element is a binary search away.
+// A surface word and the rank of its first surface voxel (the exclusive
+// popcount prefix of the surface words before it, arena-wide), side by side
+// so that one 8-byte load gives both.
+struct __align__(8) WordRank {
+    uint32_t bits, rank;
+};
+
 struct Batch {
     const Unit* units;
     uint32_t nUnits;
@@ -97,23 +104,24 @@ void launch_surface_prepare(const Batch& b, uint32_t nWork, uint32_t* codes, uin
 // entries), one thread per column.  mode 0: set bits in the `surf` arena and
 // append (bit position << 24 | key) to `list` (entries past listCap are
 // counted, not stored); mode 1: merge every hit's key at its rank (needs
-// complete bits and `ranks`).  wide: 64-bit keys (PartialNode).  kind: the
+// complete bits and their `ranks`).  wide: 64-bit keys (PartialNode).  kind: the
 // node type, whose instantiation of the class kernels the arithmetic
 // follows.  queue: as for launch_solid_toggle, per warp.
 void launch_surface_work(int kind, int mode, int wide, const Batch& b, const void* recs, const void* ovl,
                          const uint32_t* offsets, uint32_t nWork, const uint32_t* total, const uint32_t* buckets,
-                         uint32_t* surf, const uint32_t* ranks, void* keys, uint32_t keysCap,
+                         uint32_t* surf, const WordRank* ranks, void* keys, uint32_t keysCap,
                          unsigned long long* list, uint32_t* listCount, uint32_t listCap, uint32_t blocksPerSm,
                          uint32_t batch, uint32_t* queue, cudaStream_t s, uint32_t* launches);
-// Exclusive popcount prefix over `words` surface words; *total = surface voxels.
-void launch_surface_rank(const uint32_t* bits, uint64_t words, uint32_t* ranks, uint32_t* tileSums, uint32_t* total,
+// Exclusive popcount prefix over `words` surface words, stored beside each
+// word; *total = surface voxels.
+void launch_surface_rank(const uint32_t* bits, uint64_t words, WordRank* ranks, uint32_t* tileSums, uint32_t* total,
                          cudaStream_t s, uint32_t* launches);
 // Zeroes min(*count, cap) keys.
 void launch_surface_keys_zero(void* keys, const uint32_t* count, uint32_t cap, int wide, cudaStream_t s,
                               uint32_t* launches);
 // Keys at ranks >= keysCap are dropped (the host re-merges after growing).
 void launch_surface_merge(const unsigned long long* list, const uint32_t* listCount, uint32_t listCap,
-                          const uint32_t* bits, const uint32_t* ranks, uint32_t* keys, uint32_t keysCap,
+                          const WordRank* ranks, uint32_t* keys, uint32_t keysCap,
                           uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches);
 
 // Mesh checks of vxb_create (vxb_meshcheck.cu): hostOut[0..2] / [3..5]
@@ -169,7 +177,7 @@ void launch_prune_list(const Batch& b, const PruneRegion* regions, uint32_t* sol
 void launch_rotate_vertices(const float* V, float* R, uint32_t n, double a, double b, cudaStream_t s,
                             uint32_t* launches);
 void launch_emit_raw(int nodeKind, const Batch& b, uint64_t totalWords, const uint32_t* fill, const uint32_t* surf,
-                     const uint32_t* ranks, const void* keys, uint32_t keysCap, cudaStream_t s, uint32_t* launches);
+                     const WordRank* ranks, const void* keys, uint32_t keysCap, cudaStream_t s, uint32_t* launches);
 void launch_unrotate(const void* in, void* out, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nodeBytes,
                      cudaStream_t s, uint32_t* launches);
 void launch_id_pass(void* nodes, uint32_t X, uint32_t Y, uint32_t Z, uint32_t nodeBytes, uint32_t idMask,
@@ -187,7 +195,7 @@ void launch_fcc_boundaries(void* nodes, uint32_t X, uint32_t Y, uint32_t Z, uint
 // Words [wordBegin, totalWords) of the arena (wordBegin a multiple of 32).
 void launch_emit_cartesian(int nodeKind, const Batch& b, uint64_t wordBegin, uint64_t totalWords,
                            const uint32_t* finalSolid,
-                           const uint32_t* fill, const uint32_t* surf, const uint32_t* ranks, const void* keys,
+                           const uint32_t* fill, const uint32_t* surf, const WordRank* ranks, const void* keys,
                            uint32_t keysCap, uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches);
 
 // An FCC mesh: its four sub-lattice units are units [unit0, unit0 + 4).
@@ -200,7 +208,7 @@ struct FccMesh {
 // solid bit, the surface material), for slices along x.
 void launch_emit_fcc(int nodeKind, const Batch& b, const FccMesh* meshes, const uint64_t* groupBase,
                      uint32_t nMeshes, uint64_t totalGroups, const uint32_t* fill, const uint32_t* surf,
-                     const uint32_t* ranks, const void* keys, uint32_t keysCap, bool raw, cudaStream_t s,
+                     const WordRank* ranks, const void* keys, uint32_t keysCap, bool raw, cudaStream_t s,
                      uint32_t* launches);
 
 }  // namespace vxb

@@ -275,7 +275,7 @@ struct EmitArgs {
     const uint32_t* fin;     // pruned solid arena
     const uint32_t* fill;    // parity fill arena (unpruned)
     const uint32_t* surf;    // surface arena
-    const uint32_t* ranks;   // exclusive popcount prefix of surf words (arena-wide)
+    const WordRank* ranks;   // surface words with their ranks (arena-wide)
     const void* keys;        // merged material keys by rank
     uint32_t keysCap;        // keys past it read as 0
 };
@@ -461,7 +461,7 @@ __global__ void __launch_bounds__(256, 6) emitNarrowKernel(EmitArgs a, uint64_t 
         }
         if (sm) {
             const uint32_t* keys = reinterpret_cast<const uint32_t*>(a.keys);
-            const uint32_t rank0 = __ldg(a.ranks + uBase + w);
+            const uint32_t rank0 = a.ranks[uBase + w].rank;
             if (sm == 0xFFFFFFFFu && (uint64_t)rank0 + 32u <= a.keysCap) {
                 // 32 surface nodes: their keys are the 32 from rank0 on.
 #pragma unroll 8
@@ -518,7 +518,7 @@ __global__ void __launch_bounds__(256) emitPartialKernel(EmitArgs a, uint64_t wo
             for (int i = 0; i < 16; ++i) out[i] = make_uint4(0, 0, 0, 0);
             continue;
         }
-        uint32_t matRank = n.s0 ? __ldg(a.ranks + U.wordBase + w) : 0u;
+        uint32_t matRank = n.s0 ? a.ranks[U.wordBase + w].rank : 0u;
         // Node coordinates of the word's first node (ratio of surface nodes).
         const int x0 = (int)(w % U.g.ipx) * 32, y0 = (int)(w / U.g.ipx % U.g.AY), z0 = (int)(w / U.g.ipx / U.g.AY);
 #pragma unroll
@@ -557,7 +557,7 @@ struct FccArgs {
     uint32_t nMeshes;
     const uint32_t* fill;
     const uint32_t* surf;
-    const uint32_t* ranks;
+    const WordRank* ranks;
     const void* keys;
     uint32_t keysCap;
     uint32_t raw;   // nodes before the boundaries: id = solid bit, no face clearing
@@ -647,7 +647,7 @@ __global__ void emitFccKernel(FccArgs A, uint64_t totalGroups) {
             uint32_t mat = 0;
             if (sb) {
                 const uint32_t bt = x & 31u;
-                const uint32_t r = __ldg(A.ranks + G.wordBase[gt] + w) + (bt ? __popc(sw >> (32 - bt)) : 0u);
+                const uint32_t r = A.ranks[G.wordBase[gt] + w].rank + (bt ? __popc(sw >> (32 - bt)) : 0u);
                 mat = r < A.keysCap ? NT::keyMat(reinterpret_cast<const uint32_t*>(A.keys)[r]) : 0u;
             }
             // zeroPadding of an FCC device space with neighbours
@@ -703,7 +703,7 @@ void launch_prune_list(const Batch& b, const PruneRegion* regions, uint32_t* sol
 
 void launch_emit_cartesian(int nodeKind, const Batch& b, uint64_t wordBegin, uint64_t totalWords,
                            const uint32_t* finalSolid,
-                           const uint32_t* fill, const uint32_t* surf, const uint32_t* ranks, const void* keys,
+                           const uint32_t* fill, const uint32_t* surf, const WordRank* ranks, const void* keys,
                            uint32_t keysCap, uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches) {
     EmitArgs a;
     a.keysCap = keysCap;
@@ -725,7 +725,7 @@ void launch_emit_cartesian(int nodeKind, const Batch& b, uint64_t wordBegin, uin
 
 void launch_emit_fcc(int nodeKind, const Batch& b, const FccMesh* meshes, const uint64_t* groupBase,
                      uint32_t nMeshes, uint64_t totalGroups, const uint32_t* fill, const uint32_t* surf,
-                     const uint32_t* ranks, const void* keys, uint32_t keysCap, bool raw, cudaStream_t s,
+                     const WordRank* ranks, const void* keys, uint32_t keysCap, bool raw, cudaStream_t s,
                      uint32_t* launches) {
     FccArgs A;
     A.keysCap = keysCap;

@@ -302,7 +302,7 @@ int Pipeline::prepare(const std::vector<MeshJob>& jobs, cudaStream_t s) {
         if ((rc = sOffsets.ensure(4 * ((size_t)nWork_ + 2)))) return rc;
         if ((rc = sTileSums.ensure(4 * ((size_t)nWork_ / 4096 + 2)))) return rc;
         if ((rc = surf.ensure(wordBytes))) return rc;
-        if ((rc = ranks.ensure(wordBytes))) return rc;
+        if ((rc = ranks.ensure(2 * wordBytes))) return rc;
         if ((rc = rankTiles.ensure(4 * ((size_t)totalWords_ / 2048 + 2)))) return rc;
         if ((rc = codes.ensure(4 * (size_t)nWork_))) return rc;
         if ((rc = unitCounts.ensure(4 * (size_t)nWork_))) return rc;
@@ -368,14 +368,14 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
         tuneMark(kKnobSurfaceSpan, false, ss);
         tuneMark(kKnobSurface, false, ss);
         launch_surface_work(nodeKind_, retraverse ? 2 : 0, wide_ ? 1 : 0, b, recs.p, ovl.p, sOffsets.as<uint32_t>(), nWork_,
-                            st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(),
+                            st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<WordRank>(),
                             keys.p, keysCap_, hitList.as<unsigned long long>(), st + kHitCount, listCap_,
                             shape.surfBlocksPerSm, shape.surfBatch, shape.surfQueue ? st + kSurfQueue : nullptr, ss,
                             &launches);
         tuneMark(kKnobSurface, true, ss);
         if (timer) timer->mark(5, true, ss);
         VXB_CUDA(cudaEventRecord(evSurfBits_, ss));
-        launch_surface_rank(surf.as<uint32_t>(), totalWords_, ranks.as<uint32_t>(), rankTiles.as<uint32_t>(),
+        launch_surface_rank(surf.as<uint32_t>(), totalWords_, ranks.as<WordRank>(), rankTiles.as<uint32_t>(),
                             st + kSurfaceVoxels, ss, &launches);
         if (timer) timer->mark(1, true, ss);
         // Material keys by surface rank (independent of pruning).
@@ -383,12 +383,11 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
         launch_surface_keys_zero(keys.p, st + kSurfaceVoxels, keysCap_, wide_ ? 1 : 0, ss, &launches);
         tuneMark(kKnobMerge, false, ss);
         if (!retraverse)
-            launch_surface_merge(hitList.as<unsigned long long>(), st + kHitCount, listCap_, surf.as<uint32_t>(),
-                                  ranks.as<uint32_t>(), keys.as<uint32_t>(), keysCap_, shape.mergeBlocksPerSm, ss,
-                                  &launches);
+            launch_surface_merge(hitList.as<unsigned long long>(), st + kHitCount, listCap_, ranks.as<WordRank>(),
+                                 keys.as<uint32_t>(), keysCap_, shape.mergeBlocksPerSm, ss, &launches);
         else
             launch_surface_work(nodeKind_, 1, wide_ ? 1 : 0, b, recs.p, ovl.p, sOffsets.as<uint32_t>(), nWork_,
-                                st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(),
+                                st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<WordRank>(),
                                 keys.p, keysCap_, nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch,
                                 shape.surfQueue ? st + kSurfQueue : nullptr, ss, &launches);
         tuneMark(kKnobMerge, true, ss);
@@ -454,7 +453,7 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
     // Node emission.
     mark(3, false);
     if (raw_ && anyCartesian_)
-        launch_emit_raw(nodeKind_, b, totalWords_, fillP, surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_,
+        launch_emit_raw(nodeKind_, b, totalWords_, fillP, surf.as<uint32_t>(), ranks.as<WordRank>(), keys.p, keysCap_,
                         s, &launches);
     else if (anyCartesian_) {
         tuneMark(kKnobEmit, false, s);
@@ -470,7 +469,7 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
                 const uint64_t w1 = k + 1 == kOutChunks ? words : (words * (k + 1) / kOutChunks) & ~uint64_t(31);
                 if (w1 <= w0) continue;
                 launch_emit_cartesian(nodeKind_, b, w0, w1, fin.as<uint32_t>(), fillP, surf.as<uint32_t>(),
-                                      ranks.as<uint32_t>(), keys.p, keysCap_, shape.emitBlocksPerSm, s, &launches);
+                                      ranks.as<WordRank>(), keys.p, keysCap_, shape.emitBlocksPerSm, s, &launches);
                 if (!outEv_[k]) VXB_CUDA(cudaEventCreateWithFlags(&outEv_[k], cudaEventDisableTiming));
                 VXB_CUDA(cudaEventRecord(outEv_[k], s));
                 VXB_CUDA(cudaStreamWaitEvent(copyStream_, outEv_[k], 0));
@@ -481,14 +480,14 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
             hostCopied_ = true;
         } else {
             launch_emit_cartesian(nodeKind_, b, 0, totalWords_, fin.as<uint32_t>(), fillP, surf.as<uint32_t>(),
-                                  ranks.as<uint32_t>(), keys.p, keysCap_, shape.emitBlocksPerSm, s, &launches);
+                                  ranks.as<WordRank>(), keys.p, keysCap_, shape.emitBlocksPerSm, s, &launches);
         }
         tuneMark(kKnobEmit, true, s);
     }
     if (nFcc_)
         launch_emit_fcc(nodeKind_, b, reinterpret_cast<const FccMesh*>(tables.as<uint8_t>() + oFcc_),
                         reinterpret_cast<const uint64_t*>(tables.as<uint8_t>() + oGroupBase_), nFcc_, totalGroups_,
-                        fillP, surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_, raw_, s, &launches);
+                        fillP, surf.as<uint32_t>(), ranks.as<WordRank>(), keys.p, keysCap_, raw_, s, &launches);
     mark(3, true);
     VXB_CUDA(cudaGetLastError());
     return 0;
@@ -600,7 +599,7 @@ int Pipeline::finish(cudaStream_t s) {
             }
             launch_surface_keys_zero(keys.p, st + kSurfaceVoxels, keysCap_, wide_ ? 1 : 0, s, &launches);
             launch_surface_work(nodeKind_, 1, wide_ ? 1 : 0, b, recs.p, ovl.p, sOffsets.as<uint32_t>(), nWork_,
-                                st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<uint32_t>(),
+                                st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<WordRank>(),
                                 keys.p, keysCap_, nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch,
                                 shape.surfQueue ? st + kSurfQueue : nullptr, s, &launches);
             reemit = true;
@@ -627,15 +626,15 @@ int Pipeline::finish(cudaStream_t s) {
     }
     if (reemit) {
         if (raw_ && anyCartesian_)
-            launch_emit_raw(nodeKind_, b, totalWords_, fillP, surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p,
+            launch_emit_raw(nodeKind_, b, totalWords_, fillP, surf.as<uint32_t>(), ranks.as<WordRank>(), keys.p,
                             keysCap_, s, &launches);
         else if (anyCartesian_)
             launch_emit_cartesian(nodeKind_, b, 0, totalWords_, fin.as<uint32_t>(), fillP, surf.as<uint32_t>(),
-                                  ranks.as<uint32_t>(), keys.p, keysCap_, shape.emitBlocksPerSm, s, &launches);
+                                  ranks.as<WordRank>(), keys.p, keysCap_, shape.emitBlocksPerSm, s, &launches);
         if (nFcc_)
             launch_emit_fcc(nodeKind_, b, reinterpret_cast<const FccMesh*>(tables.as<uint8_t>() + oFcc_),
                             reinterpret_cast<const uint64_t*>(tables.as<uint8_t>() + oGroupBase_), nFcc_,
-                            totalGroups_, fillP, surf.as<uint32_t>(), ranks.as<uint32_t>(), keys.p, keysCap_, raw_, s,
+                            totalGroups_, fillP, surf.as<uint32_t>(), ranks.as<WordRank>(), keys.p, keysCap_, raw_, s,
                             &launches);
         VXB_CUDA(cudaGetLastError());
         VXB_CUDA(cudaStreamSynchronize(s));

@@ -374,7 +374,7 @@ struct UnitGrid {
 // mode 2: set the bit only (a mode-1 traversal merges the keys).
 struct Sink {
     uint32_t* bits;            // surface arena
-    const uint32_t* wordRank;  // exclusive popcount prefix per word (mode 1)
+    const WordRank* wordRank;  // complete surface words with their ranks (mode 1)
     void* keys;                // compact key array (mode 1)
     uint32_t keysCap;          // keys at ranks past it are dropped
     unsigned long long* list;
@@ -403,8 +403,8 @@ struct Sink {
                 if (gat < listCap) list[gat] = e;
             }
         } else {
-            const uint32_t word = __ldg(bits + w);
-            const uint32_t r = __ldg(wordRank + w) + (b ? __popc(word >> (32 - b)) : 0u);
+            const WordRank wr = wordRank[w];
+            const uint32_t r = wr.rank + (b ? __popc(wr.bits >> (32 - b)) : 0u);
             if (r >= keysCap) return;
             if (wide) atomicMax(reinterpret_cast<unsigned long long*>(keys) + r, (unsigned long long)key);
             else atomicMax(reinterpret_cast<uint32_t*>(keys) + r, (uint32_t)key);
@@ -665,22 +665,23 @@ constexpr uint32_t kRankTile = kBlock * kRankItems;
 // the ranks (tile offset plus the block's exclusive scan).  The words were
 // just written by the surface pass and are read from L2 where they stay.
 template <bool kApply>
-__global__ void rankTileKernel(const uint32_t* __restrict__ words, uint64_t n, uint32_t* __restrict__ ranks,
+__global__ void rankTileKernel(const uint32_t* __restrict__ words, uint64_t n, WordRank* __restrict__ ranks,
                                uint32_t* __restrict__ tileSums) {
     __shared__ uint32_t warpSums[33];
     const uint64_t base = (uint64_t)blockIdx.x * kRankTile + (uint64_t)threadIdx.x * kRankItems;
     const bool whole = base + kRankItems <= n;   // 32-byte aligned: kRankItems words per thread
-    uint32_t c[kRankItems];
+    uint32_t x[kRankItems], c[kRankItems];
     if (whole) {
         const uint4 a = __ldg(reinterpret_cast<const uint4*>(words + base));
         const uint4 b = __ldg(reinterpret_cast<const uint4*>(words + base) + 1);
-        const uint32_t x[kRankItems] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-#pragma unroll
-        for (int i = 0; i < kRankItems; ++i) c[i] = (uint32_t)__popc(x[i]);
+        x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+        x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
     } else {
 #pragma unroll
-        for (int i = 0; i < kRankItems; ++i) c[i] = base + i < n ? (uint32_t)__popc(__ldg(words + base + i)) : 0u;
+        for (int i = 0; i < kRankItems; ++i) x[i] = base + i < n ? __ldg(words + base + i) : 0u;
     }
+#pragma unroll
+    for (int i = 0; i < kRankItems; ++i) c[i] = (uint32_t)__popc(x[i]);
     uint32_t sum = 0;
 #pragma unroll
     for (int i = 0; i < kRankItems; ++i) sum += c[i];
@@ -717,12 +718,13 @@ __global__ void rankTileKernel(const uint32_t* __restrict__ words, uint64_t n, u
         ex += c[i];
     }
     if (whole) {
-        reinterpret_cast<uint4*>(ranks + base)[0] = make_uint4(r[0], r[1], r[2], r[3]);
-        reinterpret_cast<uint4*>(ranks + base)[1] = make_uint4(r[4], r[5], r[6], r[7]);
+        uint4* out = reinterpret_cast<uint4*>(ranks + base);
+#pragma unroll
+        for (int i = 0; i < kRankItems; i += 2) out[i / 2] = make_uint4(x[i], r[i], x[i + 1], r[i + 1]);
     } else {
 #pragma unroll
         for (int i = 0; i < kRankItems; ++i)
-            if (base + i < n) ranks[base + i] = r[i];
+            if (base + i < n) ranks[base + i] = WordRank{x[i], r[i]};
     }
 }
 
@@ -768,35 +770,36 @@ __global__ void zeroKeysKernel(void* keys, const uint32_t* __restrict__ countPtr
     }
 }
 
-// Max-merges the hit list into the rank-indexed key array.
+// Max-merges the hit list into the rank-indexed key array.  Each thread
+// takes two pairs of consecutive entries (16-byte loads) per iteration, so
+// the scattered word / rank loads of four entries overlap; one 8-byte load
+// gives an entry's surface word and rank.
 __global__ void mergeKeysKernel(const unsigned long long* __restrict__ list, const uint32_t* __restrict__ countPtr,
-                                uint32_t cap, const uint32_t* __restrict__ bits, const uint32_t* __restrict__ ranks,
-                                uint32_t* keys, uint32_t keysCap) {
-    // Four independent entries per thread and iteration: the scattered
-    // loads of one entry overlap those of the others.
-    constexpr int U = 4;
+                                uint32_t cap, const WordRank* __restrict__ ranks, uint32_t* keys, uint32_t keysCap) {
+    constexpr int U = 2;   // entry pairs per thread and iteration
     const uint32_t n = min(*countPtr, cap);
+    const uint32_t pairs = (n + 1) / 2;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += U * stride) {
-        unsigned long long e[U];
+    const ulonglong2* list2 = reinterpret_cast<const ulonglong2*>(list);
+    for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < pairs; i0 += U * stride) {
+        unsigned long long e[2 * U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const uint32_t i = i0 + u * stride;
-            e[u] = i < n ? list[i] : ~0ull;
+            ulonglong2 q = make_ulonglong2(~0ull, ~0ull);
+            if (i < pairs) q = list2[i];
+            e[2 * u] = q.x;
+            e[2 * u + 1] = 2 * i + 1 < n ? q.y : ~0ull;
         }
-        uint32_t word[U], rk[U];
+        WordRank wr[2 * U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            if (e[u] == ~0ull) continue;
-            const uint64_t w = (e[u] >> 24) >> 5;
-            word[u] = __ldg(bits + w);
-            rk[u] = __ldg(ranks + w);
-        }
+        for (int u = 0; u < 2 * U; ++u)
+            if (e[u] != ~0ull) wr[u] = ranks[(e[u] >> 24) >> 5];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
+        for (int u = 0; u < 2 * U; ++u) {
             if (e[u] == ~0ull) continue;
             const uint32_t b = (uint32_t)((e[u] >> 24) & 31u);
-            const uint32_t r = rk[u] + (b ? __popc(word[u] >> (32 - b)) : 0u);
+            const uint32_t r = wr[u].rank + (b ? __popc(wr[u].bits >> (32 - b)) : 0u);
             if (r < keysCap) atomicMax(keys + r, (uint32_t)(e[u] & 0xFFFFFFull));
         }
     }
@@ -828,7 +831,7 @@ static void launchSurfaceWorkKind(uint32_t batch, uint32_t grid, const Sink& sin
 
 void launch_surface_work(int kind, int mode, int wide, const Batch& b, const void* recs, const void* ovl,
                          const uint32_t* offsets, uint32_t nWork, const uint32_t* total, const uint32_t* buckets,
-                         uint32_t* surf, const uint32_t* ranks, void* keys, uint32_t keysCap,
+                         uint32_t* surf, const WordRank* ranks, void* keys, uint32_t keysCap,
                          unsigned long long* list, uint32_t* listCount, uint32_t listCap, uint32_t blocksPerSm,
                          uint32_t batch, uint32_t* queue, cudaStream_t s, uint32_t* launches) {
     if (queue) cudaMemsetAsync(queue, 0, sizeof(uint32_t), s);
@@ -861,7 +864,7 @@ void launch_surface_work(int kind, int mode, int wide, const Batch& b, const voi
     *launches += 1;
 }
 
-void launch_surface_rank(const uint32_t* bits, uint64_t words, uint32_t* ranks, uint32_t* tileSums, uint32_t* total,
+void launch_surface_rank(const uint32_t* bits, uint64_t words, WordRank* ranks, uint32_t* tileSums, uint32_t* total,
                          cudaStream_t s, uint32_t* launches) {
     const uint32_t tiles = (uint32_t)((words + kRankTile - 1) / kRankTile);
     rankTileKernel<false><<<tiles ? tiles : 1, kBlock, 0, s>>>(bits, words, ranks, tileSums);
@@ -877,9 +880,9 @@ void launch_surface_keys_zero(void* keys, const uint32_t* count, uint32_t cap, i
 }
 
 void launch_surface_merge(const unsigned long long* list, const uint32_t* listCount, uint32_t listCap,
-                          const uint32_t* bits, const uint32_t* ranks, uint32_t* keys, uint32_t keysCap,
+                          const WordRank* ranks, uint32_t* keys, uint32_t keysCap,
                           uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches) {
-    mergeKeysKernel<<<148u * blocksPerSm, 256, 0, s>>>(list, listCount, listCap, bits, ranks, keys, keysCap);
+    mergeKeysKernel<<<148u * blocksPerSm, 256, 0, s>>>(list, listCount, listCap, ranks, keys, keysCap);
     *launches += 1;
 }
 

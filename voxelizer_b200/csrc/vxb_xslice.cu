@@ -40,7 +40,7 @@ __global__ void rotateKernel(const float* __restrict__ V, float* __restrict__ R,
 // Nodes before the boundary ids, one thread per 32-node word of the unit.
 template <int K>
 __global__ void emitRawKernel(Batch b, uint64_t totalWords, const uint32_t* __restrict__ fill,
-                              const uint32_t* __restrict__ surf, const uint32_t* __restrict__ ranks, const void* keys,
+                              const uint32_t* __restrict__ surf, const WordRank* __restrict__ ranks, const void* keys,
                               uint32_t keysCap) {
     typedef NodeT<K> NT;
     for (uint64_t gw = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gw < totalWords;
@@ -51,7 +51,7 @@ __global__ void emitRawKernel(Batch b, uint64_t totalWords, const uint32_t* __re
         if (w >= U.g.ipx * U.g.AY * U.g.AZ) continue;
         const uint32_t f = __ldg(fill + U.wordBase + w);
         const uint32_t s = U.materials ? __ldg(surf + U.wordBase + w) : 0u;
-        uint32_t rank = s ? __ldg(ranks + U.wordBase + w) : 0u;
+        uint32_t rank = s ? ranks[U.wordBase + w].rank : 0u;
         const int x0 = (int)(w % U.g.ipx) * 32, y0 = (int)(w / U.g.ipx % U.g.AY), z0 = (int)(w / U.g.ipx / U.g.AY);
         uint8_t* out = static_cast<uint8_t*>(U.out) + (size_t)w * 32 * NT::bytes;
         for (uint32_t bt = 0; bt < 32; ++bt) {
@@ -193,7 +193,7 @@ void launch_rotate_vertices(const float* V, float* R, uint32_t n, double a, doub
 }
 
 void launch_emit_raw(int nodeKind, const Batch& b, uint64_t totalWords, const uint32_t* fill, const uint32_t* surf,
-                     const uint32_t* ranks, const void* keys, uint32_t keysCap, cudaStream_t s, uint32_t* launches) {
+                     const WordRank* ranks, const void* keys, uint32_t keysCap, cudaStream_t s, uint32_t* launches) {
     const uint32_t grid = gridFor(totalWords, 128, 148u * 8u);
     switch (nodeKind) {
     case kShort: emitRawKernel<kShort><<<grid, 128, 0, s>>>(b, totalWords, fill, surf, ranks, keys, keysCap); break;
