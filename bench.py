@@ -718,6 +718,7 @@ def main():
         vx.voxelize_device(1, MAX_DIM, out, stream=sh)
         for k, v in vx.stage_times().items():
             stage_acc.setdefault(k, []).append(v)
+        timeline = vx.stage_timeline()
     vx.set_profiling(False)
     stream.synchronize()
 
@@ -778,6 +779,7 @@ def main():
                               "achieved": round(path_bytes / (ms * 1e-3) / 1e9, 1),
                               "frac": round(path_bytes / (ms * 1e-3) / 1e9 / peak, 4)},
             "stages_ms": {k: round(sorted(v)[len(v) // 2], 4) for k, v in stage_acc.items()},
+            "stage_timeline_ms": {k: [round(a, 3), round(b, 3)] for k, (a, b) in timeline.items() if a == a},
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "ms_per_step": round(e2e, 3),
                     "h2d_bytes_per_step": int(12 * mesh.n_vertices + 13 * mesh.n_triangles),
                     "d2h_bytes_per_step": int(info.bytes)},

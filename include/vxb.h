@@ -225,6 +225,12 @@ vxb_status vxb_last_stats(vxb_voxelizer* v, vxb_stats* stats);
  * milliseconds of up to n stages (-1 for a stage that did not run). */
 vxb_status vxb_set_profiling(vxb_voxelizer* v, int enable);
 vxb_status vxb_stage_times(vxb_voxelizer* v, float* ms, uint32_t n);
+/* The same stages on one time axis: start_end[2k] and start_end[2k + 1] are
+ * the start and end of stage k in milliseconds after the start of stage 0
+ * (negative for work queued on the second stream before it), NaN for a
+ * stage that did not run.  Shows how the surface stages overlap the solid
+ * and pruning stages. */
+vxb_status vxb_stage_timeline(vxb_voxelizer* v, float* start_end, uint32_t n);
 
 /* Batches (no reference counterpart; the reference voxelizes one mesh per
  * call).  A batch runs the meshes of several voxelizers through one sequence

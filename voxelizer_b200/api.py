@@ -196,6 +196,13 @@ class Voxelizer:
         check(lib().vxb_stage_times(self._h, buf, len(self.STAGES)))
         return dict(zip(self.STAGES, [float(x) for x in buf]))
 
+    def stage_timeline(self):
+        """(start, end) in ms after the solid stage's start, per stage of the
+        last call (NaN: stage did not run)."""
+        buf = (ctypes.c_float * (2 * len(self.STAGES)))()
+        check(lib().vxb_stage_timeline(self._h, buf, len(self.STAGES)))
+        return {k: (float(buf[2 * i]), float(buf[2 * i + 1])) for i, k in enumerate(self.STAGES)}
+
     def last_launch_count(self):
         n = ctypes.c_uint32()
         check(lib().vxb_last_launch_count(self._h, ctypes.byref(n)))

@@ -49,8 +49,6 @@ struct Unit {
     void* out;            // node output (Cartesian units)
 };
 
-// Device tables of a batch.  Bases have nUnits + 1 entries (the last one is
-// the total), so that the unit of an element is a binary search away.
 // A surface word and the rank of its first surface voxel (the exclusive
 // popcount prefix of the surface words before it, arena-wide), side by side
 // so that one 8-byte load gives both.
@@ -58,6 +56,8 @@ struct __align__(8) WordRank {
     uint32_t bits, rank;
 };
 
+// Device tables of a batch.  Bases have nUnits + 1 entries (the last one is
+// the total), so that the unit of an element is a binary search away.
 struct Batch {
     const Unit* units;
     uint32_t nUnits;
