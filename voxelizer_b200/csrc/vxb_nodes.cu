@@ -434,8 +434,10 @@ __global__ void __launch_bounds__(256, 6) emitNarrowKernel(EmitArgs a, uint64_t 
             zero = borderMask(uw, w);
         }
         // Ids: none, all 27 (every node solid with six solid neighbours), or
-        // the bit-sliced planes.  Materials of surface nodes follow by rank.
+        // the bit-sliced planes.  Materials of surface nodes follow by rank
+        // (the rank is loaded first, so that its latency overlaps the ids).
         const uint32_t cm = n.c & ~zero, sm = n.s0 & ~zero;
+        const uint32_t rank0 = sm ? a.ranks[uBase + w].rank : 0u;
         if (cm == 0u || (cm & n.L & n.R & n.In & n.Out & n.Dn & n.Up) == 0xFFFFFFFFu) {
             const uint32_t rep = cm == 0u ? 0u : NB == 1 ? v27 * 0x01010101u : v27 * 0x00010001u;
 #pragma unroll
@@ -461,7 +463,6 @@ __global__ void __launch_bounds__(256, 6) emitNarrowKernel(EmitArgs a, uint64_t 
         }
         if (sm) {
             const uint32_t* keys = reinterpret_cast<const uint32_t*>(a.keys);
-            const uint32_t rank0 = a.ranks[uBase + w].rank;
             if (sm == 0xFFFFFFFFu && (uint64_t)rank0 + 32u <= a.keysCap) {
                 // 32 surface nodes: their keys are the 32 from rank0 on.
 #pragma unroll 8
@@ -471,14 +472,31 @@ __global__ void __launch_bounds__(256, 6) emitNarrowKernel(EmitArgs a, uint64_t 
                     else my[2 * j + 1] = (uint8_t)mat;
                 }
             } else {
+                // Four surface nodes per step, so that their key loads are
+                // in flight together.
+                constexpr int kKeys = 4;
                 uint32_t rest = sm;
                 do {
-                    const uint32_t bt = __clz(rest);       // node index in the word
-                    const uint32_t r = rank0 + (bt ? __popc(n.s0 >> (32u - bt)) : 0u);
-                    const uint32_t mat = r < a.keysCap ? NT::keyMat(__ldg(keys + r)) : 0u;
-                    if (NB == 1) my[bt] |= (uint8_t)(mat << 5);
-                    else my[2 * bt + 1] = (uint8_t)mat;
-                    rest &= ~(0x80000000u >> bt);
+                    uint32_t bt[kKeys], mat[kKeys];
+#pragma unroll
+                    for (int q = 0; q < kKeys; ++q) {
+                        bt[q] = 32u;
+                        if (rest) {
+                            bt[q] = __clz(rest);       // node index in the word
+                            rest &= ~(0x80000000u >> bt[q]);
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < kKeys; ++q) {
+                        const uint32_t r = rank0 + (bt[q] ? __popc(n.s0 >> (32u - bt[q])) : 0u);
+                        mat[q] = bt[q] < 32u && r < a.keysCap ? NT::keyMat(__ldg(keys + r)) : 0u;
+                    }
+#pragma unroll
+                    for (int q = 0; q < kKeys; ++q) {
+                        if (bt[q] == 32u) break;
+                        if (NB == 1) my[bt[q]] |= (uint8_t)(mat[q] << 5);
+                        else my[2 * bt[q] + 1] = (uint8_t)mat[q];
+                    }
                 } while (rest);
             }
         }
