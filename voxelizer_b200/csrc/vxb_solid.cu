@@ -173,42 +173,56 @@ __device__ __forceinline__ void solidCandidate(const SolidStage& st, const Batch
     }
     const uint32_t nty = (hi[0] - 1) / 4 - lo[0] / 4 + 1;
     const uint32_t tileY = lo[0] / 4 + local % nty, tileZ = lo[1] / 4 + local / nty;
+    // Unfused edge functions (the pinned forms of E_BIN and E_GEN) keep the
+    // product of the row's coordinate across the row: the same operations
+    // in the same order as evaluating each centre from scratch.
+    static_assert(site::E_BIN == 0 && site::E_GEN == 0, "row products assume the unfused edge forms");
     bool member = false;
     for (uint32_t iy = tileY * 4; iy < tileY * 4 + 4 && iy < hi[0] && !member; ++iy) {
         if (iy < lo[0]) continue;
         const double py = lin<site::P_BIN>((double)iy, d, g.mn[1]);
+        double ry[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) ry[k] = __dmul_rn(st.bnx[k], py);
         for (uint32_t iz = tileZ * 4; iz < tileZ * 4 + 4 && iz < hi[1]; ++iz) {
             if (iz < lo[1]) continue;
             const double pz = lin<site::P_BIN>((double)iz, d, g.mn[2]);
             bool ok = true;
 #pragma unroll
-            for (int k = 0; k < 3; ++k) ok &= sum2p1<site::E_BIN>(st.bnx[k], py, st.bny[k], pz, st.bd[k]) >= 0.0;
+            for (int k = 0; k < 3; ++k) ok &= __dadd_rn(__dadd_rn(ry[k], __dmul_rn(st.bny[k], pz)), st.bd[k]) >= 0.0;
             if (ok) { member = true; break; }
         }
     }
     if (!member) return;
     const D3* v = st.b.v;
-    for (uint32_t c = 0; c < 16; ++c) {
-        const uint32_t vz = tileZ * 4 + c / 4, vy = tileY * 4 + c % 4;
-        if (vy < sp.y0 || vy >= sp.y1 || vz < sp.z0 || vz >= sp.z1) continue;
-        const double py = lin<site::P_GEN>((double)vy, d, g.mn[1]);
+    for (uint32_t cz = 0; cz < 4; ++cz) {
+        const uint32_t vz = tileZ * 4 + cz;
+        if (vz < sp.z0 || vz >= sp.z1) continue;
         const double pz = lin<site::P_GEN>((double)vz, d, g.mn[2]);
-        int pass = 0;
+        double rz[3];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            double r = sum2p1<site::E_GEN>(st.ex[i], py, st.ey[i], pz, st.ed[i]);
-            if ((st.tl >> i) & 1u) r = __dadd_rn(r, kDblMin);
-            pass += r > 0.0;
+        for (int i = 0; i < 3; ++i) rz[i] = __dmul_rn(st.ey[i], pz);
+        for (uint32_t cy = 0; cy < 4; ++cy) {
+            const uint32_t vy = tileY * 4 + cy;
+            if (vy < sp.y0 || vy >= sp.y1) continue;
+            const double py = lin<site::P_GEN>((double)vy, d, g.mn[1]);
+            int pass = 0;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                double r = __dadd_rn(__dadd_rn(__dmul_rn(st.ex[i], py), rz[i]), st.ed[i]);
+                if ((st.tl >> i) & 1u) r = __dadd_rn(r, kDblMin);
+                pass += r > 0.0;
+            }
+            if (pass != 3) continue;
+            const double ax = __dsub_rn(v[0].x, g.mn[0]), ay = __dsub_rn(v[0].y, py), az = __dsub_rn(v[0].z, pz);
+            const double B = sum3<site::B_GEN>(ax, st.n.x, ay, st.n.y, az, st.n.z);
+            double px = __ddiv_rn(B, st.n.x);
+            px = px < 0.0 ? 0.0 : px;
+            const uint32_t vx = __double2uint_rz(ceil(__ddiv_rn(px, d))) + 1u;
+            if (vx >= g.X) continue;
+            const uint32_t row = (vz + g.padZ) * g.AY + (vy + g.padY);
+            atomicXor(toggles + (size_t)row * g.ipx + (vx >> 5), 0x80000000u >> (vx & 31u));
         }
-        if (pass != 3) continue;
-        const double ax = __dsub_rn(v[0].x, g.mn[0]), ay = __dsub_rn(v[0].y, py), az = __dsub_rn(v[0].z, pz);
-        const double B = sum3<site::B_GEN>(ax, st.n.x, ay, st.n.y, az, st.n.z);
-        double px = __ddiv_rn(B, st.n.x);
-        px = px < 0.0 ? 0.0 : px;
-        const uint32_t vx = __double2uint_rz(ceil(__ddiv_rn(px, d))) + 1u;
-        if (vx >= g.X) continue;
-        const uint32_t row = (vz + g.padZ) * g.AY + (vy + g.padY);
-        atomicXor(toggles + (size_t)row * g.ipx + (vx >> 5), 0x80000000u >> (vx & 31u));
     }
 }
 
