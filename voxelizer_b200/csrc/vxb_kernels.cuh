@@ -94,12 +94,11 @@ constexpr size_t kSurfRecBytes = 64;
 constexpr size_t kSurfOvlBytes = 112;
 
 // Classify (codes / units in work-triangle order, per-bucket counts in
-// buckets[0..9)), partition (perm, unitsP in partitioned order;
-// buckets[9..18) are cursors) and set up (records) the work triangles of
-// units with materials.  buckets and unitsP[0..nWork] must be zero on entry.
+// buckets[0..9)), then partition (unitsP in partitioned order; buckets[9..18)
+// are cursors) and set up (records) the work triangles of units with
+// materials.  buckets and unitsP[0..nWork] must be zero on entry.
 void launch_surface_prepare(const Batch& b, uint32_t nWork, uint32_t* codes, uint32_t* units, uint32_t* buckets,
-                            uint32_t* perm, uint32_t* unitsP, void* recs, void* ovl, cudaStream_t s,
-                            uint32_t* launches);
+                            uint32_t* unitsP, void* recs, void* ovl, cudaStream_t s, uint32_t* launches);
 // Surface work over the exclusive scan `offsets` of unitsP (nWork + 1
 // entries), one thread per column.  mode 0: set bits in the `surf` arena and
 // append (bit position << 24 | key) to `list` (entries past listCap are

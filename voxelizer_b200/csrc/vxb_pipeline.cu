@@ -306,7 +306,6 @@ int Pipeline::prepare(const std::vector<MeshJob>& jobs, cudaStream_t s) {
         if ((rc = rankTiles.ensure(4 * ((size_t)totalWords_ / 2048 + 2)))) return rc;
         if ((rc = codes.ensure(4 * (size_t)nWork_))) return rc;
         if ((rc = unitCounts.ensure(4 * (size_t)nWork_))) return rc;
-        if ((rc = perm.ensure(4 * (size_t)nWork_))) return rc;
         if ((rc = buckets.ensure(4 * 2 * kSurfaceBuckets))) return rc;
         if ((rc = recs.ensure(kSurfRecBytes * (size_t)nWork_))) return rc;
         if ((rc = ovl.ensure(kSurfOvlBytes * (size_t)nWork_))) return rc;
@@ -357,7 +356,7 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
         VXB_CUDA(cudaMemsetAsync(sCounts.p, 0, 4 * ((size_t)nWork_ + 1), ss));
         VXB_CUDA(cudaMemsetAsync(st + kHitCount, 0, 4, ss));
         launch_surface_prepare(b, nWork_, codes.as<uint32_t>(), unitCounts.as<uint32_t>(), buckets.as<uint32_t>(),
-                               perm.as<uint32_t>(), sCounts.as<uint32_t>(), recs.p, ovl.p, ss, &launches);
+                               sCounts.as<uint32_t>(), recs.p, ovl.p, ss, &launches);
         launch_scan(sCounts.as<uint32_t>(), sOffsets.as<uint32_t>(), nWork_, sTileSums.as<uint32_t>(),
                     st + kSurfTotal, st + kSurfOverflow, ss, &launches);
         // Without a hit list (PartialNode keys, or the tuned strategy) the

@@ -133,7 +133,7 @@ private:
 
     DevBuf tables, status, counts, offsets, tileSums;
     DevBuf fill, surf, fin, ranks, rankTiles, pruneScratch, pruneLists;
-    DevBuf codes, unitCounts, perm, buckets, recs, ovl, hitList, keys;
+    DevBuf codes, unitCounts, buckets, recs, ovl, hitList, keys;
     // The surface pass runs on a second stream beside the solid pass (its
     // own work-list scan buffers), joined before pruning (surface bits) and
     // before emission (merged keys).

@@ -174,38 +174,6 @@ __global__ void surfaceClassifyKernel(Batch b, uint32_t nWork, uint32_t* __restr
     }
 }
 
-// Pass 2 (work-triangle order): position of every triangle with work in the
-// partitioned order; unitsP holds its units there (zero past the end).
-__global__ void surfaceScatterKernel(const uint32_t* __restrict__ codes, const uint32_t* __restrict__ units,
-                                     uint32_t nT, const uint32_t* __restrict__ bucketCount,
-                                     uint32_t* __restrict__ bucketCursor, uint32_t* __restrict__ perm,
-                                     uint32_t* __restrict__ unitsP) {
-    __shared__ uint32_t bucketBase[kSurfaceBuckets];
-    if (threadIdx.x < kSurfaceBuckets) {
-        uint32_t s = 0;
-        for (uint32_t k = 0; k < threadIdx.x; ++k) s += bucketCount[k];
-        bucketBase[threadIdx.x] = s;
-    }
-    __syncthreads();
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < nT; base += stride) {
-        const uint32_t t = base + lane;
-        const uint32_t u = t < nT ? __ldg(units + t) : 0u;
-        const uint32_t b = t < nT ? bucketOf(__ldg(codes + t), u) : kNone;
-        const uint32_t peers = __match_any_sync(kFull, b);
-        const uint32_t leader = __ffs(peers) - 1;
-        uint32_t start = 0;
-        if (b != kNone && lane == leader) start = atomicAdd(bucketCursor + b, (uint32_t)__popc(peers));
-        start = __shfl_sync(kFull, start, leader);
-        if (b != kNone) {
-            const uint32_t pos = bucketBase[b] + start + __popc(peers & laneMaskLt());
-            perm[pos] = t;
-            unitsP[pos] = u;
-        }
-    }
-}
-
 struct Overlap { float nx[3], ny[3], de[3]; };
 
 // Set-up record of one partitioned triangle (64 bytes) and its projection
@@ -264,51 +232,78 @@ template <int OT> __device__ __forceinline__ bool overlapTest(const Overlap& o, 
     return r;
 }
 
-// Pass 3 (partitioned order): the set-up record of every triangle with work.
-__global__ void surfaceSetupKernel(Batch b, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ codes,
-                                   const uint32_t* __restrict__ bucketCount, SurfRec* __restrict__ recs,
-                                   SurfOvl* __restrict__ ovl) {
-    uint32_t nP = 0;
+// The set-up record of work triangle wt at partitioned position pos.
+__device__ __forceinline__ void setupRecord(const Batch& b, uint32_t wt, uint32_t code, uint32_t pos,
+                                            SurfRec* __restrict__ recs, SurfOvl* __restrict__ ovl) {
+    uint32_t t;
+    const uint32_t unit = workUnit(b, wt, &t);
+    const Unit& U = b.units[unit];
+    const PassGeom g = U.g;
+    F3 v[3];
+    loadTriF(U.V, U.I, t, v);
+    const uint32_t bb = code >> 30, axis = (code >> 28) & 3u;
+    const IBox box = gridClamp(voxBoundsHalf(v, g), g);
+    SurfRec r;
 #pragma unroll
-    for (uint32_t k = 0; k < kSurfaceBuckets; ++k) nP += __ldg(bucketCount + k);
-    for (uint32_t pos = blockIdx.x * blockDim.x + threadIdx.x; pos < nP; pos += gridDim.x * blockDim.x) {
-        const uint32_t wt = __ldg(perm + pos);
-        uint32_t t;
-        const uint32_t unit = workUnit(b, wt, &t);
-        const Unit& U = b.units[unit];
-        const PassGeom g = U.g;
-        F3 v[3];
-        loadTriF(U.V, U.I, t, v);
-        const uint32_t code = __ldg(codes + wt);
-        const uint32_t bb = code >> 30, axis = (code >> 28) & 3u;
-        const IBox box = gridClamp(voxBoundsHalf(v, g), g);
-        SurfRec r;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) { r.lo[a] = box.lo[a]; r.hi[a] = box.hi[a]; }
-        r.code = code;
-        r.key = (bb << 8) | (U.M ? __ldg(U.M + t) : 0u);
-        r.tri = t;
-        r.v0[0] = v[0].x; r.v0[1] = v[0].y; r.v0[2] = v[0].z;
-        r.n[0] = r.n[1] = r.n[2] = 0.0f;
-        r.unit = unit;
-        const float d = g.df;
-        if (bb == 2) {
-            const F3 n = crossF<site::CRF_2D>(subF(v[0], v[2]), subF(v[1], v[0]));
-            r.n[0] = n.x; r.n[1] = n.y; r.n[2] = n.z;
-            if (axis == 0) ovl[pos].o[0] = setupOverlap<0, site::DE_2D_YZ>(v, n, d);
-            else if (axis == 1) ovl[pos].o[1] = setupOverlap<1, site::DE_2D_ZX>(v, n, d);
-            else ovl[pos].o[2] = setupOverlap<2, site::DE_2D_XY>(v, n, d);
-        } else if (bb == 3) {
-            const F3 n = crossF<site::CRF_3D>(subF(v[0], v[2]), subF(v[1], v[0]));
-            r.n[0] = n.x; r.n[1] = n.y; r.n[2] = n.z;
-            SurfOvl o;
-            o.o[0] = setupOverlap<0, site::DE_3D_YZ>(v, n, d);
-            o.o[1] = setupOverlap<1, site::DE_3D_ZX>(v, n, d);
-            o.o[2] = setupOverlap<2, site::DE_3D_XY>(v, n, d);
-            o.pad = 0;
-            ovl[pos] = o;
+    for (int a = 0; a < 3; ++a) { r.lo[a] = box.lo[a]; r.hi[a] = box.hi[a]; }
+    r.code = code;
+    r.key = (bb << 8) | (U.M ? __ldg(U.M + t) : 0u);
+    r.tri = t;
+    r.v0[0] = v[0].x; r.v0[1] = v[0].y; r.v0[2] = v[0].z;
+    r.n[0] = r.n[1] = r.n[2] = 0.0f;
+    r.unit = unit;
+    const float d = g.df;
+    if (bb == 2) {
+        const F3 n = crossF<site::CRF_2D>(subF(v[0], v[2]), subF(v[1], v[0]));
+        r.n[0] = n.x; r.n[1] = n.y; r.n[2] = n.z;
+        if (axis == 0) ovl[pos].o[0] = setupOverlap<0, site::DE_2D_YZ>(v, n, d);
+        else if (axis == 1) ovl[pos].o[1] = setupOverlap<1, site::DE_2D_ZX>(v, n, d);
+        else ovl[pos].o[2] = setupOverlap<2, site::DE_2D_XY>(v, n, d);
+    } else if (bb == 3) {
+        const F3 n = crossF<site::CRF_3D>(subF(v[0], v[2]), subF(v[1], v[0]));
+        r.n[0] = n.x; r.n[1] = n.y; r.n[2] = n.z;
+        SurfOvl o;
+        o.o[0] = setupOverlap<0, site::DE_3D_YZ>(v, n, d);
+        o.o[1] = setupOverlap<1, site::DE_3D_ZX>(v, n, d);
+        o.o[2] = setupOverlap<2, site::DE_3D_XY>(v, n, d);
+        o.pad = 0;
+        ovl[pos] = o;
+    }
+    recs[pos] = r;
+}
+
+// Pass 2 (work-triangle order): the position of every triangle with work in
+// the partitioned order, its units there (unitsP, zero past the end) and its
+// set-up record.
+__global__ void surfacePartitionKernel(Batch bt, const uint32_t* __restrict__ codes,
+                                       const uint32_t* __restrict__ units, uint32_t nT,
+                                       const uint32_t* __restrict__ bucketCount, uint32_t* __restrict__ bucketCursor,
+                                       uint32_t* __restrict__ unitsP, SurfRec* __restrict__ recs,
+                                       SurfOvl* __restrict__ ovl) {
+    __shared__ uint32_t bucketBase[kSurfaceBuckets];
+    if (threadIdx.x < kSurfaceBuckets) {
+        uint32_t s = 0;
+        for (uint32_t k = 0; k < threadIdx.x; ++k) s += bucketCount[k];
+        bucketBase[threadIdx.x] = s;
+    }
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < nT; base += stride) {
+        const uint32_t t = base + lane;
+        const uint32_t u = t < nT ? __ldg(units + t) : 0u;
+        const uint32_t code = t < nT ? __ldg(codes + t) : 0u;
+        const uint32_t b = t < nT ? bucketOf(code, u) : kNone;
+        const uint32_t peers = __match_any_sync(kFull, b);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t start = 0;
+        if (b != kNone && lane == leader) start = atomicAdd(bucketCursor + b, (uint32_t)__popc(peers));
+        start = __shfl_sync(kFull, start, leader);
+        if (b != kNone) {
+            const uint32_t pos = bucketBase[b] + start + __popc(peers & laneMaskLt());
+            unitsP[pos] = u;
+            setupRecord(bt, t, code, pos, recs, ovl);
         }
-        recs[pos] = r;
     }
 }
 
@@ -808,14 +803,13 @@ __global__ void mergeKeysKernel(const unsigned long long* __restrict__ list, con
 }  // namespace
 
 void launch_surface_prepare(const Batch& b, uint32_t nWork, uint32_t* codes, uint32_t* units, uint32_t* buckets,
-                            uint32_t* perm, uint32_t* unitsP, void* recs, void* ovl, cudaStream_t s,
+                            uint32_t* unitsP, void* recs, void* ovl, cudaStream_t s,
                             uint32_t* launches) {
     const uint32_t grid = gridFor(nWork, 256);
     surfaceClassifyKernel<<<grid, 256, 0, s>>>(b, nWork, codes, units, buckets);
-    surfaceScatterKernel<<<grid, 256, 0, s>>>(codes, units, nWork, buckets, buckets + kSurfaceBuckets, perm, unitsP);
-    surfaceSetupKernel<<<grid, 256, 0, s>>>(b, perm, codes, buckets, static_cast<SurfRec*>(recs),
-                                            static_cast<SurfOvl*>(ovl));
-    *launches += 3;
+    surfacePartitionKernel<<<grid, 256, 0, s>>>(b, codes, units, nWork, buckets, buckets + kSurfaceBuckets, unitsP,
+                                                static_cast<SurfRec*>(recs), static_cast<SurfOvl*>(ovl));
+    *launches += 2;
 }
 
 template <int K>
