@@ -21,7 +21,7 @@ def _tuner_off():
 
 def test_modes_and_cache_file(tmp_path):
     path = tmp_path / "shapes.json"
-    good = {"surf_blocks_per_sm": 16, "surf_batch": 8, "merge_blocks_per_sm": 32, "emit_blocks_per_sm": 8,
+    good = {"surf_blocks_per_sm": 16, "surf_batch": 8, "merge_blocks_per_sm": 16, "emit_blocks_per_sm": 8,
             "toggle_blocks_per_sm": 6, "surf_queue": 1, "toggle_queue": 1, "surf_merge": 1}
     bad_shape = dict(good, surf_blocks_per_sm=7)
     bad_merge = dict(good, surf_merge=2)

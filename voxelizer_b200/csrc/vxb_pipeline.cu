@@ -380,7 +380,6 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
         // Material keys by surface rank (independent of pruning).
         if (timer) timer->mark(4, false, ss);
         launch_surface_keys_zero(keys.p, st + kSurfaceVoxels, keysCap_, wide_ ? 1 : 0, ss, &launches);
-        tuneMark(kKnobMerge, false, ss);
         if (!retraverse)
             launch_surface_merge(hitList.as<unsigned long long>(), st + kHitCount, listCap_, ranks.as<WordRank>(),
                                  keys.as<uint32_t>(), keysCap_, shape.mergeBlocksPerSm, ss, &launches);
@@ -389,7 +388,6 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
                                 st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<WordRank>(),
                                 keys.p, keysCap_, nullptr, st + kHitCount, 0, shape.surfBlocksPerSm, shape.surfBatch,
                                 shape.surfQueue ? st + kSurfQueue : nullptr, ss, &launches);
-        tuneMark(kKnobMerge, true, ss);
         tuneMark(kKnobSurfaceSpan, true, ss);
         if (timer) timer->mark(4, true, ss);
         VXB_CUDA(cudaEventRecord(evSurfDone_, ss));
@@ -414,9 +412,17 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
         VXB_CUDA(cudaGetLastError());
         return 0;
     }
+    // The merge knob is timed on this stream from the join with the surface
+    // bits (pruning runs beside the merge) to the join with the merged keys:
+    // the merge's cost on the way to emission, not its own duration.
+    bool mergeSpan = false;
     // Split-ordered pruning (src/host_side.cpp:1183-1206).
     if (anyCartesian_ && !raw_) {
-        if (anyMaterials_) VXB_CUDA(cudaStreamWaitEvent(s, evSurfBits_, 0));
+        if (anyMaterials_) {
+            VXB_CUDA(cudaStreamWaitEvent(s, evSurfBits_, 0));
+            tuneMark(kKnobMerge, false, s);
+            mergeSpan = true;
+        }
         mark(2, false);
         if (anyMaterials_)
             launch_combine(fillP, surf.as<uint32_t>(), fin.as<uint32_t>(), totalWords_, s, &launches);
@@ -448,7 +454,11 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
         mark(2, true);
     }
     // Join: emission reads the merged keys.
-    if (anyMaterials_) VXB_CUDA(cudaStreamWaitEvent(s, evSurfDone_, 0));
+    if (anyMaterials_) {
+        if (!mergeSpan) tuneMark(kKnobMerge, false, s);
+        VXB_CUDA(cudaStreamWaitEvent(s, evSurfDone_, 0));
+        tuneMark(kKnobMerge, true, s);
+    }
     // Node emission.
     mark(3, false);
     if (raw_ && anyCartesian_)

@@ -17,7 +17,7 @@ namespace vxb {
 struct LaunchShape {
     uint32_t surfBlocksPerSm = 16;   // surfaceWorkKernel blocks per SM
     uint32_t surfBatch = 8;          // surfaceWorkKernel 32-item chunks per owner search
-    uint32_t mergeBlocksPerSm = 8;   // mergeKeysKernel
+    uint32_t mergeBlocksPerSm = 8;   // mergeKeysKernel (timed from the surface-bits join to the keys join)
     uint32_t emitBlocksPerSm = 16;   // emitNarrowKernel
     uint32_t toggleBlocksPerSm = 3;  // solidToggleKernel
     // Work distribution of surfaceWorkKernel / solidToggleKernel: 0 a fixed
