@@ -543,6 +543,9 @@ def served_rows(args, local, rates, seconds):
     from voxelizer_b200.serve import VoxelServer
 
     torch.cuda.set_device(local)
+    # Default launch shapes: no tuning trials inside the timed request streams.
+    from voxelizer_b200 import _lib
+    _lib.set_autotune(0)
     pool = scenes.batch_mix(args.batch_meshes, seed=1)
     rng = np.random.default_rng(7)
     rows = []
@@ -610,10 +613,10 @@ def served_rows(args, local, rates, seconds):
     return rows
 
 
-def autotune(args, call, rounds=12):
+def autotune(args, call, rounds=16):
     """With --autotune on: switch the launch-shape tuner on and make
-    `rounds` untimed calls (3 candidate shapes x 2 samples, then 2
-    material-key strategies x 2 samples settle a size bucket); returns the
+    `rounds` untimed calls (3 candidate shapes x 3 samples, then 2
+    material-key strategies x 3 samples settle a size bucket); returns the
     settled shapes (None when off)."""
     if args.autotune != "on":
         return None

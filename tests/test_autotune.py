@@ -21,7 +21,7 @@ def _tuner_off():
 
 def test_modes_and_cache_file(tmp_path):
     path = tmp_path / "shapes.json"
-    good = {"surf_blocks_per_sm": 16, "surf_batch": 8, "merge_blocks_per_sm": 16, "emit_blocks_per_sm": 8,
+    good = {"surf_blocks_per_sm": 16, "surf_batch": 8, "merge_blocks_per_sm": 4, "emit_blocks_per_sm": 8,
             "toggle_blocks_per_sm": 6, "surf_queue": 1, "toggle_queue": 1, "surf_merge": 1}
     bad_shape = dict(good, surf_blocks_per_sm=7)
     bad_merge = dict(good, surf_merge=2)
@@ -50,9 +50,9 @@ def test_tuning_keeps_results_and_settles(tmp_path):
         want, _ = vx.voxelizeToNodesToRAM(160)
         wbits, _ = vx.voxelizeToRAM(160)
         _lib.set_autotune(1, str(path))
-        # 3 shape candidates x 2 samples, then (node grids with materials)
-        # 2 material-key strategies x 2 samples settle a bucket.
-        for _ in range(12):
+        # 3 shape candidates x 3 samples, then (node grids with materials)
+        # 2 material-key strategies x 3 samples settle a bucket.
+        for _ in range(16):
             got, _ = vx.voxelizeToNodesToRAM(160)
             assert np.array_equal(got, want)
             bits, _ = vx.voxelizeToRAM(160)

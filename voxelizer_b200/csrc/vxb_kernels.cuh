@@ -119,9 +119,11 @@ void launch_surface_rank(const uint32_t* bits, uint64_t words, WordRank* ranks, 
 void launch_surface_keys_zero(void* keys, const uint32_t* count, uint32_t cap, int wide, cudaStream_t s,
                               uint32_t* launches);
 // Keys at ranks >= keysCap are dropped (the host re-merges after growing).
+// blocksPerSm 0 sizes the grid for `entries` entries, a block per 1,024
+// (non-persistent).
 void launch_surface_merge(const unsigned long long* list, const uint32_t* listCount, uint32_t listCap,
                           const WordRank* ranks, uint32_t* keys, uint32_t keysCap,
-                          uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches);
+                          uint32_t blocksPerSm, uint32_t entries, cudaStream_t s, uint32_t* launches);
 
 // Mesh checks of vxb_create (vxb_meshcheck.cu): hostOut[0..2] / [3..5]
 // name the first vertex (after vertex 0) holding the smallest / largest

@@ -290,13 +290,22 @@ int Pipeline::prepare(const std::vector<MeshJob>& jobs, cudaStream_t s) {
     if (anyCartesian_ && (rc = pruneScratch.ensure(4 * (groups_.size() * kPasses + 1)))) return rc;
     if (anyCartesian_ && (rc = pruneLists.ensure(2 * 8 * (size_t)pruneCap_))) return rc;
     listCap_ = 0;
+    mergeEntries_ = 0;
     keysCap_ = 0;
     if (anyMaterials_) {
         if (!side_) {
+            // Pruning and emission (on the way to the result) run on a stream
+            // of the greatest priority, so that their blocks are placed
+            // before the merge's when both wait for room on the SMs.
+            int least = 0, greatest = 0;
+            VXB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
             VXB_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+            VXB_CUDA(cudaStreamCreateWithPriority(&hi_, cudaStreamNonBlocking, greatest));
             VXB_CUDA(cudaEventCreateWithFlags(&evFork_, cudaEventDisableTiming));
             VXB_CUDA(cudaEventCreateWithFlags(&evSurfBits_, cudaEventDisableTiming));
             VXB_CUDA(cudaEventCreateWithFlags(&evSurfDone_, cudaEventDisableTiming));
+            VXB_CUDA(cudaEventCreateWithFlags(&evSolid_, cudaEventDisableTiming));
+            VXB_CUDA(cudaEventCreateWithFlags(&evHiDone_, cudaEventDisableTiming));
         }
         if ((rc = sCounts.ensure(4 * ((size_t)nWork_ + 2)))) return rc;
         if ((rc = sOffsets.ensure(4 * ((size_t)nWork_ + 2)))) return rc;
@@ -314,6 +323,9 @@ int Pipeline::prepare(const std::vector<MeshJob>& jobs, cudaStream_t s) {
         // list, the surface voxels are at most its entries.
         if (!wide_) {
             listCap_ = (uint32_t)std::min<uint64_t>(96ull << 20, std::max<uint64_t>(8ull << 20, nodeCount / 12));
+            // Entries the merge's non-persistent grid is sized for (more are
+            // taken by its blocks' grid-stride loops).
+            mergeEntries_ = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(listCap_, nodeCount / 4));
             if ((rc = hitList.ensure((size_t)listCap_ * 8))) return rc;
             keysCap_ = listCap_ + 1;
         } else {
@@ -333,8 +345,11 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
     uint32_t* fillP = aliasFill_ ? static_cast<uint32_t*>(jobs_[0].out) : fill.as<uint32_t>();
     const size_t wordBytes = aliasFill_ ? (size_t)units_[0].g.ipx * units_[0].g.AY * units_[0].g.AZ * 4
                                         : 4 * (size_t)totalWords_;
+    // The stream of the stages on the way to the result: `s`, then (with a
+    // surface pass) the high-priority stream from pruning on.
+    cudaStream_t ps = s;
     auto mark = [&](int stage, bool end) {
-        if (timer) timer->mark(stage, end, s);
+        if (timer) timer->mark(stage, end, ps);
     };
     // Launch shapes of this run; tuning trials are timed per kernel (not
     // while a graph is being captured).
@@ -382,7 +397,7 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
         launch_surface_keys_zero(keys.p, st + kSurfaceVoxels, keysCap_, wide_ ? 1 : 0, ss, &launches);
         if (!retraverse)
             launch_surface_merge(hitList.as<unsigned long long>(), st + kHitCount, listCap_, ranks.as<WordRank>(),
-                                 keys.as<uint32_t>(), keysCap_, shape.mergeBlocksPerSm, ss, &launches);
+                                 keys.as<uint32_t>(), keysCap_, shape.mergeBlocksPerSm, mergeEntries_, ss, &launches);
         else
             launch_surface_work(nodeKind_, 1, wide_ ? 1 : 0, b, recs.p, ovl.p, sOffsets.as<uint32_t>(), nWork_,
                                 st + kSurfTotal, buckets.as<uint32_t>(), surf.as<uint32_t>(), ranks.as<WordRank>(),
@@ -416,24 +431,29 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
     // bits (pruning runs beside the merge) to the join with the merged keys:
     // the merge's cost on the way to emission, not its own duration.
     bool mergeSpan = false;
+    if (anyMaterials_) {
+        VXB_CUDA(cudaEventRecord(evSolid_, s));
+        VXB_CUDA(cudaStreamWaitEvent(hi_, evSolid_, 0));
+        ps = hi_;
+    }
     // Split-ordered pruning (src/host_side.cpp:1183-1206).
     if (anyCartesian_ && !raw_) {
         if (anyMaterials_) {
-            VXB_CUDA(cudaStreamWaitEvent(s, evSurfBits_, 0));
-            tuneMark(kKnobMerge, false, s);
+            VXB_CUDA(cudaStreamWaitEvent(ps, evSurfBits_, 0));
+            tuneMark(kKnobMerge, false, ps);
             mergeSpan = true;
         }
         mark(2, false);
         if (anyMaterials_)
-            launch_combine(fillP, surf.as<uint32_t>(), fin.as<uint32_t>(), totalWords_, s, &launches);
+            launch_combine(fillP, surf.as<uint32_t>(), fin.as<uint32_t>(), totalWords_, ps, &launches);
         else
-            VXB_CUDA(cudaMemcpyAsync(fin.p, fillP, 4 * (size_t)totalWords_, cudaMemcpyDeviceToDevice, s));
-        VXB_CUDA(cudaMemsetAsync(st + kFlags, 0, 4 * (size_t)nRegions_ * kPasses, s));
+            VXB_CUDA(cudaMemcpyAsync(fin.p, fillP, 4 * (size_t)totalWords_, cudaMemcpyDeviceToDevice, ps));
+        VXB_CUDA(cudaMemsetAsync(st + kFlags, 0, 4 * (size_t)nRegions_ * kPasses, ps));
         // Per subspace index and pass: the count of its change list; the
         // last word is the list overflow flag.
         uint32_t* counts = pruneScratch.as<uint32_t>();
         uint32_t* overflow = counts + groups_.size() * kPasses;
-        VXB_CUDA(cudaMemsetAsync(counts, 0, 4 * (groups_.size() * kPasses + 1), s));
+        VXB_CUDA(cudaMemsetAsync(counts, 0, 4 * (groups_.size() * kPasses + 1), ps));
         const PruneRegion* regions = reinterpret_cast<const PruneRegion*>(tables.as<uint8_t>() + oRegions_);
         unsigned long long* lists[2] = {pruneLists.as<unsigned long long>(),
                                         pruneLists.as<unsigned long long>() + pruneCap_};
@@ -442,30 +462,30 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
             const Group& gr = groups_[gi];
             uint32_t* c = counts + gi * kPasses;
             launch_prune(b, regions + gr.first, gr.count, gr.words, fin.as<uint32_t>(), fillP, surfP, st + kFlags,
-                         gr.flagBase, kPasses, lists[0], c, pruneCap_, overflow, s, &launches);
+                         gr.flagBase, kPasses, lists[0], c, pruneCap_, overflow, ps, &launches);
             // Pass 1 over the whole device; later lists are short (usually
             // empty), so passes 2 .. kPasses - 1 run in one block.
             launch_prune_list(b, regions + gr.first, fin.as<uint32_t>(), fillP, surfP, st + kFlags, gr.flagBase,
-                              kPasses, 1, lists[0], c, lists[1], c + 1, pruneCap_, overflow, s, &launches);
+                              kPasses, 1, lists[0], c, lists[1], c + 1, pruneCap_, overflow, ps, &launches);
             launch_prune_list_loop(b, regions + gr.first, gr.count, fin.as<uint32_t>(), fillP, surfP, st + kFlags,
-                                   gr.flagBase, kPasses, 2, lists[0], lists[1], c, pruneCap_, kLoopListMax, overflow, s,
+                                   gr.flagBase, kPasses, 2, lists[0], lists[1], c, pruneCap_, kLoopListMax, overflow, ps,
                                    &launches);
         }
         mark(2, true);
     }
     // Join: emission reads the merged keys.
     if (anyMaterials_) {
-        if (!mergeSpan) tuneMark(kKnobMerge, false, s);
-        VXB_CUDA(cudaStreamWaitEvent(s, evSurfDone_, 0));
-        tuneMark(kKnobMerge, true, s);
+        if (!mergeSpan) tuneMark(kKnobMerge, false, ps);
+        VXB_CUDA(cudaStreamWaitEvent(ps, evSurfDone_, 0));
+        tuneMark(kKnobMerge, true, ps);
     }
     // Node emission.
     mark(3, false);
     if (raw_ && anyCartesian_)
         launch_emit_raw(nodeKind_, b, totalWords_, fillP, surf.as<uint32_t>(), ranks.as<WordRank>(), keys.p, keysCap_,
-                        s, &launches);
+                        ps, &launches);
     else if (anyCartesian_) {
-        tuneMark(kKnobEmit, false, s);
+        tuneMark(kKnobEmit, false, ps);
         if (hostOut_ && units_.size() == 1) {
             // The node array in kOutChunks word ranges, each copied to the
             // caller's pinned host buffer on the copy stream as soon as it
@@ -478,9 +498,9 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
                 const uint64_t w1 = k + 1 == kOutChunks ? words : (words * (k + 1) / kOutChunks) & ~uint64_t(31);
                 if (w1 <= w0) continue;
                 launch_emit_cartesian(nodeKind_, b, w0, w1, fin.as<uint32_t>(), fillP, surf.as<uint32_t>(),
-                                      ranks.as<WordRank>(), keys.p, keysCap_, shape.emitBlocksPerSm, s, &launches);
+                                      ranks.as<WordRank>(), keys.p, keysCap_, shape.emitBlocksPerSm, ps, &launches);
                 if (!outEv_[k]) VXB_CUDA(cudaEventCreateWithFlags(&outEv_[k], cudaEventDisableTiming));
-                VXB_CUDA(cudaEventRecord(outEv_[k], s));
+                VXB_CUDA(cudaEventRecord(outEv_[k], ps));
                 VXB_CUDA(cudaStreamWaitEvent(copyStream_, outEv_[k], 0));
                 VXB_CUDA(cudaMemcpyAsync(static_cast<uint8_t*>(hostOut_) + w0 * wordBytes,
                                          static_cast<const uint8_t*>(u.out) + w0 * wordBytes, (w1 - w0) * wordBytes,
@@ -489,15 +509,19 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
             hostCopied_ = true;
         } else {
             launch_emit_cartesian(nodeKind_, b, 0, totalWords_, fin.as<uint32_t>(), fillP, surf.as<uint32_t>(),
-                                  ranks.as<WordRank>(), keys.p, keysCap_, shape.emitBlocksPerSm, s, &launches);
+                                  ranks.as<WordRank>(), keys.p, keysCap_, shape.emitBlocksPerSm, ps, &launches);
         }
-        tuneMark(kKnobEmit, true, s);
+        tuneMark(kKnobEmit, true, ps);
     }
     if (nFcc_)
         launch_emit_fcc(nodeKind_, b, reinterpret_cast<const FccMesh*>(tables.as<uint8_t>() + oFcc_),
                         reinterpret_cast<const uint64_t*>(tables.as<uint8_t>() + oGroupBase_), nFcc_, totalGroups_,
-                        fillP, surf.as<uint32_t>(), ranks.as<WordRank>(), keys.p, keysCap_, raw_, s, &launches);
+                        fillP, surf.as<uint32_t>(), ranks.as<WordRank>(), keys.p, keysCap_, raw_, ps, &launches);
     mark(3, true);
+    if (ps != s) {
+        VXB_CUDA(cudaEventRecord(evHiDone_, ps));
+        VXB_CUDA(cudaStreamWaitEvent(s, evHiDone_, 0));
+    }
     VXB_CUDA(cudaGetLastError());
     return 0;
 }
@@ -529,9 +553,10 @@ int Pipeline::pruneGroupUntilStable(const Group& gr, cudaStream_t s) {
 }
 
 Pipeline::~Pipeline() {
-    for (cudaEvent_t e : {evFork_, evSurfBits_, evSurfDone_})
+    for (cudaEvent_t e : {evFork_, evSurfBits_, evSurfDone_, evSolid_, evHiDone_})
         if (e) cudaEventDestroy(e);
     if (side_) cudaStreamDestroy(side_);
+    if (hi_) cudaStreamDestroy(hi_);
     for (cudaEvent_t& e : tuneEv_)
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t& e : outEv_)

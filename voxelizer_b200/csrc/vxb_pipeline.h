@@ -125,7 +125,7 @@ private:
     uint64_t totalWords_ = 0, totalRows_ = 0, totalGroups_ = 0;
     int nodeKind_ = 0, nodes_ = 1;
     bool anyMaterials_ = false, anyCartesian_ = false, wide_ = false, aliasFill_ = false, raw_ = false;
-    uint32_t listCap_ = 0, keysCap_ = 0, pruneCap_ = 0;
+    uint32_t listCap_ = 0, keysCap_ = 0, pruneCap_ = 0, mergeEntries_ = 0;
     // table offsets (bytes) in `tables`
     size_t oUnits_ = 0, oWork_ = 0, oRow_ = 0, oWord_ = 0, oSplits_ = 0, oSlices_ = 0, oLater_ = 0, oRegions_ = 0,
            oFcc_ = 0, oGroupBase_ = 0;
@@ -138,8 +138,9 @@ private:
     // own work-list scan buffers), joined before pruning (surface bits) and
     // before emission (merged keys).
     DevBuf sCounts, sOffsets, sTileSums;
-    cudaStream_t side_ = nullptr;
-    cudaEvent_t evFork_ = nullptr, evSurfBits_ = nullptr, evSurfDone_ = nullptr;
+    cudaStream_t side_ = nullptr, hi_ = nullptr;
+    cudaEvent_t evFork_ = nullptr, evSurfBits_ = nullptr, evSurfDone_ = nullptr, evSolid_ = nullptr,
+                evHiDone_ = nullptr;
 };
 
 }  // namespace vxb

@@ -33,6 +33,8 @@
 #include "vxb_device.cuh"
 #include "vxb_kernels.cuh"
 
+#include <algorithm>
+
 namespace vxb {
 
 using namespace detail;
@@ -875,8 +877,13 @@ void launch_surface_keys_zero(void* keys, const uint32_t* count, uint32_t cap, i
 
 void launch_surface_merge(const unsigned long long* list, const uint32_t* listCount, uint32_t listCap,
                           const WordRank* ranks, uint32_t* keys, uint32_t keysCap,
-                          uint32_t blocksPerSm, cudaStream_t s, uint32_t* launches) {
-    mergeKeysKernel<<<148u * blocksPerSm, 256, 0, s>>>(list, listCount, listCap, ranks, keys, keysCap);
+                          uint32_t blocksPerSm, uint32_t entries, cudaStream_t s, uint32_t* launches) {
+    // blocksPerSm 0: a block per 1,024 of the expected entries, so that blocks
+    // retire as they finish and other streams' blocks get room (blocks past
+    // the count exit at once; entries past the grid are taken by its
+    // grid-stride loop).
+    const uint32_t grid = blocksPerSm ? 148u * blocksPerSm : std::max(1u, (entries / 2 + 511) / 512);
+    mergeKeysKernel<<<grid, 256, 0, s>>>(list, listCount, listCap, ranks, keys, keysCap);
     *launches += 1;
 }
 

@@ -19,7 +19,7 @@ namespace {
 const uint32_t kSurfBlocks[kTuneCandidates] = {16, 16, 8};
 const uint32_t kSurfBatch[kTuneCandidates] = {8, 8, 16};
 const uint32_t kSurfQueue[kTuneCandidates] = {0, 1, 1};
-const uint32_t kMerge[kTuneCandidates] = {8, 4, 16};
+const uint32_t kMerge[kTuneCandidates] = {0, 8, 4};
 const uint32_t kEmit[kTuneCandidates] = {16, 8, 32};
 const uint32_t kToggle[kTuneCandidates] = {3, 3, 6};
 const uint32_t kToggleQueue[kTuneCandidates] = {0, 1, 1};

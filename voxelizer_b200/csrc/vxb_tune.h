@@ -17,7 +17,10 @@ namespace vxb {
 struct LaunchShape {
     uint32_t surfBlocksPerSm = 16;   // surfaceWorkKernel blocks per SM
     uint32_t surfBatch = 8;          // surfaceWorkKernel 32-item chunks per owner search
-    uint32_t mergeBlocksPerSm = 8;   // mergeKeysKernel (timed from the surface-bits join to the keys join)
+    // mergeKeysKernel (timed from the surface-bits join to the keys join);
+    // 0: one block per 1,024 expected list entries instead of a persistent
+    // grid (its blocks retire as they finish, so pruning's blocks get room).
+    uint32_t mergeBlocksPerSm = 0;
     uint32_t emitBlocksPerSm = 16;   // emitNarrowKernel
     uint32_t toggleBlocksPerSm = 3;  // solidToggleKernel
     // Work distribution of surfaceWorkKernel / solidToggleKernel: 0 a fixed
@@ -37,7 +40,7 @@ struct LaunchShape {
 enum TuneKnob { kKnobSurface = 0, kKnobMerge = 1, kKnobEmit = 2, kKnobToggle = 3, kKnobSurfaceSpan = 4, kKnobs = 5 };
 constexpr int kTuneCandidates = 3;
 constexpr int kMergeCandidates = 2;
-constexpr int kTuneSamples = 2;
+constexpr int kTuneSamples = 3;
 
 enum TuneMode { kTuneOff = 0, kTuneOn = 1, kTuneFrozen = 2 };
 
