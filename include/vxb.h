@@ -288,6 +288,16 @@ vxb_status vxb_voxelize_bits_noalloc(const float* dev_vertices, const uint32_t* 
  * device and allocates nothing. */
 vxb_status vxb_noalloc_status(void);
 
+/* No counterpart in the reference (the reference sums its tile counts on the
+ * host).  The exclusive scan that sizes every work list, exported so that
+ * its overflow detection can be tested without a work list of 2^32
+ * entries: scans n device counts into offsets (n + 1 device entries) on
+ * `stream`, waits, and writes the 32-bit total and the overflow flag (1 when
+ * the sum is 2^32 - 1 or more, and the offsets are then not valid).
+ * Allocates its tile sums. */
+vxb_status vxb_scan_counts(const uint32_t* counts, uint32_t n, uint32_t* offsets, uint32_t* total,
+                           uint32_t* overflow, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

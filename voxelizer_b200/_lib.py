@@ -24,7 +24,7 @@ NODE_BYTES = {SHORT: 1, LONG: 2, PARTIAL: 8, SHORT_FCC: 2, LONG_FCC: 4}
 EXPORTS = ["vxb_last_error", "vxb_version", "vxb_create", "vxb_destroy", "vxb_set_materials",
            "vxb_set_material_output", "vxb_verbose_output", "vxb_plan", "vxb_get_array_dimensions",
            "vxb_voxelize_to_host", "vxb_voxelize_to_device", "vxb_last_launch_count", "vxb_set_profiling",
-           "vxb_stage_times", "vxb_stage_timeline", "vxb_voxelize_bits_noalloc", "vxb_trim_cache", "vxb_batch_create",
+           "vxb_stage_times", "vxb_stage_timeline", "vxb_scan_counts", "vxb_voxelize_bits_noalloc", "vxb_trim_cache", "vxb_batch_create",
            "vxb_batch_destroy", "vxb_batch_add", "vxb_batch_clear", "vxb_batch_run", "vxb_batch_last_launch_count",
            "vxb_last_stats", "vxb_plan_parts", "vxb_voxelize_parts_to_device", "vxb_voxelize_parts_to_host",
            "vxb_plan_slice", "vxb_voxelize_slice_to_device", "vxb_voxelize_slice_to_host", "vxb_set_autotune",
@@ -109,6 +109,8 @@ def lib():
         "vxb_set_profiling": (ctypes.c_int, [vp, ctypes.c_int]),
         "vxb_stage_times": (ctypes.c_int, [vp, P(ctypes.c_float), ctypes.c_uint32]),
         "vxb_stage_timeline": (ctypes.c_int, [vp, P(ctypes.c_float), ctypes.c_uint32]),
+        "vxb_scan_counts": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, P(ctypes.c_uint32),
+                                           P(ctypes.c_uint32), ctypes.c_void_p]),
         "vxb_plan_parts": (ctypes.c_int, [vp, ctypes.c_int, P(Request), ctypes.c_uint32, ctypes.c_uint32,
                                           P(GridInfo)]),
         "vxb_voxelize_parts_to_device": (ctypes.c_int, [vp, ctypes.c_int, P(Request), ctypes.c_uint32,

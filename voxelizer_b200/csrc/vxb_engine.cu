@@ -555,6 +555,27 @@ vxb_status vxb_create(vxb_voxelizer** out, int node_type, const float* vertices,
     return VXB_OK;
 }
 
+vxb_status vxb_scan_counts(const uint32_t* counts, uint32_t n, uint32_t* offsets, uint32_t* total,
+                           uint32_t* overflow, void* stream) {
+    if ((!counts && n) || !offsets || !total || !overflow) return failf(VXB_EINVAL, "NULL argument");
+    int dev = 0;
+    VXB_CUDA(cudaGetDevice(&dev));
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    vxb::DevBuf tiles, status;
+    tiles.dev = status.dev = dev;
+    int rc;
+    if ((rc = tiles.ensure(4 * ((size_t)n / 4096 + 2))) || (rc = status.ensure(8))) return rc;
+    uint32_t launches = 0;
+    vxb::launch_scan(counts, offsets, n, tiles.as<uint32_t>(), status.as<uint32_t>(), status.as<uint32_t>() + 1, s,
+                     &launches);
+    uint32_t h[2];
+    VXB_CUDA(cudaMemcpyAsync(h, status.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    VXB_CUDA(cudaStreamSynchronize(s));
+    *total = h[0];
+    *overflow = h[1];
+    return VXB_OK;
+}
+
 vxb_status vxb_bounding_box(const vxb_voxelizer* v, double min_vertex[3], double max_vertex[3]) {
     if (!v || !min_vertex || !max_vertex) return failf(VXB_EINVAL, "NULL argument");
     for (int a = 0; a < 3; ++a) {
