@@ -219,7 +219,9 @@ vxb_status vxb_last_stats(vxb_voxelizer* v, vxb_stats* stats);
 
 /* Stage timing with CUDA events on the call's stream (off by default; no
  * reference counterpart, the reference only prints clock() stamps in verbose
- * mode).  Stages: 0 solid voxelization, 1 surface voxelization, 2 pruning,
+ * mode).  enable: 0 off, 1 on, 2 on with the stages run one after another
+ * on the call's stream instead of the surface pass beside the solid pass
+ * (each stage's time is then its own; results are the same).  Stages: 0 solid voxelization, 1 surface voxelization, 2 pruning,
  * 3 node emission, 4 material merge, 5 the surface work kernel alone (part
  * of stage 1).  vxb_stage_times waits for the last call and writes the
  * milliseconds of up to n stages (-1 for a stage that did not run). */

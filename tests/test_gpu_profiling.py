@@ -2,7 +2,7 @@
 events change no result, every stage of a node grid with materials is
 timed, and the timeline shows the order the streams impose: the surface
 work inside the surface stage, emission after both pruning and the
-material merge."""
+material merge.  The serial mode runs the stages one after another."""
 
 import math
 
@@ -36,3 +36,22 @@ def test_stage_times_and_timeline():
     assert tl["emit"][0] + eps >= tl["prune"][1]
     assert tl["emit"][0] + eps >= tl["merge"][1]
     assert tl["prune"][0] + eps >= tl["solid"][1]
+
+
+@pytest.mark.gpu
+def test_serial_profiling_keeps_results_and_orders_the_stages():
+    v, f = torus(96, 48, 0.6, 0.25)
+    m = Mesh(v, f, (1 + np.arange(f.shape[0]) % 5).astype(np.uint8), 6)
+    with Voxelizer(m.vertices, m.indices, m.materials, m.n_materials, node_type=LONG) as vx:
+        want, _ = vx.voxelizeToNodesToRAM(160)
+        vx.set_profiling(True, serial=True)
+        got, _ = vx.voxelizeToNodesToRAM(160)
+        tl = vx.stage_timeline()
+        vx.set_profiling(False)
+        assert np.array_equal(got, want)
+    eps = 1e-3
+    # The surface pass (with its merge) runs first, then the solid pass,
+    # pruning and emission, none beside another.
+    assert tl["surface"][1] <= eps and tl["merge"][1] <= eps
+    assert tl["prune"][0] + eps >= tl["solid"][1]
+    assert tl["emit"][0] + eps >= tl["prune"][1]

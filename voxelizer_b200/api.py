@@ -185,8 +185,10 @@ class Voxelizer:
         check(lib().vxb_voxelize_parts_to_host(self._h, int(bool(nodes)), ctypes.byref(r), dy, dz, ptrs, sizes, arr))
         return list(zip(outs, list(arr)))
 
-    def set_profiling(self, enable):
-        check(lib().vxb_set_profiling(self._h, int(bool(enable))))
+    def set_profiling(self, enable, serial=False):
+        """Stage events on (off with enable False); serial runs the stages
+        one after another so that each stage's time is its own."""
+        check(lib().vxb_set_profiling(self._h, (2 if serial else 1) if enable else 0))
 
     STAGES = ("solid", "surface", "prune", "emit", "merge", "surface_work")
 

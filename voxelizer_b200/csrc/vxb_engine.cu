@@ -846,7 +846,9 @@ vxb_status vxb_voxelize_to_host(vxb_voxelizer* v, int nodes, const vxb_request* 
 
 vxb_status vxb_set_profiling(vxb_voxelizer* v, int enable) {
     if (!v) return failf(VXB_EINVAL, "voxelizer is NULL");
+    if (enable < 0 || enable > 2) return failf(VXB_EINVAL, "profiling mode must be 0, 1 or 2");
     v->timer.enabled = enable != 0;
+    v->timer.serial = enable == 2;
     return VXB_OK;
 }
 

@@ -361,10 +361,13 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
     // Surface voxelization, hit list and surface ranks on the side stream,
     // beside the solid pass (they share no buffer).
     cudaStream_t ss = s;
+    const bool serial = timer && timer->enabled && timer->serial;
     if (anyMaterials_) {
-        ss = side_;
-        VXB_CUDA(cudaEventRecord(evFork_, s));
-        VXB_CUDA(cudaStreamWaitEvent(ss, evFork_, 0));
+        if (!serial) {
+            ss = side_;
+            VXB_CUDA(cudaEventRecord(evFork_, s));
+            VXB_CUDA(cudaStreamWaitEvent(ss, evFork_, 0));
+        }
         if (timer) timer->mark(1, false, ss);
         VXB_CUDA(cudaMemsetAsync(surf.p, 0, 4 * (size_t)totalWords_, ss));
         VXB_CUDA(cudaMemsetAsync(buckets.p, 0, 4 * 2 * kSurfaceBuckets, ss));
@@ -431,7 +434,7 @@ int Pipeline::enqueue(cudaStream_t s, StageTimer* timer) {
     // bits (pruning runs beside the merge) to the join with the merged keys:
     // the merge's cost on the way to emission, not its own duration.
     bool mergeSpan = false;
-    if (anyMaterials_) {
+    if (anyMaterials_ && !serial) {
         VXB_CUDA(cudaEventRecord(evSolid_, s));
         VXB_CUDA(cudaStreamWaitEvent(hi_, evSolid_, 0));
         ps = hi_;

@@ -52,6 +52,9 @@ struct StageTimer {
     // work kernel alone (inside stage 1)
     static constexpr int kStages = 6;
     bool enabled = false;
+    // Stages one after another on the call's stream (no second stream), so
+    // that each stage's time is its own.
+    bool serial = false;
     cudaEvent_t ev[2 * kStages] = {};
     bool used[kStages] = {};
     void reset() {
