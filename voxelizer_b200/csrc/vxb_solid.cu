@@ -177,6 +177,21 @@ __device__ __forceinline__ void solidCandidate(const SolidStage& st, const Batch
     // product of the row's coordinate across the row: the same operations
     // in the same order as evaluating each centre from scratch.
     static_assert(site::E_BIN == 0 && site::E_GEN == 0, "row products assume the unfused edge forms");
+    static_assert(site::P_BIN == 0, "corner test assumes the unfused centre form");
+    // Every operation of an unfused binning edge function is monotone in the
+    // centre's row and column (d > 0), so its largest value over the tile's
+    // centres is at the corner its normal points to: a tile where one edge
+    // is negative even there has no member centre.
+    {
+        const uint32_t y0 = max(tileY * 4, lo[0]), y1 = min(tileY * 4 + 4, hi[0]);
+        const uint32_t z0 = max(tileZ * 4, lo[1]), z1 = min(tileZ * 4 + 4, hi[1]);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const double py = lin<site::P_BIN>((double)(st.bnx[k] > 0.0 ? y1 - 1 : y0), d, g.mn[1]);
+            const double pz = lin<site::P_BIN>((double)(st.bny[k] > 0.0 ? z1 - 1 : z0), d, g.mn[2]);
+            if (__dadd_rn(__dadd_rn(__dmul_rn(st.bnx[k], py), __dmul_rn(st.bny[k], pz)), st.bd[k]) < 0.0) return;
+        }
+    }
     bool member = false;
     for (uint32_t iy = tileY * 4; iy < tileY * 4 + 4 && iy < hi[0] && !member; ++iy) {
         if (iy < lo[0]) continue;
