@@ -785,6 +785,7 @@ def main():
             "roofline": roofs[0],
             "roofline_next_kernel": roofs[1],
             "work": stats,
+            "mtriangles_per_s": round(mesh.n_triangles * world / (ms * 1e-3) / 1e6, 1),
             "path_roofline": {"algorithmic_bytes": int(path_bytes),
                               "achieved": round(path_bytes / (ms * 1e-3) / 1e9, 1),
                               "frac": round(path_bytes / (ms * 1e-3) / 1e9 / peak, 4)},
