@@ -564,8 +564,10 @@ def served_rows(args, local, rates, seconds):
                 srv.release(req)
                 return t
 
-            # Warm-up at the measured rate over the whole pool: the lanes'
-            # batch buffers grow to the sizes this load needs before timing.
+            # Warm-up: the whole pool at once (the largest batches the lanes
+            # can form), then the measured rate over the pool, so that the
+            # lanes' batch buffers have grown before timing.
+            _drive(submit, wait, pool, np.zeros(len(pool)))
             _drive(submit, wait, pool, _poisson(rate, min(len(pool), n), rng))
             lat_s, span_s = _drive(submit, wait, pool, arrivals)
             batches = srv.batches
