@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(kBlock, 3) solidToggleKernel(Batch b, uint32_t
             if (threadIdx.x == 32) tLast = t;
         }
         __syncthreads();
-        const uint32_t t0 = tFirst, ns = min(tLast - t0 + 1, kSlots);
+        const uint32_t t0 = tFirst, t1 = tLast, ns = min(t1 - t0 + 1, kSlots);
         // Triangles without candidates between them are never selected
         // (their offset equals the next one) and are not staged.
         if (threadIdx.x < ns) {
@@ -287,7 +287,16 @@ __global__ void __launch_bounds__(kBlock, 3) solidToggleKernel(Batch b, uint32_t
                 }
                 solidCandidate(stage[lo], b, item - stOff[lo], fill);
             } else {
-                const uint32_t wt = findOwner(offsets, nWork, item);
+                // The owner lies past the staged triangles and at most at
+                // the batch's last owner: offsets[t0 + ns] <= item <
+                // offsets[t1 + 1].
+                uint32_t lo = t0 + ns, hi = t1 + 1;
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (__ldg(offsets + mid) <= item) lo = mid;
+                    else hi = mid;
+                }
+                const uint32_t wt = lo;
                 SolidStage st;
                 stageSolid(st, b, wt);
                 solidCandidate(st, b, item - __ldg(offsets + wt), fill);
